@@ -1,0 +1,100 @@
+/*
+ * Additive entry points of the B200 parallax runtime. None of these exists in the
+ * reference ABI; code that links only against parallax/runtime.h never needs them.
+ * They expose what the reference's synchronous, host-coherent ABI cannot express:
+ * device residency of arena blocks, stream-ordered (asynchronous) calls, built-in
+ * kernel handles without a compiler, segmented launches and the serving loop.
+ */
+#ifndef PARALLAX_RUNTIME_EXT_H
+#define PARALLAX_RUNTIME_EXT_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "parallax/runtime.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- errors ---------------------------------------------------------------------- */
+enum parallax_status {
+    PARALLAX_OK = 0,
+    PARALLAX_ERR_INVALID_HANDLE = 1,
+    PARALLAX_ERR_INVALID_ARGUMENT = 2,
+    PARALLAX_ERR_OUT_OF_MEMORY = 3,
+    PARALLAX_ERR_CUDA = 4,
+    PARALLAX_ERR_TIMEOUT = 5,        /* a host wait passed its deadline */
+    PARALLAX_ERR_DEVICE_SPIN = 6,    /* an in-kernel bounded wait gave up */
+    PARALLAX_ERR_UNSUPPORTED = 7,
+    PARALLAX_ERR_NO_DEVICE = 8,
+    PARALLAX_ERR_SHUTDOWN = 9,
+};
+/* Status of the calling thread's most recent ABI call. */
+int parallax_last_error(void);
+const char* parallax_error_string(int status);
+void parallax_clear_error(void);
+
+/* ---- built-in kernels ------------------------------------------------------------ */
+/* Handle for a built-in sm_100a kernel named by a spec string:
+ *   "reduce:<sum|max|min>:<dtype>"        "scan:<dtype>"   "exclusive_scan:<dtype>"
+ *   "sort:<dtype>"                        "sort_kv:u32"   (u64 composite (key<<32|value))
+ *   "copy_if:<dtype>:<pred>"              "remove_if:<dtype>:<pred>"
+ *   "partition:<dtype>:<pred>"            "unique:<dtype>"
+ *   "count_if:<dtype>:<pred>"             "find:<dtype>:<pred>"
+ *   "argminmax:<dtype>"                   "mismatch:<dtype>"
+ *   "map:<name>"                          fixed element-wise ops: "map:saxpy_gather_f32"
+ *                                         (transform2 of 16-byte {float x; u32 pad;
+ *                                         float* p} records to y = a*x + *p, a = the
+ *                                         first 4 capture bytes), "map:affine_f32"
+ *                                         (in-place x = a*x + b, captures {a, b})
+ * dtype: f32 f64 i32 i64 u32 u64. pred: gt:<c> ge:<c> lt:<c> le:<c> eq:<c> ne:<c>
+ * mod:<m>:<r> (x % m == r, integers) nonzero. The handle of a partition spec is also
+ * the partition-scatter handle. Returns NULL on a malformed spec. */
+parallax_kernel_t parallax_builtin_kernel(const char* spec);
+
+/* ---- arena residency ------------------------------------------------------------- */
+enum parallax_residency {
+    /* Default. Every ABI call uploads the arena ranges it reads from the pinned host
+     * mirror and downloads the ranges it writes, so host code sees the reference's
+     * synchronous unified-memory behaviour. */
+    PARALLAX_COHERENT = 0,
+    /* The device copy is authoritative; ABI calls move nothing. Host code moves data
+     * explicitly with parallax_arena_sync_to_device / _to_host. */
+    PARALLAX_DEVICE_RESIDENT = 1,
+};
+/* Applies to the whole arena block that contains ptr. Returns a parallax_status. */
+int parallax_arena_set_residency(void* ptr, int mode);
+int parallax_arena_get_residency(const void* ptr);
+int parallax_arena_sync_to_device(const void* ptr, size_t bytes);
+int parallax_arena_sync_to_host(void* ptr, size_t bytes);
+/* dev_base + (ptr - host_base), or NULL when ptr is not in the arena. */
+void* parallax_arena_device_ptr(const void* host_ptr);
+void parallax_arena_bases(uint64_t* host_base, uint64_t* dev_base);
+size_t parallax_arena_capacity(void);
+size_t parallax_arena_used(void);      /* bytes currently allocated */
+size_t parallax_arena_mapped(void);    /* bytes of device memory backing the arena */
+
+/* ---- streams and asynchronous calls ---------------------------------------------- */
+/* Thread-local CUDA stream for subsequent calls (NULL = the runtime's own per-thread
+ * stream). */
+int parallax_set_stream(void* cuda_stream);
+/* Thread-local. With async != 0, ABI calls only enqueue work on the thread's stream and
+ * return; outputs are valid after parallax_synchronize(). Host-memory operands are not
+ * allowed in async mode (device pointers and DEVICE_RESIDENT arena blocks are). A
+ * reduce `result` must then be a device pointer; copy_if returns SIZE_MAX and the
+ * count is available from parallax_last_count() after synchronizing. */
+int parallax_set_async(int async);
+int parallax_synchronize(void);
+size_t parallax_last_count(void);
+
+/* ---- instrumentation ------------------------------------------------------------- */
+/* Number of runtime kernel launches issued by this process so far. */
+uint64_t parallax_launch_count(void);
+/* Device ordinal, SM count and device name; returns a parallax_status. */
+int parallax_device_info(int* device, int* sm_count, char* name, size_t name_cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PARALLAX_RUNTIME_EXT_H */

@@ -1,0 +1,105 @@
+"""Build recipe for libparallax-runtime.so (sm_100a).
+
+Compiles every CUDA/C++ source under csrc/ with nvcc for sm_100a and links one shared
+library, lib/libparallax-runtime.so, that exports the parallax C ABI. Objects go to
+_build/ and are rebuilt when a source or any header is newer than the object.
+
+    python parallax-runtime_b200/build.py [--force] [--jobs N]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB_DIR = PKG / "lib"
+LIB = LIB_DIR / "libparallax-runtime.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [
+    "-std=c++17", "-O3", "-lineinfo", *ARCH,
+    "-Xcompiler", "-fPIC,-fvisibility=hidden,-Wall,-Wno-unused-function",
+    "--expt-relaxed-constexpr",
+    "-I", str(ROOT / "include"), "-I", str(CSRC),
+]
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def sources() -> list[Path]:
+    return sorted(CSRC.rglob("*.cu"))
+
+
+def headers() -> list[Path]:
+    hs = list(CSRC.rglob("*.cuh")) + list(CSRC.rglob("*.hpp"))
+    hs += list((ROOT / "include").rglob("*.h"))
+    return hs
+
+
+def obj_for(src: Path) -> Path:
+    rel = src.relative_to(CSRC).with_suffix(".o")
+    return BUILD / str(rel).replace(os.sep, "__")
+
+
+def compile_one(src: Path, newest_header: float, force: bool, extra: list[str]) -> tuple[Path, str]:
+    obj = obj_for(src)
+    if (not force and obj.exists() and obj.stat().st_mtime >= src.stat().st_mtime
+            and obj.stat().st_mtime >= newest_header):
+        return obj, ""
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")
+    return obj, r.stderr
+
+
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False,
+          ptxas_verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    LIB_DIR.mkdir(exist_ok=True)
+    newest_header = max((h.stat().st_mtime for h in headers()), default=0.0)
+    extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+    srcs = sources()
+    jobs = jobs or min(len(srcs), os.cpu_count() or 4)
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(lambda s: compile_one(s, newest_header, force or ptxas_verbose, extra), srcs))
+    objs = [o for o, _ in results]
+    if verbose or ptxas_verbose:
+        for o, log in results:
+            if log:
+                print(f"== {o.name}\n{log}", file=sys.stderr)
+    if (force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs)):
+        tmp = LIB.with_suffix(".so.tmp")
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs),
+               "-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, LIB)
+    return LIB
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--jobs", type=int, default=None)
+    ap.add_argument("--ptxas-verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, jobs=a.jobs, verbose=True, ptxas_verbose=a.ptxas_verbose))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,376 @@
+// Device-resident arena with a pinned host mirror.
+//
+// Replaces the reference UnifiedArena (src/memory/arena.cpp:21-181, :336-406 and the C
+// accessors in src/memory/unified_allocator.cpp:55-103). The reference maps one Vulkan
+// buffer into the host (UMA) or keeps a device buffer plus a staging copy and moves the
+// WHOLE used range both ways around every top-level call (arena.cpp:296-304). Here:
+//   * device side: one contiguous virtual range (cuMemAddressReserve) whose physical
+//     HBM is mapped in 512 MiB chunks as the arena grows, so a 64 GiB capacity costs
+//     nothing until used;
+//   * host side: one contiguous anonymous mapping of the same size; every mapped chunk
+//     is page-locked so host<->device copies run at full link speed;
+//   * the relocation formula of the reference stays exact: the device address of a
+//     host arena pointer p is dev_base + (p - host_base);
+//   * blocks carry a residency mode; ABI calls move only the byte ranges they name
+//     (see abi.cu), never the whole arena;
+//   * allocation is first-fit over an offset-ordered free map with coalescing (the
+//     reference never coalesces, arena.cpp:354-355), 256-byte minimum alignment.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/mman.h>
+
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "runtime.hpp"
+
+namespace pxb {
+
+namespace {
+
+constexpr size_t kAlign = 256;
+constexpr size_t kDefaultCapacityMiB = 64 * 1024;  // 64 GiB of address space
+
+struct DriverFns {
+    PFN_cuMemAddressReserve reserve = nullptr;
+    PFN_cuMemCreate create = nullptr;
+    PFN_cuMemMap map = nullptr;
+    PFN_cuMemSetAccess set_access = nullptr;
+    PFN_cuMemGetAllocationGranularity granularity = nullptr;
+    bool load() {
+        cudaDriverEntryPointQueryResult q;
+        auto get = [&](const char* name, void** fn) {
+            return cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess && *fn;
+        };
+        return get("cuMemAddressReserve", (void**)&reserve) &&
+               get("cuMemCreate", (void**)&create) && get("cuMemMap", (void**)&map) &&
+               get("cuMemSetAccess", (void**)&set_access) &&
+               get("cuMemGetAllocationGranularity", (void**)&granularity);
+    }
+};
+
+struct Arena {
+    std::mutex mu;
+    bool tried = false;
+    bool ok = false;
+    size_t capacity = 0;
+    char* host_base = nullptr;
+    CUdeviceptr dev_base = 0;
+    size_t chunk = 512ull << 20;
+    size_t mapped = 0;     // bytes with device memory mapped and host pages locked
+    size_t bump = 0;       // first never-used offset
+    size_t used = 0;       // bytes in live blocks
+    std::map<size_t, size_t> free_blocks;       // offset -> size, coalesced
+    std::map<size_t, ArenaBlock> live;          // offset -> block
+    DriverFns drv;
+    std::vector<CUmemGenericAllocationHandle> handles;
+
+    static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+    bool init() {
+        if (tried) return ok;
+        tried = true;
+        if (!ensure_device()) return false;
+        size_t mib = kDefaultCapacityMiB;
+        if (const char* e = getenv("PARALLAX_ARENA_SIZE")) {
+            unsigned long long v = strtoull(e, nullptr, 10);
+            if (v > 0) mib = v;
+        }
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        capacity = mib << 20;
+        if (total_b && capacity > total_b / 10 * 9) capacity = total_b / 10 * 9;
+        if (!drv.load()) {
+            set_error(PARALLAX_ERR_CUDA, "arena: CUDA virtual memory entry points unavailable");
+            return false;
+        }
+        CUmemAllocationProp prop{};
+        prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+        prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+        prop.location.id = device_info().device;
+        size_t gran = 0;
+        if (drv.granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED) != CUDA_SUCCESS ||
+            gran == 0)
+            gran = 2ull << 20;
+        chunk = align_up(chunk, gran);
+        capacity = align_up(capacity, chunk);
+        if (drv.reserve(&dev_base, capacity, chunk, 0, 0) != CUDA_SUCCESS) {
+            set_error(PARALLAX_ERR_OUT_OF_MEMORY, "arena: cannot reserve %zu MiB of device VA",
+                      capacity >> 20);
+            return false;
+        }
+        void* h = mmap(nullptr, capacity, PROT_READ | PROT_WRITE,
+                       MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE, -1, 0);
+        if (h == MAP_FAILED) {
+            set_error(PARALLAX_ERR_OUT_OF_MEMORY, "arena: cannot reserve %zu MiB of host VA",
+                      capacity >> 20);
+            return false;
+        }
+        host_base = static_cast<char*>(h);
+        ok = true;
+        if (getenv("PARALLAX_DEBUG"))
+            fprintf(stderr, "[parallax] arena: capacity %zu MiB host_base=%p dev_base=0x%llx\n",
+                    capacity >> 20, (void*)host_base, (unsigned long long)dev_base);
+        return true;
+    }
+
+    // Maps device memory (and locks the host mirror) up to `end` bytes.
+    bool grow_to(size_t end) {
+        while (mapped < end) {
+            CUmemAllocationProp prop{};
+            prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+            prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+            prop.location.id = device_info().device;
+            CUmemGenericAllocationHandle hdl;
+            if (drv.create(&hdl, chunk, &prop, 0) != CUDA_SUCCESS) return false;
+            if (drv.map(dev_base + mapped, chunk, 0, hdl, 0) != CUDA_SUCCESS) return false;
+            CUmemAccessDesc acc{};
+            acc.location = prop.location;
+            acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+            if (drv.set_access(dev_base + mapped, chunk, &acc, 1) != CUDA_SUCCESS) return false;
+            if (cudaHostRegister(host_base + mapped, chunk, cudaHostRegisterDefault) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+            handles.push_back(hdl);
+            mapped += chunk;
+        }
+        return true;
+    }
+
+    void* allocate(size_t size, size_t align) {
+        if (size == 0) return nullptr;
+        std::lock_guard<std::mutex> g(mu);
+        if (!init()) return nullptr;
+        size_t a = align < kAlign ? kAlign : align;
+        if (a & (a - 1)) a = align_up(a, kAlign);
+        size_t need = align_up(size, kAlign);
+        // first fit in offset order
+        for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
+            size_t off = align_up(it->first, a);
+            size_t pad = off - it->first;
+            if (it->second < pad + need) continue;
+            size_t blk_off = it->first, blk_size = it->second;
+            free_blocks.erase(it);
+            if (pad) free_blocks[blk_off] = pad;
+            size_t rest = blk_size - pad - need;
+            if (rest) free_blocks[off + need] = rest;
+            return commit(off, need);
+        }
+        size_t off = align_up(bump, a);
+        if (off + need > capacity) {
+            set_error(PARALLAX_ERR_OUT_OF_MEMORY,
+                      "arena: out of memory (requested %zu bytes, %zu of %zu in use)", need, used,
+                      capacity);
+            return nullptr;
+        }
+        if (!grow_to(off + need)) {
+            set_error(PARALLAX_ERR_OUT_OF_MEMORY, "arena: cannot map device memory for %zu bytes",
+                      need);
+            return nullptr;
+        }
+        if (off > bump) free_blocks[bump] = off - bump;
+        bump = off + need;
+        return commit(off, need);
+    }
+
+    void* commit(size_t off, size_t need) {
+        ArenaBlock b;
+        b.offset = off;
+        b.size = need;
+        b.residency = PARALLAX_COHERENT;
+        live[off] = b;
+        used += need;
+        return host_base + off;
+    }
+
+    void deallocate(void* p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> g(mu);
+        if (!ok || !contains(p)) return;
+        size_t off = static_cast<char*>(p) - host_base;
+        auto it = live.find(off);
+        if (it == live.end()) return;  // not a block start or double free: ignore
+        size_t size = it->second.size;
+        live.erase(it);
+        used -= size;
+        // insert and coalesce with neighbours
+        auto nx = free_blocks.lower_bound(off);
+        if (nx != free_blocks.end() && off + size == nx->first) {
+            size += nx->second;
+            nx = free_blocks.erase(nx);
+        }
+        if (nx != free_blocks.begin()) {
+            auto pv = std::prev(nx);
+            if (pv->first + pv->second == off) {
+                pv->second += size;
+                return;
+            }
+        }
+        free_blocks[off] = size;
+    }
+
+    bool contains(const void* p) const {
+        const char* c = static_cast<const char*>(p);
+        return ok && c >= host_base && c < host_base + capacity;
+    }
+
+    bool find(const void* p, ArenaBlock* out) {
+        std::lock_guard<std::mutex> g(mu);
+        if (!contains(p)) return false;
+        size_t off = static_cast<const char*>(p) - host_base;
+        auto it = live.upper_bound(off);
+        if (it == live.begin()) return false;
+        --it;
+        if (off >= it->first + it->second.size) return false;
+        if (out) *out = it->second;
+        return true;
+    }
+
+    bool set_residency(const void* p, int mode) {
+        std::lock_guard<std::mutex> g(mu);
+        if (!contains(p)) return false;
+        size_t off = static_cast<const char*>(p) - host_base;
+        auto it = live.upper_bound(off);
+        if (it == live.begin()) return false;
+        --it;
+        if (off >= it->first + it->second.size) return false;
+        it->second.residency = mode;
+        return true;
+    }
+};
+
+Arena& arena() {
+    static Arena* a = new Arena();  // never destroyed: outlives late users at exit
+    return *a;
+}
+
+}  // namespace
+
+bool arena_contains(const void* p) { return arena().contains(p); }
+bool arena_find(const void* p, ArenaBlock* out) { return arena().find(p, out); }
+void* arena_dev(const void* p) {
+    Arena& a = arena();
+    if (!a.contains(p)) return nullptr;
+    return reinterpret_cast<void*>(a.dev_base + (static_cast<const char*>(p) - a.host_base));
+}
+uint64_t arena_host_base() { return reinterpret_cast<uint64_t>(arena().host_base); }
+uint64_t arena_dev_base() { return static_cast<uint64_t>(arena().dev_base); }
+uint64_t arena_mapped_bytes() {
+    Arena& a = arena();
+    std::lock_guard<std::mutex> g(a.mu);
+    return a.mapped;
+}
+
+bool arena_sync_coherent(Workspace& ws, bool to_device) {
+    Arena& a = arena();
+    std::vector<std::pair<size_t, size_t>> ranges;  // [begin, end) offsets
+    {
+        std::lock_guard<std::mutex> g(a.mu);
+        if (!a.ok) return true;
+        for (const auto& kv : a.live) {
+            const ArenaBlock& b = kv.second;
+            if (b.residency != PARALLAX_COHERENT) continue;
+            if (!ranges.empty() && ranges.back().second == b.offset) ranges.back().second += b.size;
+            else ranges.emplace_back(b.offset, b.offset + b.size);
+        }
+    }
+    for (const auto& r : ranges) {
+        char* h = a.host_base + r.first;
+        char* d = reinterpret_cast<char*>(a.dev_base) + r.first;
+        size_t bytes = r.second - r.first;
+        cudaError_t e = to_device
+            ? cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ws.stream())
+            : cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ws.stream());
+        if (!cuda_ok(e, "arena coherent sync")) return false;
+    }
+    return true;
+}
+
+}  // namespace pxb
+
+using namespace pxb;
+
+PXB_EXPORT void* parallax_arena_alloc(size_t size, size_t align) {
+    void* p = arena().allocate(size, align ? align : 16);
+    if (getenv("PARALLAX_DEBUG"))
+        fprintf(stderr, "[parallax_arena_alloc] %zu bytes -> %p\n", size, p);
+    return p;
+}
+PXB_EXPORT void parallax_arena_free(void* ptr) { arena().deallocate(ptr); }
+PXB_EXPORT int parallax_arena_contains(const void* ptr) {
+    Arena& a = arena();
+    if (!a.ok) {
+        std::lock_guard<std::mutex> g(a.mu);
+        a.init();
+    }
+    return ptr && a.contains(ptr) ? 1 : 0;
+}
+PXB_EXPORT int parallax_heap_contains(const void*) { return 0; }
+
+PXB_EXPORT void* parallax_umalloc(size_t size, unsigned) { return parallax_arena_alloc(size, 256); }
+PXB_EXPORT void parallax_ufree(void* ptr) { parallax_arena_free(ptr); }
+
+PXB_EXPORT int parallax_arena_set_residency(void* ptr, int mode) {
+    if (mode != PARALLAX_COHERENT && mode != PARALLAX_DEVICE_RESIDENT)
+        return PARALLAX_ERR_INVALID_ARGUMENT;
+    return arena().set_residency(ptr, mode) ? PARALLAX_OK : PARALLAX_ERR_INVALID_ARGUMENT;
+}
+PXB_EXPORT int parallax_arena_get_residency(const void* ptr) {
+    ArenaBlock b;
+    return arena().find(ptr, &b) ? b.residency : -1;
+}
+PXB_EXPORT void* parallax_arena_device_ptr(const void* host_ptr) { return arena_dev(host_ptr); }
+PXB_EXPORT void parallax_arena_bases(uint64_t* host_base, uint64_t* dev_base) {
+    Arena& a = arena();
+    {
+        std::lock_guard<std::mutex> g(a.mu);
+        a.init();
+    }
+    if (host_base) *host_base = reinterpret_cast<uint64_t>(a.host_base);
+    if (dev_base) *dev_base = static_cast<uint64_t>(a.dev_base);
+}
+PXB_EXPORT size_t parallax_arena_capacity(void) {
+    Arena& a = arena();
+    std::lock_guard<std::mutex> g(a.mu);
+    a.init();
+    return a.capacity;
+}
+PXB_EXPORT size_t parallax_arena_used(void) {
+    Arena& a = arena();
+    std::lock_guard<std::mutex> g(a.mu);
+    return a.used;
+}
+PXB_EXPORT size_t parallax_arena_mapped(void) {
+    Arena& a = arena();
+    std::lock_guard<std::mutex> g(a.mu);
+    return a.mapped;
+}
+
+static int arena_copy(const void* ptr, size_t bytes, bool to_device) {
+    Workspace* ws = workspace();
+    if (!ws) return PARALLAX_ERR_NO_DEVICE;
+    ArenaBlock b;
+    if (!arena().find(ptr, &b)) return PARALLAX_ERR_INVALID_ARGUMENT;
+    size_t off = static_cast<const char*>(ptr) - arena().host_base;
+    if (off + bytes > b.offset + b.size) return PARALLAX_ERR_INVALID_ARGUMENT;
+    void* dev = arena_dev(ptr);
+    cudaError_t e = to_device
+        ? cudaMemcpyAsync(dev, ptr, bytes, cudaMemcpyHostToDevice, ws->stream())
+        : cudaMemcpyAsync(const_cast<void*>(ptr), dev, bytes, cudaMemcpyDeviceToHost,
+                          ws->stream());
+    if (!cuda_ok(e, "arena sync copy")) return PARALLAX_ERR_CUDA;
+    return ws->async ? PARALLAX_OK : sync_stream(*ws);
+}
+PXB_EXPORT int parallax_arena_sync_to_device(const void* ptr, size_t bytes) {
+    return arena_copy(ptr, bytes, true);
+}
+PXB_EXPORT int parallax_arena_sync_to_host(void* ptr, size_t bytes) {
+    return arena_copy(ptr, bytes, false);
+}

@@ -1,0 +1,289 @@
+// Device context, per-thread workspaces, error reporting and bounded host waits.
+//
+// Replaces the reference's Vulkan backend + single command buffer/fence
+// (src/backend/vulkan/device.cpp:14-43, src/kernel/kernel_launcher.cpp:54-100,
+// :438-443): one CUDA device, one non-blocking stream per submitting host thread, and
+// host waits that poll an event against a deadline instead of waiting forever.
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <unistd.h>
+
+#include <chrono>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "runtime.hpp"
+
+namespace pxb {
+
+// ---- errors ------------------------------------------------------------------------------
+static thread_local int tls_status = 0;
+
+static bool debug_enabled() {
+    static const bool on = getenv("PARALLAX_DEBUG") != nullptr;
+    return on;
+}
+
+void set_error(int status, const char* fmt, ...) {
+    tls_status = status;
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    fprintf(stderr, "[parallax] %s\n", buf);
+}
+void set_ok() { tls_status = 0; }
+int last_error() { return tls_status; }
+
+bool cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(PARALLAX_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return false;
+}
+
+// ---- device ------------------------------------------------------------------------------
+static DeviceInfo g_dev;
+static std::once_flag g_dev_once;
+static bool g_dev_ok = false;
+static std::atomic<uint64_t> g_launches{0};
+
+bool ensure_device() {
+    std::call_once(g_dev_once, [] {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            return;
+        }
+        int dev = 0;
+        if (const char* e = getenv("PARALLAX_DEVICE")) dev = atoi(e);
+        if (dev < 0 || dev >= n) dev = 0;
+        if (cudaSetDevice(dev) != cudaSuccess) return;
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return;
+        g_dev.device = dev;
+        g_dev.sm_count = prop.multiProcessorCount;
+        g_dev.max_threads_per_sm = prop.maxThreadsPerMultiProcessor;
+        g_dev.smem_per_sm = prop.sharedMemPerMultiprocessor;
+        snprintf(g_dev.name, sizeof g_dev.name, "%s", prop.name);
+        g_dev_ok = true;
+        if (debug_enabled())
+            fprintf(stderr, "[parallax] device %d: %s, %d SMs, cc %d.%d\n", dev, prop.name,
+                    prop.multiProcessorCount, prop.major, prop.minor);
+    });
+    if (g_dev_ok) cudaSetDevice(g_dev.device);  // per-thread current device
+    return g_dev_ok;
+}
+const DeviceInfo& device_info() { return g_dev; }
+void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+// ---- workspaces ------------------------------------------------------------------------------
+// Workspaces are owned by a global list and never destroyed before process exit: a
+// thread that exits leaves its (idle) stream and scratch behind, which keeps teardown
+// order trivial for a library loaded into arbitrary host programs.
+static std::mutex g_ws_mu;
+static std::vector<Workspace*>* g_ws_list = nullptr;
+static thread_local Workspace* tls_ws = nullptr;
+
+Workspace* workspace() {
+    if (tls_ws) return tls_ws;
+    if (!ensure_device()) {
+        set_error(PARALLAX_ERR_NO_DEVICE, "no CUDA device available");
+        return nullptr;
+    }
+    auto* ws = new Workspace();
+    if (!cuda_ok(cudaStreamCreateWithFlags(&ws->own_stream, cudaStreamNonBlocking),
+                 "cudaStreamCreate") ||
+        !cuda_ok(cudaHostAlloc((void**)&ws->h_slot, sizeof(HostSlot), cudaHostAllocMapped),
+                 "cudaHostAlloc(slot)") ||
+        !cuda_ok(cudaHostGetDevicePointer((void**)&ws->d_slot, ws->h_slot, 0),
+                 "cudaHostGetDevicePointer") ||
+        !cuda_ok(cudaEventCreateWithFlags(&ws->done, cudaEventDisableTiming),
+                 "cudaEventCreate")) {
+        delete ws;
+        return nullptr;
+    }
+    memset(ws->h_slot, 0, sizeof(HostSlot));
+    {
+        std::lock_guard<std::mutex> g(g_ws_mu);
+        if (!g_ws_list) g_ws_list = new std::vector<Workspace*>();
+        g_ws_list->push_back(ws);
+    }
+    tls_ws = ws;
+    return ws;
+}
+
+// Bytes of one look-back status entry (lookback.cuh): {u32 flag, u32 pad, u64 agg,
+// u64 inc} for every accumulator type, so flag words sit at the same addresses in every
+// launch.
+static constexpr size_t kStatusEntry = 24;
+
+char* Workspace::scratch(uint64_t tiles) {
+    size_t bytes = kScratchSmall + tiles * kStatusEntry;
+    if (bytes <= scratch_cap) return static_cast<char*>(d_scratch);
+    // Growth: earlier launches on this stream may still use the old buffer.
+    cudaStream_t s = stream();
+    if (d_scratch) {
+        if (!cuda_ok(cudaStreamSynchronize(s), "scratch sync")) return nullptr;
+        cudaFree(d_scratch);
+        d_scratch = nullptr;
+        scratch_cap = 0;
+    }
+    size_t cap = 1 << 20;
+    while (cap < bytes) cap <<= 1;
+    if (!cuda_ok(cudaMalloc(&d_scratch, cap), "cudaMalloc(scratch)")) return nullptr;
+    // Zero once: look-back status words then read as "not ready" for every epoch, and
+    // the self-resetting ticket counters start at zero.
+    if (!cuda_ok(cudaMemsetAsync(d_scratch, 0, cap, s), "cudaMemset(scratch)")) return nullptr;
+    scratch_cap = cap;
+    epoch = 1;
+    return static_cast<char*>(d_scratch);
+}
+
+void* Workspace::temp(size_t bytes) {
+    if (bytes <= temp_cap) return d_temp;
+    cudaStream_t s = stream();
+    if (d_temp) {
+        if (!cuda_ok(cudaStreamSynchronize(s), "temp sync")) return nullptr;
+        cudaFree(d_temp);
+        d_temp = nullptr;
+        temp_cap = 0;
+    }
+    size_t cap = 1 << 20;
+    while (cap < bytes) cap <<= 1;
+    if (!cuda_ok(cudaMalloc(&d_temp, cap), "cudaMalloc(temp)")) return nullptr;
+    temp_cap = cap;
+    return d_temp;
+}
+
+void* Workspace::stage(int slot, size_t bytes) {
+    if (bytes <= stage_cap[slot]) return d_stage[slot];
+    cudaStream_t s = stream();
+    if (d_stage[slot]) {
+        if (!cuda_ok(cudaStreamSynchronize(s), "stage sync")) return nullptr;
+        cudaFree(d_stage[slot]);
+        d_stage[slot] = nullptr;
+        stage_cap[slot] = 0;
+    }
+    size_t cap = 1 << 20;
+    while (cap < bytes) cap <<= 1;
+    if (!cuda_ok(cudaMalloc(&d_stage[slot], cap), "cudaMalloc(stage)")) return nullptr;
+    stage_cap[slot] = cap;
+    return d_stage[slot];
+}
+
+uint32_t Workspace::next_epoch() {
+    // 30 bits of epoch sit above a 2-bit state in each status word. On wrap-around the
+    // scratch is cleared so no stale word can alias a reused epoch.
+    uint32_t e = epoch++;
+    if (epoch >= (1u << 30)) {
+        cudaMemsetAsync(d_scratch, 0, scratch_cap, stream());
+        epoch = 1;
+        e = epoch++;
+    }
+    return e;
+}
+
+static long sync_timeout_ms() {
+    static const long v = [] {
+        const char* e = getenv("PARALLAX_SYNC_TIMEOUT_MS");
+        long t = e ? atol(e) : 120000;
+        return t > 0 ? t : 120000;
+    }();
+    return v;
+}
+
+int sync_stream(Workspace& ws) {
+    cudaStream_t s = ws.stream();
+    if (!cuda_ok(cudaEventRecord(ws.done, s), "cudaEventRecord")) return PARALLAX_ERR_CUDA;
+    auto t0 = std::chrono::steady_clock::now();
+    const long limit = sync_timeout_ms();
+    unsigned spins = 0;
+    for (;;) {
+        cudaError_t q = cudaEventQuery(ws.done);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) {
+            cuda_ok(q, "kernel execution");
+            return PARALLAX_ERR_CUDA;
+        }
+        // Spin briefly for low latency, then back off to avoid burning a core.
+        if (++spins > 2000) {
+            std::this_thread::sleep_for(std::chrono::microseconds(spins > 20000 ? 200 : 20));
+            auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                          std::chrono::steady_clock::now() - t0)
+                          .count();
+            if (ms > limit) {
+                set_error(PARALLAX_ERR_TIMEOUT, "device work did not finish within %ld ms",
+                          limit);
+                return PARALLAX_ERR_TIMEOUT;
+            }
+        }
+    }
+    if (ws.h_slot->spin_error) {
+        int code = ws.h_slot->spin_error;
+        ws.h_slot->spin_error = 0;
+        set_error(PARALLAX_ERR_DEVICE_SPIN, "an in-kernel bounded wait gave up (code %d)", code);
+        return PARALLAX_ERR_DEVICE_SPIN;
+    }
+    return PARALLAX_OK;
+}
+
+}  // namespace pxb
+
+// ---- exported: errors / streams / instrumentation ---------------------------------------------
+using namespace pxb;
+
+PXB_EXPORT int parallax_last_error(void) { return last_error(); }
+PXB_EXPORT void parallax_clear_error(void) { set_ok(); }
+PXB_EXPORT const char* parallax_error_string(int status) {
+    switch (status) {
+        case PARALLAX_OK: return "ok";
+        case PARALLAX_ERR_INVALID_HANDLE: return "invalid kernel handle";
+        case PARALLAX_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case PARALLAX_ERR_OUT_OF_MEMORY: return "out of memory";
+        case PARALLAX_ERR_CUDA: return "CUDA error";
+        case PARALLAX_ERR_TIMEOUT: return "host wait deadline passed";
+        case PARALLAX_ERR_DEVICE_SPIN: return "in-kernel bounded wait gave up";
+        case PARALLAX_ERR_UNSUPPORTED: return "unsupported";
+        case PARALLAX_ERR_NO_DEVICE: return "no CUDA device";
+        case PARALLAX_ERR_SHUTDOWN: return "runtime shut down";
+        default: return "unknown status";
+    }
+}
+
+PXB_EXPORT int parallax_set_stream(void* cuda_stream) {
+    Workspace* ws = workspace();
+    if (!ws) return PARALLAX_ERR_NO_DEVICE;
+    ws->user_stream = static_cast<cudaStream_t>(cuda_stream);
+    return PARALLAX_OK;
+}
+PXB_EXPORT int parallax_set_async(int async) {
+    Workspace* ws = workspace();
+    if (!ws) return PARALLAX_ERR_NO_DEVICE;
+    ws->async = async != 0;
+    return PARALLAX_OK;
+}
+PXB_EXPORT int parallax_synchronize(void) {
+    Workspace* ws = workspace();
+    if (!ws) return PARALLAX_ERR_NO_DEVICE;
+    int st = sync_stream(*ws);
+    if (st == PARALLAX_OK) ws->last_count = ws->h_slot->count[0];
+    return st;
+}
+PXB_EXPORT size_t parallax_last_count(void) {
+    Workspace* ws = workspace();
+    return ws ? ws->last_count : 0;
+}
+PXB_EXPORT uint64_t parallax_launch_count(void) { return launch_count(); }
+PXB_EXPORT int parallax_device_info(int* device, int* sm_count, char* name, size_t name_cap) {
+    if (!ensure_device()) return PARALLAX_ERR_NO_DEVICE;
+    if (device) *device = g_dev.device;
+    if (sm_count) *sm_count = g_dev.sm_count;
+    if (name && name_cap) snprintf(name, name_cap, "%s", g_dev.name);
+    return PARALLAX_OK;
+}

@@ -1,0 +1,309 @@
+// Ascending sort: bitonic tile sort in registers / shuffles / shared memory, then
+// merge-path merge passes over HBM.
+//
+// Reference: a global bitonic network, one dispatch + fence wait per (k, j) stage,
+// log2(n)(log2(n)+1)/2 passes over the whole array (351 at n = 2^26), n a power of two
+// (src/kernel/kernel_launcher.cpp:1568-1606, shaders/bitonic.comp:15-29).
+//
+// Here the same compare-exchange network runs only inside 16 KiB tiles (4096 4-byte or
+// 2048 8-byte keys per 256-thread CTA): stages whose partner distance j is below the
+// per-thread run use registers, j up to 32 runs uses warp shuffles, larger j goes through
+// shared memory. Sorted tiles are then merged pairwise, doubling the run length each
+// pass, with a merge-path split per 16 KiB output tile (one warp per split, 32-ary
+// search) and a stable in-shared-memory merge. Any n is accepted (the last tile is padded
+// with the largest key in registers only).
+// Keys are sorted as unsigned integers after an order-preserving transform: signed
+// integers flip the sign bit; IEEE floats flip all bits when negative and the sign bit
+// otherwise (the IEEE total order: -0.0 sorts before +0.0). The transform is fused into
+// the first load and its inverse into the last store. 8-byte records of the key-value
+// sort are (key << 32 | value) and sort as plain 64-bit keys, i.e. stably by key.
+#include <stdint.h>
+
+#include "../runtime.hpp"
+
+namespace pxb {
+namespace {
+
+constexpr int kBlock = 256;
+
+template <typename K> struct SortShape;
+template <> struct SortShape<uint32_t> { static constexpr int ITEMS = 16; };
+template <> struct SortShape<uint64_t> { static constexpr int ITEMS = 8; };
+
+// XF: 0 unsigned (identity), 1 signed integer, 2 IEEE float
+template <typename K, int XF>
+__device__ __forceinline__ K to_key(K b) {
+    constexpr K sign = K(1) << (sizeof(K) * 8 - 1);
+    if constexpr (XF == 1) return b ^ sign;
+    if constexpr (XF == 2) return (b & sign) ? ~b : (b | sign);
+    return b;
+}
+template <typename K, int XF>
+__device__ __forceinline__ K from_key(K k) {
+    constexpr K sign = K(1) << (sizeof(K) * 8 - 1);
+    if constexpr (XF == 1) return k ^ sign;
+    if constexpr (XF == 2) return (k & sign) ? (k ^ sign) : ~k;
+    return k;
+}
+
+template <typename K>
+__device__ __forceinline__ K kmin(K a, K b) { return b < a ? b : a; }
+template <typename K>
+__device__ __forceinline__ K kmax(K a, K b) { return b < a ? a : b; }
+
+// ---- bitonic network, unrolled at compile time -------------------------------------------
+// Thread t holds keys [t*ITEMS, t*ITEMS + ITEMS) of the tile in x[]. Stage (k, j) pairs
+// element i with i ^ j, ascending when (i & k) == 0.
+template <typename K, int ITEMS, int k, int j>
+__device__ __forceinline__ void bitonic_stage(K (&x)[ITEMS], K* sm, int t, int lane, int row0) {
+    if constexpr (j < ITEMS) {  // partner in the same thread
+#pragma unroll
+        for (int r = 0; r < ITEMS; ++r) {
+            if (r & j) continue;
+            const int r2 = r | j;
+            const bool asc = (k < ITEMS) ? ((r & k) == 0) : ((row0 & k) == 0);
+            const K a = x[r], b = x[r2];
+            const K lo = kmin(a, b), hi = kmax(a, b);
+            x[r] = asc ? lo : hi;
+            x[r2] = asc ? hi : lo;
+        }
+    } else if constexpr (j < 32 * ITEMS) {  // partner in the same warp
+        constexpr int m = j / ITEMS;
+        const bool keep_min = ((lane & m) == 0) == ((row0 & k) == 0);
+#pragma unroll
+        for (int r = 0; r < ITEMS; ++r) {
+            const K o = __shfl_xor_sync(0xffffffffu, x[r], m);
+            x[r] = keep_min ? kmin(x[r], o) : kmax(x[r], o);
+        }
+    } else {  // partner in another warp: exchange through shared memory
+        constexpr int m = j / ITEMS;
+        const bool keep_min = ((t & m) == 0) == ((row0 & k) == 0);
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < ITEMS; ++r) sm[r * kBlock + t] = x[r];
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < ITEMS; ++r) {
+            const K o = sm[r * kBlock + (t ^ m)];
+            x[r] = keep_min ? kmin(x[r], o) : kmax(x[r], o);
+        }
+    }
+}
+template <typename K, int ITEMS, int k, int j>
+__device__ __forceinline__ void bitonic_j(K (&x)[ITEMS], K* sm, int t, int lane, int row0) {
+    bitonic_stage<K, ITEMS, k, j>(x, sm, t, lane, row0);
+    if constexpr (j > 1) bitonic_j<K, ITEMS, k, j / 2>(x, sm, t, lane, row0);
+}
+template <typename K, int ITEMS, int TILE, int k>
+__device__ __forceinline__ void bitonic_k(K (&x)[ITEMS], K* sm, int t, int lane, int row0) {
+    bitonic_j<K, ITEMS, k, k / 2>(x, sm, t, lane, row0);
+    if constexpr (k < TILE) bitonic_k<K, ITEMS, TILE, k * 2>(x, sm, t, lane, row0);
+}
+
+// ---- tile sort ----------------------------------------------------------------------------
+template <typename K, int XF>
+__global__ void __launch_bounds__(kBlock)
+k_tile_sort(const K* in, K* out, uint64_t n, bool apply_inverse) {
+    constexpr int ITEMS = SortShape<K>::ITEMS;
+    constexpr int TILE = kBlock * ITEMS;
+    constexpr int V = 16 / sizeof(K);
+    __shared__ K sm[TILE];
+    const int t = threadIdx.x, lane = t & 31;
+    const uint64_t base = (uint64_t)blockIdx.x * TILE;
+    const uint64_t rem = n - base;
+    const int cnt = rem < (uint64_t)TILE ? (int)rem : TILE;
+    const int row0 = t * ITEMS;
+
+    K x[ITEMS];
+    const bool full = cnt == TILE && (reinterpret_cast<uintptr_t>(in) % 16 == 0);
+    if (full) {
+        const uint4* src = reinterpret_cast<const uint4*>(in + base + row0);
+#pragma unroll
+        for (int v = 0; v < ITEMS / V; ++v) {
+            uint4 r = src[v];
+            const K* e = reinterpret_cast<const K*>(&r);
+#pragma unroll
+            for (int k = 0; k < V; ++k) x[v * V + k] = to_key<K, XF>(e[k]);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < ITEMS; ++r)
+            x[r] = row0 + r < cnt ? to_key<K, XF>(in[base + row0 + r]) : ~K(0);
+    }
+
+    bitonic_k<K, ITEMS, TILE, 2>(x, sm, t, lane, row0);
+
+    if (full && (reinterpret_cast<uintptr_t>(out) % 16 == 0)) {
+        uint4* dst = reinterpret_cast<uint4*>(out + base + row0);
+#pragma unroll
+        for (int v = 0; v < ITEMS / V; ++v) {
+            uint4 r;
+            K* e = reinterpret_cast<K*>(&r);
+#pragma unroll
+            for (int k = 0; k < V; ++k)
+                e[k] = apply_inverse ? from_key<K, XF>(x[v * V + k]) : x[v * V + k];
+            dst[v] = r;
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < ITEMS; ++r)
+            if (row0 + r < cnt)
+                out[base + row0 + r] = apply_inverse ? from_key<K, XF>(x[r]) : x[r];
+    }
+}
+
+// ---- merge path ---------------------------------------------------------------------------
+// Pair geometry of output tile `o`: runs A = [ps, ps+la) and B = [ps+la, ps+la+lb).
+struct Pair {
+    uint64_t ps, la, lb;
+};
+__device__ __forceinline__ Pair pair_of(uint64_t o, uint64_t n, uint64_t L) {
+    Pair p;
+    p.ps = o / (2 * L) * (2 * L);
+    const uint64_t r = n - p.ps;
+    p.la = r < L ? r : L;
+    const uint64_t r2 = r - p.la;
+    p.lb = r2 < L ? r2 : L;
+    return p;
+}
+
+// One warp per output tile: number of A elements among the first d outputs of the
+// stable merge (A wins ties): the first i with !(A[i] <= B[d-1-i]).
+template <typename K>
+__global__ void __launch_bounds__(kBlock)
+k_merge_path(const K* __restrict__ src, uint64_t n, uint64_t L, uint64_t OT, uint64_t tiles,
+             uint64_t* __restrict__ splits) {
+    const uint64_t tile = ((uint64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (tile >= tiles) return;
+    const uint64_t o = tile * OT;
+    const Pair p = pair_of(o, n, L);
+    const uint64_t d = o - p.ps;
+    const K* A = src + p.ps;
+    const K* B = src + p.ps + p.la;
+    uint64_t lo = d > p.lb ? d - p.lb : 0;
+    uint64_t hi = d < p.la ? d : p.la;
+    while (hi - lo > 32) {
+        const uint64_t stride = (hi - lo + 31) / 32;
+        const uint64_t q = lo + (uint64_t)lane * stride;
+        const bool valid = q < hi;
+        const bool tr = valid && !(B[d - 1 - q] < A[q]);
+        const int c = __popc(__ballot_sync(0xffffffffu, tr));
+        const int nvalid = __popc(__ballot_sync(0xffffffffu, valid));
+        const uint64_t nlo = c ? lo + (uint64_t)(c - 1) * stride + 1 : lo;
+        const uint64_t nhi = c < nvalid ? lo + (uint64_t)c * stride : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    const uint64_t q = lo + lane;
+    const bool tr = q < hi && !(B[d - 1 - q] < A[q]);
+    const int c = __popc(__ballot_sync(0xffffffffu, tr));
+    if (lane == 0) splits[tile] = lo + c;
+}
+
+template <typename K, int XF, bool FINAL>
+__global__ void __launch_bounds__(kBlock)
+k_merge(const K* __restrict__ src, K* __restrict__ dst, uint64_t n, uint64_t L,
+        const uint64_t* __restrict__ splits) {
+    constexpr int IPT = SortShape<K>::ITEMS;
+    constexpr int OT = kBlock * IPT;
+    __shared__ K sm[OT];
+    __shared__ K so[IPT * (kBlock + 1)];
+    const int t = threadIdx.x;
+    const uint64_t o = (uint64_t)blockIdx.x * OT;
+    const Pair p = pair_of(o, n, L);
+    const uint64_t pair_end = p.ps + p.la + p.lb;
+    const uint64_t tile_end = o + OT < pair_end ? o + OT : pair_end;
+    const uint64_t d0 = o - p.ps, d1 = tile_end - p.ps;
+    const uint64_t a_s = splits[blockIdx.x];
+    const uint64_t a_e = o + OT < pair_end ? splits[blockIdx.x + 1] : p.la;
+    const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
+    const int na = (int)(a_e - a_s), nb = (int)(b_e - b_s);
+    const int total = na + nb;
+    const K* A = src + p.ps + a_s;
+    const K* B = src + p.ps + p.la + b_s;
+    for (int e = t; e < na; e += kBlock) sm[e] = A[e];
+    for (int e = t; e < nb; e += kBlock) sm[na + e] = B[e];
+    __syncthreads();
+
+    const int dt = t * IPT < total ? t * IPT : total;
+    int lo = dt > nb ? dt - nb : 0, hi = dt < na ? dt : na;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (!(sm[na + dt - 1 - mid] < sm[mid])) lo = mid + 1;
+        else hi = mid;
+    }
+    int i = lo, j = dt - lo;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        if (dt + k < total) {
+            bool take_a;
+            if (i >= na) take_a = false;
+            else if (j >= nb) take_a = true;
+            else take_a = !(sm[na + j] < sm[i]);
+            const K v = take_a ? sm[i++] : sm[na + j++];
+            so[k * (kBlock + 1) + t] = v;
+        }
+    }
+    __syncthreads();
+    for (int e = t; e < total; e += kBlock) {
+        const K v = so[(e % IPT) * (kBlock + 1) + e / IPT];
+        dst[o + e] = FINAL ? from_key<K, XF>(v) : v;
+    }
+}
+
+template <typename K, int XF>
+bool sort_keys(Workspace& ws, void* d_data, uint64_t n) {
+    constexpr int TILE = kBlock * SortShape<K>::ITEMS;
+    const uint64_t tiles = (n + TILE - 1) / TILE;
+    if (tiles > 0x7fffffffull) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "sort: too many elements");
+        return false;
+    }
+    int passes = 0;
+    while ((uint64_t(1) << passes) < tiles) ++passes;
+    K* data = static_cast<K*>(d_data);
+    K* tmp = nullptr;
+    uint64_t* splits = nullptr;
+    if (passes) {
+        const size_t key_bytes = (n * sizeof(K) + 255) / 256 * 256;
+        char* t = static_cast<char*>(ws.temp(key_bytes + (tiles + 1) * sizeof(uint64_t)));
+        if (!t) return false;
+        tmp = reinterpret_cast<K*>(t);
+        splits = reinterpret_cast<uint64_t*>(t + key_bytes);
+    }
+    cudaStream_t s = ws.stream();
+    K* cur = (passes % 2 == 0) ? data : tmp;
+    k_tile_sort<K, XF><<<(unsigned)tiles, kBlock, 0, s>>>(data, cur, n, passes == 0);
+    count_launch();
+    for (int pass = 1; pass <= passes; ++pass) {
+        const uint64_t L = (uint64_t)TILE << (pass - 1);
+        K* nxt = cur == data ? tmp : data;
+        const unsigned search_blocks = (unsigned)((tiles * 32 + kBlock - 1) / kBlock);
+        k_merge_path<K><<<search_blocks, kBlock, 0, s>>>(cur, n, L, TILE, tiles, splits);
+        if (pass == passes) k_merge<K, XF, true><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, splits);
+        else k_merge<K, XF, false><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, splits);
+        count_launch(2);
+        cur = nxt;
+    }
+    return cuda_ok(cudaGetLastError(), "sort launch");
+}
+
+}  // namespace
+
+bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
+    if (n <= 1) return true;
+    switch (t) {
+        case DType::U32: return sort_keys<uint32_t, 0>(ws, d_data, n);
+        case DType::I32: return sort_keys<uint32_t, 1>(ws, d_data, n);
+        case DType::F32: return sort_keys<uint32_t, 2>(ws, d_data, n);
+        case DType::U64: return sort_keys<uint64_t, 0>(ws, d_data, n);
+        case DType::I64: return sort_keys<uint64_t, 1>(ws, d_data, n);
+        case DType::F64: return sort_keys<uint64_t, 2>(ws, d_data, n);
+        default: break;
+    }
+    set_error(PARALLAX_ERR_INVALID_ARGUMENT, "sort: unsupported element type");
+    return false;
+}
+
+}  // namespace pxb

@@ -1,0 +1,128 @@
+// Decoupled look-back: the single-pass inter-tile carry shared by the scan and the
+// compaction kernels.
+//
+// Replaces the reference's multi-pass carry (per-block scan -> recursive scan of block
+// sums -> add-offsets pass, src/kernel/kernel_launcher.cpp:1280-1342,
+// shaders/scan.comp + scan_add.comp). Each tile publishes its aggregate as soon as it is
+// known (state AGG) and its inclusive prefix once its look-back completes (state INC).
+// A tile's look-back walks predecessors 32 at a time (one warp), summing aggregates until
+// it meets an inclusive prefix. Tiles are processed in blockIdx order, so every tile a
+// CTA waits on belongs to a CTA that was dispatched earlier: the waits always end.
+// Each wait is still bounded: after kSpinLimit polls the kernel records an error code in
+// host-visible memory and carries on with a zero contribution, so a fault can never
+// hang the GPU; the host turns the code into PARALLAX_ERR_DEVICE_SPIN.
+//
+// Status words: bits [31:2] = launch epoch (30 bits), bits [1:0] = state
+// (0 none, 1 AGG, 2 INC). Words left by earlier launches carry an older epoch and read as
+// "none", so the status array is never cleared between launches.
+#pragma once
+
+#include <string.h>
+
+#include "common.cuh"
+#include "runtime.hpp"
+
+namespace pxb {
+
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// One status entry per tile; the same 24-byte layout for every accumulator type keeps
+// flag words at fixed addresses across launches (see Workspace::scratch).
+struct StatusEntry {
+    uint32_t flag;
+    uint32_t pad;
+    uint64_t agg;
+    uint64_t inc;
+};
+static_assert(sizeof(StatusEntry) == 24, "status entry layout");
+
+template <typename A>
+struct TileStatus {
+    StatusEntry* e;
+    uint32_t epoch;
+    volatile int32_t* err;
+};
+
+template <typename A>
+__device__ __forceinline__ void put_val(uint64_t* p, A v) {
+    uint64_t bits = 0;
+    memcpy(&bits, &v, sizeof(A));
+    *p = bits;
+}
+template <typename A>
+__device__ __forceinline__ A get_val(const uint64_t* p) {
+    uint64_t bits = (uint64_t)__ldcg(reinterpret_cast<const unsigned long long*>(p));
+    A v;
+    memcpy(&v, &bits, sizeof(A));
+    return v;
+}
+
+// Must be called by all 32 lanes of exactly one warp of the CTA. Returns the exclusive
+// prefix (sum of aggregates of tiles 0..tile-1) in every lane.
+template <typename A>
+__device__ __forceinline__ A lookback(const TileStatus<A>& ts, uint64_t tile, A agg) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t ep = (ts.epoch & 0x3fffffffu) << 2;
+    if (tile == 0) {
+        if (lane == 0) {
+            put_val(&ts.e[0].inc, agg);
+            st_release_u32(&ts.e[0].flag, ep | 2u);
+        }
+        return A(0);
+    }
+    if (lane == 0) {
+        put_val(&ts.e[tile].agg, agg);
+        st_release_u32(&ts.e[tile].flag, ep | 1u);
+    }
+    A excl = A(0);
+    int64_t pred = (int64_t)tile - 1;
+    for (;;) {
+        const int64_t idx = pred - lane;
+        uint32_t state = 2u;
+        A v = A(0);
+        if (idx >= 0) {
+            uint32_t f = 0, spins = 0;
+            bool gave_up = false;
+            for (;;) {
+                f = ld_acquire_u32(&ts.e[idx].flag);
+                if ((f & ~3u) == ep && (f & 3u) != 0u) break;
+                if (++spins > kSpinLimit) {
+                    *ts.err = 1;
+                    gave_up = true;
+                    break;
+                }
+                if (spins > 16) nanosleep_ns(64);
+            }
+            if (gave_up) {
+                state = 2u;
+            } else {
+                state = f & 3u;
+                v = state == 2u ? get_val<A>(&ts.e[idx].inc) : get_val<A>(&ts.e[idx].agg);
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, state == 2u);
+        const int first = m ? __ffs(m) - 1 : 32;
+        A c = lane <= first ? v : A(0);
+        c = warp_reduce(c, OpSum());
+        excl = c + excl;
+        if (m) break;
+        pred -= 32;
+    }
+    if (lane == 0) {
+        put_val(&ts.e[tile].inc, excl + agg);
+        st_release_u32(&ts.e[tile].flag, ep | 2u);
+    }
+    return excl;
+}
+
+// Status entries live after the small scratch region.
+template <typename A>
+inline TileStatus<A> tile_status_at(char* scratch, uint32_t epoch, int32_t* err) {
+    TileStatus<A> ts;
+    ts.e = reinterpret_cast<StatusEntry*>(scratch + kScratchSmall);
+    ts.epoch = epoch;
+    ts.err = err;
+    return ts;
+}
+
+}  // namespace pxb

@@ -1,0 +1,200 @@
+// Internal host-side interfaces of the B200 parallax runtime: per-thread workspaces
+// (stream, device scratch, pinned result slot), the device-resident arena, kernel
+// handles, and the launchers of the sm_100a primitive kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include <atomic>
+#include <mutex>
+#include <string>
+
+#include "common.cuh"
+#include "parallax/runtime.h"
+#include "parallax/runtime_ext.h"
+
+#define PXB_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace pxb {
+
+// ---- errors ------------------------------------------------------------------------
+void set_error(int status, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+void set_ok();
+int last_error();
+bool cuda_ok(cudaError_t e, const char* what);  // records PARALLAX_ERR_CUDA on failure
+
+// ---- device context ------------------------------------------------------------------
+struct DeviceInfo {
+    int device = -1;
+    int sm_count = 0;
+    int max_threads_per_sm = 0;
+    size_t smem_per_sm = 0;
+    char name[256] = {0};
+};
+// Initializes the CUDA device once (PARALLAX_DEVICE, default 0). False when no device.
+bool ensure_device();
+const DeviceInfo& device_info();
+void count_launch(unsigned n = 1);
+uint64_t launch_count();
+
+// Pinned, device-mapped slot the kernels write small results into (reduce scalars,
+// kept counts, in-kernel wait-timeout codes) so a synchronous call needs no extra
+// device-to-host copy.
+struct HostSlot {
+    uint64_t result[4];     // up to 32 bytes of reduce / search results
+    uint64_t count[2];      // kept counts (copy_if / partition)
+    int32_t spin_error;     // nonzero when a bounded in-kernel wait gave up
+    int32_t pad[7];
+};
+
+// Offsets inside the small scratch region.
+constexpr size_t kScratchSmall = 64 << 10;
+struct ScratchOff {
+    static constexpr size_t ticket = 0;        // reduce last-block ticket (self-resetting)
+    static constexpr size_t num_true = 256;    // partition: count of the count pass
+    static constexpr size_t partials = 1024;   // reduce per-block partials (<= 48 KiB)
+};
+
+// Per-host-thread execution state. Every ABI call from a thread runs on that thread's
+// stream, so calls from different threads overlap on the device.
+struct Workspace {
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t user_stream = nullptr;   // parallax_set_stream override
+    bool async = false;
+    void* d_scratch = nullptr;            // grows on demand, zeroed on (re)allocation
+    size_t scratch_cap = 0;
+    uint32_t epoch = 1;                   // look-back flag epoch, see next_epoch()
+    HostSlot* h_slot = nullptr;
+    HostSlot* d_slot = nullptr;           // device alias of h_slot
+    size_t last_count = 0;
+    // staging for operands that are plain (pageable) host pointers
+    void* d_stage[3] = {nullptr, nullptr, nullptr};
+    size_t stage_cap[3] = {0, 0, 0};
+    cudaEvent_t done = nullptr;
+
+    void* d_temp = nullptr;               // bulk temporaries (sort ping-pong buffer)
+    size_t temp_cap = 0;
+
+    cudaStream_t stream() const { return user_stream ? user_stream : own_stream; }
+    // Device scratch with a fixed layout (zeroed whenever it is reallocated):
+    //   [0, kScratchSmall)   reduce tickets / partials / partition count (ScratchOff)
+    //   [kScratchSmall, ...) look-back status entries, `tiles` of them
+    // The regions never overlap, so a status word can only ever hold a status word.
+    char* scratch(uint64_t tiles);
+    void* temp(size_t bytes);
+    void* stage(int slot, size_t bytes);
+    // Look-back status words carry the launch epoch, so stale words from earlier
+    // launches read as "not ready" without clearing the array between launches.
+    uint32_t next_epoch();
+};
+Workspace* workspace();  // nullptr when the device is unavailable
+
+// Waits for all work on the thread's stream with a deadline (PARALLAX_SYNC_TIMEOUT_MS,
+// default 120000) and surfaces in-kernel wait timeouts. Returns a parallax_status.
+int sync_stream(Workspace& ws);
+
+// ---- arena ---------------------------------------------------------------------------
+struct ArenaBlock {
+    size_t offset = 0;
+    size_t size = 0;
+    int residency = 0;  // parallax_residency
+};
+bool arena_contains(const void* p);
+// Looks up the block containing p; false when p is not inside a live block.
+bool arena_find(const void* p, ArenaBlock* out);
+void* arena_dev(const void* host_p);  // relocation dev_base + (p - host_base)
+uint64_t arena_host_base();
+uint64_t arena_dev_base();
+uint64_t arena_mapped_bytes();  // bytes of the arena currently backed by device memory
+// Copies every PARALLAX_COHERENT block (merged into contiguous ranges) host -> device or
+// device -> host on the workspace stream. Kernels that dereference stored arena pointers
+// may touch any block, so they get the reference's whole-arena coherence
+// (src/memory/arena.cpp:296-304) restricted to blocks in coherent mode.
+bool arena_sync_coherent(Workspace& ws, bool to_device);
+
+// ---- operands --------------------------------------------------------------------------
+// How an ABI pointer reaches the device:
+//   ARENA_COHERENT  arena block; range uploaded before / downloaded after the call
+//   ARENA_RESIDENT  arena block in PARALLAX_DEVICE_RESIDENT mode; used in place
+//   DEVICE          a CUDA device (or managed) pointer; used in place
+//   HOST            any other host pointer; staged through device memory, results are
+//                   copied back (the reference never copies results back to such
+//                   pointers: src/memory/unified_buffer.cpp:126-136)
+enum class OperandKind { ARENA_COHERENT, ARENA_RESIDENT, DEVICE, HOST };
+struct Operand {
+    void* user = nullptr;
+    void* dev = nullptr;
+    size_t bytes = 0;
+    OperandKind kind = OperandKind::DEVICE;
+};
+// Resolves `p` and, when `upload`, enqueues the host-to-device copy. `stage_slot`
+// selects the workspace staging buffer used for HOST operands.
+bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int stage_slot,
+                     Operand* out);
+// Enqueues the device-to-host copy of the first `bytes` of a written operand.
+bool writeback_operand(Workspace& ws, const Operand& op, size_t bytes);
+
+// ---- kernel handles ----------------------------------------------------------------------
+enum class Kind : int {
+    NONE = 0,
+    REDUCE, SCAN, SCAN_ADD, EXSCAN_SHIFT, SORT, SORT_KV,
+    COMPACT_FLAGS,     // copy_if / remove_if predicate flags
+    UNIQUE_FLAGS,      // adjacent-difference flags
+    COMPACT_SCATTER,   // copy_if scatter
+    PARTITION_SCATTER, // partition scatter: writes every element
+    COUNT_IF, FIND, ARGMINMAX, MISMATCH,
+    MAP,               // built-in element-wise op
+    USER,              // sm_100a image loaded from a registered / loaded cubin
+};
+enum class RedOp : int { SUM = 0, MAX = 1, MIN = 2 };
+enum class PredKind : int { NONE = 0, GT, GE, LT, LE, EQ, NE, MOD, NONZERO, ODD_NONZERO };
+struct Pred {
+    PredKind kind = PredKind::NONE;
+    bool negate = false;   // remove_if keeps elements for which the predicate is false
+    double f = 0.0;        // operand for float element types
+    int64_t i = 0;         // operand for signed integer element types
+    uint64_t u = 0;        // operand for unsigned integer element types
+    int64_t mod_m = 1, mod_r = 0;
+};
+enum class MapOp : int { NONE = 0, SAXPY_GATHER_F32, AFFINE_F32, DOUBLE_PLUS_ONE_F32 };
+
+struct Handle {
+    Kind kind = Kind::NONE;
+    DType dtype = DType::INVALID;
+    RedOp op = RedOp::SUM;
+    Pred pred;
+    MapOp map = MapOp::NONE;
+    bool remove = false;      // remove_if flavour of COMPACT_FLAGS
+    // USER kernels
+    cudaLibrary_t library = nullptr;
+    cudaKernel_t kernel = nullptr;
+    std::string name;
+};
+Handle* as_handle(parallax_kernel_t k);
+Handle* builtin_handle(const char* spec);
+
+// ---- launchers (all asynchronous on `s`) -------------------------------------------------
+// Reduce: writes one element (type of dtype; sum of f32 is rounded from fp64) to d_out.
+bool launch_reduce(Workspace& ws, DType t, RedOp op, const void* d_in, size_t n, void* d_out);
+// Inclusive (init == nullptr) or exclusive scan; in-place allowed.
+bool launch_scan(Workspace& ws, DType t, bool exclusive, const void* d_in, void* d_out,
+                 size_t n, const void* init_host);
+enum class CompactMode : int { SELECT = 0, UNIQUE = 1, PARTITION = 2 };
+// Writes the kept count (uint64) to d_count.
+bool launch_compact(Workspace& ws, DType t, CompactMode mode, const Pred& p, const void* d_in,
+                    void* d_out, size_t n, uint64_t* d_count);
+bool launch_count_if(Workspace& ws, DType t, const Pred& p, const void* d_in, size_t n,
+                     uint64_t* d_count);
+bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n);
+bool launch_map(Workspace& ws, MapOp op, const void* d_in, void* d_out, size_t n,
+                const void* captures, size_t capture_size);
+bool launch_find(Workspace& ws, DType t, const Pred& p, const void* d_in, size_t n,
+                 uint64_t* d_index);
+bool launch_argminmax(Workspace& ws, DType t, bool want_max, bool want_last, const void* d_in,
+                      size_t n, uint64_t* d_index);
+bool launch_mismatch(Workspace& ws, DType t, const void* d_a, const void* d_b, size_t n,
+                     uint64_t* d_index);
+
+}  // namespace pxb
