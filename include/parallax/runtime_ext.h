@@ -90,6 +90,15 @@ size_t parallax_last_count(void);
 /* ---- instrumentation ------------------------------------------------------------- */
 /* Number of runtime kernel launches issued by this process so far. */
 uint64_t parallax_launch_count(void);
+/* Per-kernel device timing: when enabled, every runtime launch is bracketed with CUDA
+ * events on its stream (small overhead; off by default). parallax_profile_json waits for
+ * the recorded launches, folds them into per-kernel totals, writes
+ * {"kernel": {"launches", "ms", "alg_bytes"}} into buf and returns the full JSON length;
+ * totals accumulate until parallax_profile_reset(). alg_bytes is the launch's minimum HBM
+ * traffic (compaction kernels count their input only). */
+void parallax_profile_enable(int on);
+size_t parallax_profile_json(char* buf, size_t cap);
+void parallax_profile_reset(void);
 /* Device ordinal, SM count and device name; returns a parallax_status. */
 int parallax_device_info(int* device, int* sm_count, char* name, size_t name_cap);
 

@@ -84,6 +84,9 @@ _SIGNATURES = {
     "parallax_synchronize": (C.c_int, []),
     "parallax_last_count": (sz, []),
     "parallax_launch_count": (u64, []),
+    "parallax_profile_enable": (None, [C.c_int]),
+    "parallax_profile_json": (sz, [C.c_char_p, sz]),
+    "parallax_profile_reset": (None, []),
     "parallax_device_info": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p, sz]),
 }
 
@@ -140,6 +143,16 @@ def declared_functions() -> dict[str, list[str]]:
         names = re.findall(r"\b(parallax_[a-z0-9_]+)\s*\(", text)
         out[h.name] = sorted(set(names))
     return out
+
+
+def profile_json() -> dict:
+    """Per-kernel launches / device ms / algorithmic bytes recorded since the last call."""
+    import json
+    lib = load()
+    need = lib.parallax_profile_json(None, 0)
+    buf = C.create_string_buffer(need + 1)
+    lib.parallax_profile_json(buf, need + 1)
+    return json.loads(buf.value.decode() or "{}")
 
 
 def device_info() -> tuple[int, int, str]:

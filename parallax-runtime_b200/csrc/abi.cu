@@ -42,8 +42,7 @@ bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int slot
         out->kind = b.residency == PARALLAX_DEVICE_RESIDENT ? OperandKind::ARENA_RESIDENT
                                                             : OperandKind::ARENA_COHERENT;
         if (out->kind == OperandKind::ARENA_COHERENT && upload && bytes)
-            return cuda_ok(cudaMemcpyAsync(out->dev, p, bytes, cudaMemcpyHostToDevice, s),
-                           "operand upload");
+            return arena_copy_async(out->dev, p, bytes, true, s);
         return true;
     }
     cudaPointerAttributes attr;
@@ -70,7 +69,9 @@ bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int slot
 
 bool writeback_operand(Workspace& ws, const Operand& op, size_t bytes) {
     if (!bytes) return true;
-    if (op.kind == OperandKind::ARENA_COHERENT || op.kind == OperandKind::HOST)
+    if (op.kind == OperandKind::ARENA_COHERENT)
+        return arena_copy_async(op.user, op.dev, bytes, false, ws.stream());
+    if (op.kind == OperandKind::HOST)
         return cuda_ok(cudaMemcpyAsync(op.user, op.dev, bytes, cudaMemcpyDeviceToHost,
                                        ws.stream()),
                        "operand download");

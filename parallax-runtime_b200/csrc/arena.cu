@@ -268,6 +268,29 @@ uint64_t arena_mapped_bytes() {
     return a.mapped;
 }
 
+// The host mirror is page-locked chunk by chunk, and one copy may not span two
+// registrations, so arena copies are split at chunk boundaries (which are also the
+// boundaries of the device-side physical allocations).
+bool arena_copy_async(void* dst, const void* src, size_t bytes, bool to_device,
+                      cudaStream_t s) {
+    Arena& a = arena();
+    const char* h = static_cast<const char*>(to_device ? src : dst);
+    size_t off = static_cast<size_t>(h - a.host_base);
+    size_t done = 0;
+    while (done < bytes) {
+        size_t room = a.chunk - (off + done) % a.chunk;
+        size_t len = bytes - done < room ? bytes - done : room;
+        cudaError_t e = cudaMemcpyAsync(static_cast<char*>(dst) + done,
+                                        static_cast<const char*>(src) + done, len,
+                                        to_device ? cudaMemcpyHostToDevice
+                                                  : cudaMemcpyDeviceToHost,
+                                        s);
+        if (!cuda_ok(e, "arena copy")) return false;
+        done += len;
+    }
+    return true;
+}
+
 bool arena_sync_coherent(Workspace& ws, bool to_device) {
     Arena& a = arena();
     std::vector<std::pair<size_t, size_t>> ranges;  // [begin, end) offsets
@@ -285,10 +308,9 @@ bool arena_sync_coherent(Workspace& ws, bool to_device) {
         char* h = a.host_base + r.first;
         char* d = reinterpret_cast<char*>(a.dev_base) + r.first;
         size_t bytes = r.second - r.first;
-        cudaError_t e = to_device
-            ? cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ws.stream())
-            : cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ws.stream());
-        if (!cuda_ok(e, "arena coherent sync")) return false;
+        bool ok = to_device ? arena_copy_async(d, h, bytes, true, ws.stream())
+                            : arena_copy_async(h, d, bytes, false, ws.stream());
+        if (!ok) return false;
     }
     return true;
 }
@@ -361,11 +383,10 @@ static int arena_copy(const void* ptr, size_t bytes, bool to_device) {
     size_t off = static_cast<const char*>(ptr) - arena().host_base;
     if (off + bytes > b.offset + b.size) return PARALLAX_ERR_INVALID_ARGUMENT;
     void* dev = arena_dev(ptr);
-    cudaError_t e = to_device
-        ? cudaMemcpyAsync(dev, ptr, bytes, cudaMemcpyHostToDevice, ws->stream())
-        : cudaMemcpyAsync(const_cast<void*>(ptr), dev, bytes, cudaMemcpyDeviceToHost,
-                          ws->stream());
-    if (!cuda_ok(e, "arena sync copy")) return PARALLAX_ERR_CUDA;
+    bool ok = to_device ? arena_copy_async(dev, ptr, bytes, true, ws->stream())
+                        : arena_copy_async(const_cast<void*>(ptr), dev, bytes, false,
+                                           ws->stream());
+    if (!ok) return PARALLAX_ERR_CUDA;
     return ws->async ? PARALLAX_OK : sync_stream(*ws);
 }
 PXB_EXPORT int parallax_arena_sync_to_device(const void* ptr, size_t bytes) {

@@ -11,6 +11,7 @@
 #include <time.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
 #include <mutex>
 #include <thread>
@@ -189,6 +190,49 @@ uint32_t Workspace::next_epoch() {
     return e;
 }
 
+// ---- profiling -------------------------------------------------------------------------------
+namespace {
+struct ProfRecord {
+    const char* name;
+    uint64_t bytes;
+    cudaEvent_t start, stop;
+};
+std::atomic<bool> g_prof_on{false};
+std::mutex g_prof_mu;
+std::vector<ProfRecord>* g_prof = nullptr;
+std::vector<cudaEvent_t>* g_event_pool = nullptr;
+
+cudaEvent_t take_event() {
+    std::lock_guard<std::mutex> g(g_prof_mu);
+    if (!g_event_pool) g_event_pool = new std::vector<cudaEvent_t>();
+    if (!g_event_pool->empty()) {
+        cudaEvent_t e = g_event_pool->back();
+        g_event_pool->pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+}  // namespace
+
+ProfScope::ProfScope(Workspace& ws, const char* kernel, uint64_t alg_bytes) {
+    if (!g_prof_on.load(std::memory_order_relaxed)) return;
+    ws_ = &ws;
+    name_ = kernel;
+    bytes_ = alg_bytes;
+    start_ = take_event();
+    cudaEventRecord(start_, ws.stream());
+}
+ProfScope::~ProfScope() {
+    if (!ws_) return;
+    cudaEvent_t stop = take_event();
+    cudaEventRecord(stop, ws_->stream());
+    std::lock_guard<std::mutex> g(g_prof_mu);
+    if (!g_prof) g_prof = new std::vector<ProfRecord>();
+    g_prof->push_back({name_, bytes_, start_, stop});
+}
+
 static long sync_timeout_ms() {
     static const long v = [] {
         const char* e = getenv("PARALLAX_SYNC_TIMEOUT_MS");
@@ -280,6 +324,69 @@ PXB_EXPORT size_t parallax_last_count(void) {
     return ws ? ws->last_count : 0;
 }
 PXB_EXPORT uint64_t parallax_launch_count(void) { return launch_count(); }
+
+PXB_EXPORT void parallax_profile_enable(int on) { g_prof_on.store(on != 0); }
+
+namespace {
+struct ProfAgg {
+    uint64_t launches = 0, bytes = 0;
+    double ms = 0;
+};
+std::vector<std::pair<std::string, ProfAgg>> g_prof_aggs;  // guarded by g_prof_agg_mu
+std::mutex g_prof_agg_mu;
+}  // namespace
+
+PXB_EXPORT void parallax_profile_reset(void) {
+    std::lock_guard<std::mutex> g(g_prof_agg_mu);
+    g_prof_aggs.clear();
+}
+
+// Folds the launches recorded so far (waiting for them to finish) into per-kernel totals
+// and writes {"kernel": {"launches": L, "ms": T, "alg_bytes": B}, ...} into buf. Returns
+// the length the full JSON needs (excluding the terminator). Totals accumulate until
+// parallax_profile_reset().
+PXB_EXPORT size_t parallax_profile_json(char* buf, size_t cap) {
+    std::vector<ProfRecord> recs;
+    {
+        std::lock_guard<std::mutex> g(g_prof_mu);
+        if (g_prof) recs.swap(*g_prof);
+    }
+    std::lock_guard<std::mutex> ga(g_prof_agg_mu);
+    auto& aggs = g_prof_aggs;
+    for (auto& r : recs) {
+        cudaEventSynchronize(r.stop);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, r.start, r.stop);
+        auto it = std::find_if(aggs.begin(), aggs.end(),
+                               [&](const auto& a) { return a.first == r.name; });
+        if (it == aggs.end()) {
+            aggs.emplace_back(r.name, ProfAgg{});
+            it = aggs.end() - 1;
+        }
+        it->second.launches++;
+        it->second.bytes += r.bytes;
+        it->second.ms += ms;
+    }
+    {
+        std::lock_guard<std::mutex> g(g_prof_mu);
+        if (!g_event_pool) g_event_pool = new std::vector<cudaEvent_t>();
+        for (auto& r : recs) {
+            g_event_pool->push_back(r.start);
+            g_event_pool->push_back(r.stop);
+        }
+    }
+    std::string out = "{";
+    char tmp[256];
+    for (size_t i = 0; i < aggs.size(); ++i) {
+        snprintf(tmp, sizeof tmp, "%s\"%s\": {\"launches\": %llu, \"ms\": %.6f, \"alg_bytes\": %llu}",
+                 i ? ", " : "", aggs[i].first.c_str(), (unsigned long long)aggs[i].second.launches,
+                 aggs[i].second.ms, (unsigned long long)aggs[i].second.bytes);
+        out += tmp;
+    }
+    out += "}";
+    if (buf && cap) snprintf(buf, cap, "%s", out.c_str());
+    return out.size();
+}
 PXB_EXPORT int parallax_device_info(int* device, int* sm_count, char* name, size_t name_cap) {
     if (!ensure_device()) return PARALLAX_ERR_NO_DEVICE;
     if (device) *device = g_dev.device;

@@ -243,6 +243,10 @@ bool compact_typed(Workspace& ws, CompactMode mode, const Pred& pr, const void* 
     PredDev<T> p = make_pred<T>(pr);
     dim3 grid((unsigned)tiles);
     cudaStream_t s = ws.stream();
+    // profile bytes: input read (+ the kept elements written, known only on the device)
+    ProfScope prof(ws, mode == CompactMode::PARTITION ? "k_partition"
+                       : mode == CompactMode::UNIQUE ? "k_unique" : "k_copy_if",
+                   (mode == CompactMode::PARTITION ? 2 : 1) * n * sizeof(T));
     switch (mode) {
         case CompactMode::SELECT:
             launch_mode<T, 0>(grid, s, bulk, in, out, n, p, ts, nt, cnt_out);

@@ -107,7 +107,10 @@ bool launch_map(Workspace& ws, MapOp op, const void* d_in, void* d_out, size_t n
         case MapOp::SAXPY_GATHER_F32:
             if (capture_size < 4 || !c) break;
             memcpy(&a.a, c, 4);
-            k_saxpy_gather<<<grid_for(n), kBlock, 0, s>>>(a);
+            {
+                ProfScope prof(ws, "k_saxpy_gather", 24 * (uint64_t)n);
+                k_saxpy_gather<<<grid_for(n), kBlock, 0, s>>>(a);
+            }
             count_launch();
             return cuda_ok(cudaGetLastError(), "k_saxpy_gather launch");
         case MapOp::AFFINE_F32:

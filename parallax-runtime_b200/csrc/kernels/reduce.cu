@@ -235,7 +235,8 @@ uint64_t head_of(const void* p, uint64_t n) {
 
 // Ticket and partials live in the small scratch region (ScratchOff).
 template <typename T, typename A, typename R, typename Xf, typename Op>
-bool run(Workspace& ws, const void* d_in, uint64_t n, Xf xf, Op op, A ident, R* d_out) {
+bool run(Workspace& ws, const char* name, const void* d_in, uint64_t n, Xf xf, Op op, A ident,
+         R* d_out) {
     auto kernel = k_reduce<T, A, R, Xf, Op>;
     uint64_t head = head_of<T>(d_in, n);
     uint64_t nvec = (n - head) / (16 / sizeof(T));
@@ -246,8 +247,11 @@ bool run(Workspace& ws, const void* d_in, uint64_t n, Xf xf, Op op, A ident, R* 
     if (!scratch) return false;
     unsigned* ticket = reinterpret_cast<unsigned*>(scratch + ScratchOff::ticket);
     A* partials = reinterpret_cast<A*>(scratch + ScratchOff::partials);
-    kernel<<<grid, kBlock, 0, ws.stream()>>>(static_cast<const T*>(d_in), n, head, xf, op, ident,
-                                             partials, ticket, d_out);
+    {
+        ProfScope prof(ws, name, n * sizeof(T));
+        kernel<<<grid, kBlock, 0, ws.stream()>>>(static_cast<const T*>(d_in), n, head, xf, op,
+                                                 ident, partials, ticket, d_out);
+    }
     count_launch();
     return cuda_ok(cudaGetLastError(), "k_reduce launch");
 }
@@ -270,22 +274,22 @@ bool reduce_typed(Workspace& ws, RedOp op, const void* d_in, uint64_t n, void* d
     T* out = static_cast<T*>(d_out);
     if (op == RedOp::SUM) {
         using A = typename SumAcc<T>::type;
-        return run<T, A, T>(ws, d_in, n, XfValue<T, A>{}, OpSum{}, A(0), out);
+        return run<T, A, T>(ws, "k_reduce_sum", d_in, n, XfValue<T, A>{}, OpSum{}, A(0), out);
     }
     if (op == RedOp::MAX) {
         T ident = std::numeric_limits<T>::has_infinity ? -std::numeric_limits<T>::infinity()
                                                        : std::numeric_limits<T>::lowest();
-        return run<T, T, T>(ws, d_in, n, XfValue<T, T>{}, OpMax{}, ident, out);
+        return run<T, T, T>(ws, "k_reduce_max", d_in, n, XfValue<T, T>{}, OpMax{}, ident, out);
     }
     T ident = std::numeric_limits<T>::has_infinity ? std::numeric_limits<T>::infinity()
                                                    : std::numeric_limits<T>::max();
-    return run<T, T, T>(ws, d_in, n, XfValue<T, T>{}, OpMin{}, ident, out);
+    return run<T, T, T>(ws, "k_reduce_min", d_in, n, XfValue<T, T>{}, OpMin{}, ident, out);
 }
 
 template <typename T>
 bool count_typed(Workspace& ws, const Pred& p, const void* d_in, uint64_t n, uint64_t* d_out) {
     return run<T, unsigned long long, unsigned long long>(
-        ws, d_in, n, XfCount<T>{make_pred<T>(p)}, OpSum{}, 0ull,
+        ws, "k_count_if", d_in, n, XfCount<T>{make_pred<T>(p)}, OpSum{}, 0ull,
         reinterpret_cast<unsigned long long*>(d_out));
 }
 
@@ -294,7 +298,7 @@ bool find_typed(Workspace& ws, const Pred& p, const void* d_in, uint64_t n, uint
     // Non-matching elements map to ~0; seeding the min-fold with n reports "not found"
     // as n.
     return run<T, unsigned long long, unsigned long long>(
-        ws, d_in, n, XfFind<T>{make_pred<T>(p)}, OpMinU64{}, (unsigned long long)n,
+        ws, "k_find", d_in, n, XfFind<T>{make_pred<T>(p)}, OpMinU64{}, (unsigned long long)n,
         reinterpret_cast<unsigned long long*>(d_out));
 }
 
@@ -302,7 +306,7 @@ template <typename T>
 bool argminmax_typed(Workspace& ws, bool want_max, bool want_last, const void* d_in,
                      uint64_t n, uint64_t* d_out) {
     ArgVal<T> ident{T(0), ~0ull};
-    return run<T, ArgVal<T>, ArgToIndex<T>>(ws, d_in, n, XfArg<T>{}, OpArg<T>{want_max, want_last},
+    return run<T, ArgVal<T>, ArgToIndex<T>>(ws, "k_argminmax", d_in, n, XfArg<T>{}, OpArg<T>{want_max, want_last},
                                             ident, reinterpret_cast<ArgToIndex<T>*>(d_out));
 }
 
@@ -364,11 +368,14 @@ bool mismatch_typed(Workspace& ws, const void* a, const void* b, uint64_t n, uin
     if ((size_t)grid > kMaxPartials) grid = (int)kMaxPartials;
     char* scratch = ws.scratch(0);
     if (!scratch) return false;
-    kernel<<<grid, kBlock, 0, ws.stream()>>>(
-        static_cast<const T*>(a), static_cast<const T*>(b), n, vec_ok,
-        reinterpret_cast<unsigned long long*>(scratch + ScratchOff::partials),
-        reinterpret_cast<unsigned*>(scratch + ScratchOff::ticket),
-        reinterpret_cast<unsigned long long*>(d_out));
+    {
+        ProfScope prof(ws, "k_mismatch", 2 * n * sizeof(T));
+        kernel<<<grid, kBlock, 0, ws.stream()>>>(
+            static_cast<const T*>(a), static_cast<const T*>(b), n, vec_ok,
+            reinterpret_cast<unsigned long long*>(scratch + ScratchOff::partials),
+            reinterpret_cast<unsigned*>(scratch + ScratchOff::ticket),
+            reinterpret_cast<unsigned long long*>(d_out));
+    }
     count_launch();
     return cuda_ok(cudaGetLastError(), "k_mismatch launch");
 }

@@ -178,6 +178,7 @@ bool scan_typed(Workspace& ws, bool exclusive, const void* d_in, void* d_out, ui
     T* out = static_cast<T*>(d_out);
     dim3 grid((unsigned)tiles);
     cudaStream_t s = ws.stream();
+    ProfScope prof(ws, exclusive ? "k_scan_exclusive" : "k_scan_inclusive", 2 * n * sizeof(T));
     if (exclusive) {
         if (bulk) k_scan<T, true, true><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
         else k_scan<T, true, false><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);

@@ -274,15 +274,26 @@ bool sort_keys(Workspace& ws, void* d_data, uint64_t n) {
     }
     cudaStream_t s = ws.stream();
     K* cur = (passes % 2 == 0) ? data : tmp;
-    k_tile_sort<K, XF><<<(unsigned)tiles, kBlock, 0, s>>>(data, cur, n, passes == 0);
+    {
+        ProfScope prof(ws, "k_tile_sort", 2 * n * sizeof(K));
+        k_tile_sort<K, XF><<<(unsigned)tiles, kBlock, 0, s>>>(data, cur, n, passes == 0);
+    }
     count_launch();
     for (int pass = 1; pass <= passes; ++pass) {
         const uint64_t L = (uint64_t)TILE << (pass - 1);
         K* nxt = cur == data ? tmp : data;
         const unsigned search_blocks = (unsigned)((tiles * 32 + kBlock - 1) / kBlock);
-        k_merge_path<K><<<search_blocks, kBlock, 0, s>>>(cur, n, L, TILE, tiles, splits);
-        if (pass == passes) k_merge<K, XF, true><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, splits);
-        else k_merge<K, XF, false><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, splits);
+        {
+            ProfScope prof(ws, "k_merge_path", 0);
+            k_merge_path<K><<<search_blocks, kBlock, 0, s>>>(cur, n, L, TILE, tiles, splits);
+        }
+        {
+            ProfScope prof(ws, "k_merge", 2 * n * sizeof(K));
+            if (pass == passes)
+                k_merge<K, XF, true><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, splits);
+            else
+                k_merge<K, XF, false><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, splits);
+        }
         count_launch(2);
         cur = nxt;
     }

@@ -39,6 +39,23 @@ const DeviceInfo& device_info();
 void count_launch(unsigned n = 1);
 uint64_t launch_count();
 
+// Optional per-launch device timing (parallax_profile_enable). When enabled, each
+// launcher brackets its kernel with CUDA events on the launch stream and records the
+// launch's algorithmic bytes (the minimum HBM traffic of the work it does), so achieved
+// bandwidth per kernel comes from live events. Disabled: one predictable branch.
+struct Workspace;
+class ProfScope {
+  public:
+    ProfScope(Workspace& ws, const char* kernel, uint64_t alg_bytes);
+    ~ProfScope();
+
+  private:
+    Workspace* ws_ = nullptr;
+    const char* name_ = nullptr;
+    uint64_t bytes_ = 0;
+    cudaEvent_t start_ = nullptr;
+};
+
 // Pinned, device-mapped slot the kernels write small results into (reduce scalars,
 // kept counts, in-kernel wait-timeout codes) so a synchronous call needs no extra
 // device-to-host copy.
@@ -113,6 +130,9 @@ uint64_t arena_mapped_bytes();  // bytes of the arena currently backed by device
 // may touch any block, so they get the reference's whole-arena coherence
 // (src/memory/arena.cpp:296-304) restricted to blocks in coherent mode.
 bool arena_sync_coherent(Workspace& ws, bool to_device);
+// Host mirror <-> device copy of an arena range (split at page-lock chunk boundaries).
+bool arena_copy_async(void* dst, const void* src, size_t bytes, bool to_device,
+                      cudaStream_t s);
 
 // ---- operands --------------------------------------------------------------------------
 // How an ABI pointer reaches the device:

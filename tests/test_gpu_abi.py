@@ -284,3 +284,18 @@ def test_launch_counter_counts_kernels(lib, px, dev):
     before = lib.parallax_launch_count()
     lib.parallax_reduce(px.builtin("reduce:sum:f32"), d.data_ptr(), 1 << 16, 4, out)
     assert lib.parallax_launch_count() == before + 1
+
+
+def test_coherent_operand_spanning_arena_chunks(lib, px, ox, arena):
+    # 600 MiB block: its range crosses a 512 MiB page-lock chunk of the host mirror
+    n = (600 << 20) // 4
+    x = ox.gen("i32_pm1000", 31, n)
+    data = arena.array(x)
+    res = np.zeros(1, np.int32)
+    lib.parallax_reduce(px.builtin("reduce:sum:i32"), P(data), n, 4, P(res))
+    px.check()
+    assert res[0] == ox.reduce_sum(x)
+    h = px.builtin("scan:i32")
+    lib.parallax_scan(h, h, P(data), n, 4)
+    px.check()
+    assert np.array_equal(data, ox.scan(x))
