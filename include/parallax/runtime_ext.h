@@ -87,6 +87,27 @@ int parallax_set_async(int async);
 int parallax_synchronize(void);
 size_t parallax_last_count(void);
 
+/* ---- allocation-free scan -------------------------------------------------------- */
+/* No counterpart in the reference. For callers that cannot allocate device memory: code
+ * running inside an allocation hook (a malloc / operator new interposer that routes the
+ * heap into the arena would re-enter itself if the runtime allocated) or a process whose
+ * device memory belongs to its own pool. Same result as parallax_scan (init == NULL,
+ * inclusive) or parallax_exclusive_scan (init != NULL, exclusive with that init), from
+ * `input` to `output` (may be the same buffer), both DEVICE pointers, on `cuda_stream`
+ * (NULL = the legacy default stream); returns when the result is ready, with a
+ * parallax_status.
+ * The runtime allocates nothing for it: the look-back status lives in one static device
+ * array of 576.25 KiB that every GPU loading this library holds until the process exits.
+ * That caps count at 24576 tiles: 75,497,472 elements of a 4-byte type, 37,748,736 of an
+ * 8-byte type; larger counts return PARALLAX_ERR_INVALID_ARGUMENT and touch nothing.
+ * The first call on a device looks up that array's device address (once per device, with
+ * the device current); make that first call before any stream capture. All calls share
+ * the array: calls that overlap on the GPU (other streams, other threads) race and must
+ * be serialized by the caller. */
+int parallax_scan_noalloc(parallax_kernel_t scan_kernel, const void* input, void* output,
+                          size_t count, size_t elem_size, const void* init,
+                          void* cuda_stream);
+
 /* ---- instrumentation ------------------------------------------------------------- */
 /* Number of runtime kernel launches issued by this process so far. */
 uint64_t parallax_launch_count(void);

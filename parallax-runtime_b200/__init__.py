@@ -87,6 +87,7 @@ _SIGNATURES = {
     "parallax_profile_enable": (None, [C.c_int]),
     "parallax_profile_json": (sz, [C.c_char_p, sz]),
     "parallax_profile_reset": (None, []),
+    "parallax_scan_noalloc": (C.c_int, [vp, vp, vp, sz, sz, vp, vp]),
     "parallax_device_info": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p, sz]),
 }
 

@@ -18,6 +18,9 @@
 // Accumulation: fp32 data is scanned per thread in fp32 (12 terms) and carried across
 // threads, warps and tiles in fp64; integers wrap around in their unsigned type.
 #include <stdint.h>
+#include <string.h>
+
+#include <mutex>
 
 #include "../lookback.cuh"
 #include "../runtime.hpp"
@@ -208,3 +211,171 @@ bool launch_scan(Workspace& ws, DType t, bool exclusive, const void* d_in, void*
 }
 
 }  // namespace pxb
+
+// ---- allocation-free scan -----------------------------------------------------------------
+// Some callers cannot allocate device memory at all: code that runs inside an allocation
+// hook (a malloc / operator new interposer that routes the heap into the arena would
+// re-enter itself if the runtime allocated), or a process whose device memory has been
+// handed to its own pool. parallax_scan_noalloc gives them the single-pass scan with no
+// allocation by the runtime: the look-back status lives in the fixed static device array
+// below (576.25 KiB, held on every GPU that loads this library until the process exits),
+// the caller passes device buffers for input and output and a stream, and no workspace,
+// stream, event or pinned slot is created.
+namespace pxb {
+namespace {
+
+constexpr uint64_t kNoAllocTiles = 24576;  // look-back status entries
+constexpr size_t kNoAllocBytes = 256 + kNoAllocTiles * sizeof(StatusEntry);
+// [0, 4): in-kernel wait-timeout code; [256, ...): look-back status entries. Static device
+// memory starts zeroed; later calls find stale entries from older epochs, which read as
+// "not ready", so only the timeout code is cleared per call.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocDevice {
+    bool ready = false;
+    char* scratch = nullptr;  // device address of g_noalloc_scratch on that device
+    uint32_t epoch = 0;
+};
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc[kNoAllocMaxDevices];
+
+template <typename T>
+uint64_t noalloc_max_elements() {
+    return kNoAllocTiles * (uint64_t)ScanShape<T>::TILE;
+}
+
+template <typename T>
+bool noalloc_launch(const void* d_in, void* d_out, uint64_t n, const void* init_host,
+                    cudaStream_t s, char* scratch, uint32_t epoch) {
+    using A = typename ScanTypes<T>::A;
+    constexpr int TILE = ScanShape<T>::TILE;
+    const uint64_t tiles = (n + TILE - 1) / TILE;
+    TileStatus<A> ts;
+    ts.e = reinterpret_cast<StatusEntry*>(scratch + 256);
+    ts.epoch = epoch;
+    ts.err = reinterpret_cast<int32_t*>(scratch);
+    A init = A(0);
+    if (init_host) {
+        T v;
+        memcpy(&v, init_host, sizeof(T));
+        init = (A)v;
+    }
+    const bool bulk = (reinterpret_cast<uintptr_t>(d_in) % 16 == 0) &&
+                      (reinterpret_cast<uintptr_t>(d_out) % 16 == 0);
+    const T* in = static_cast<const T*>(d_in);
+    T* out = static_cast<T*>(d_out);
+    dim3 grid((unsigned)tiles);
+    if (init_host) {
+        if (bulk) k_scan<T, true, true><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
+        else k_scan<T, true, false><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
+    } else {
+        if (bulk) k_scan<T, false, true><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
+        else k_scan<T, false, false><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
+    }
+    count_launch();
+    return cuda_ok(cudaGetLastError(), "parallax_scan_noalloc launch");
+}
+
+}  // namespace
+}  // namespace pxb
+
+using namespace pxb;
+
+PXB_EXPORT int parallax_scan_noalloc(parallax_kernel_t scan_kernel, const void* input,
+                                     void* output, size_t count, size_t elem_size,
+                                     const void* init, void* cuda_stream) {
+    set_ok();
+    Handle* h = as_handle(scan_kernel);
+    if (!h || h->kind != Kind::SCAN) {
+        set_error(PARALLAX_ERR_INVALID_HANDLE, "parallax_scan_noalloc: not a scan kernel handle");
+        return PARALLAX_ERR_INVALID_HANDLE;
+    }
+    if (dtype_size(h->dtype) != elem_size || !input || !output) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT,
+                  "parallax_scan_noalloc: null buffer or elem_size %zu does not match the handle",
+                  elem_size);
+        return PARALLAX_ERR_INVALID_ARGUMENT;
+    }
+    if (count == 0) return PARALLAX_OK;
+    uint64_t max_n = 0;
+    switch (h->dtype) {
+        case DType::F32: max_n = noalloc_max_elements<float>(); break;
+        case DType::F64: max_n = noalloc_max_elements<double>(); break;
+        case DType::I32: max_n = noalloc_max_elements<int32_t>(); break;
+        case DType::I64: max_n = noalloc_max_elements<int64_t>(); break;
+        case DType::U32: max_n = noalloc_max_elements<uint32_t>(); break;
+        case DType::U64: max_n = noalloc_max_elements<uint64_t>(); break;
+        default: break;
+    }
+    if (count > max_n) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT,
+                  "parallax_scan_noalloc: %zu elements exceed its maximum of %llu for this "
+                  "element type (%llu look-back tiles in a %zu-byte static array); use "
+                  "parallax_scan or parallax_exclusive_scan",
+                  count, (unsigned long long)max_n, (unsigned long long)kNoAllocTiles,
+                  kNoAllocBytes);
+        return PARALLAX_ERR_INVALID_ARGUMENT;
+    }
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "parallax_scan_noalloc: cudaGetDevice"))
+        return PARALLAX_ERR_CUDA;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error(PARALLAX_ERR_UNSUPPORTED, "parallax_scan_noalloc: device %d out of range", dev);
+        return PARALLAX_ERR_UNSUPPORTED;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+    char* scratch = nullptr;
+    uint32_t epoch = 0;
+    {
+        std::lock_guard<std::mutex> g(g_noalloc_mu);
+        NoAllocDevice& d = g_noalloc[dev];
+        if (!d.ready) {
+            // Once per device, with that device current. The name of a __device__ array is
+            // a host-side stand-in in host code; only this address reaches the kernel.
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                cuda_ok(e == cudaSuccess ? cudaErrorInvalidSymbol : e,
+                        "parallax_scan_noalloc: cudaGetSymbolAddress");
+                return PARALLAX_ERR_CUDA;
+            }
+            d.scratch = static_cast<char*>(p);
+            d.epoch = 0;
+            d.ready = true;
+        }
+        if (++d.epoch >= (1u << 30)) {  // epoch wrap: stale words could alias, clear them
+            if (!cuda_ok(cudaMemsetAsync(d.scratch + 256, 0, kNoAllocBytes - 256, s),
+                         "parallax_scan_noalloc: clear status"))
+                return PARALLAX_ERR_CUDA;
+            d.epoch = 1;
+        }
+        scratch = d.scratch;
+        epoch = d.epoch;
+    }
+    if (!cuda_ok(cudaMemsetAsync(scratch, 0, sizeof(int32_t), s),
+                 "parallax_scan_noalloc: clear timeout code"))
+        return PARALLAX_ERR_CUDA;
+    bool ok = false;
+    switch (h->dtype) {
+        case DType::F32: ok = noalloc_launch<float>(input, output, count, init, s, scratch, epoch); break;
+        case DType::F64: ok = noalloc_launch<double>(input, output, count, init, s, scratch, epoch); break;
+        case DType::I32: ok = noalloc_launch<int32_t>(input, output, count, init, s, scratch, epoch); break;
+        case DType::I64: ok = noalloc_launch<int64_t>(input, output, count, init, s, scratch, epoch); break;
+        case DType::U32: ok = noalloc_launch<uint32_t>(input, output, count, init, s, scratch, epoch); break;
+        case DType::U64: ok = noalloc_launch<uint64_t>(input, output, count, init, s, scratch, epoch); break;
+        default: break;
+    }
+    if (!ok) return PARALLAX_ERR_CUDA;
+    int32_t code = 0;
+    if (!cuda_ok(cudaMemcpyAsync(&code, scratch, sizeof code, cudaMemcpyDeviceToHost, s),
+                 "parallax_scan_noalloc: read timeout code") ||
+        !cuda_ok(cudaStreamSynchronize(s), "parallax_scan_noalloc: stream synchronize"))
+        return PARALLAX_ERR_CUDA;
+    if (code) {
+        set_error(PARALLAX_ERR_DEVICE_SPIN, "parallax_scan_noalloc: in-kernel wait gave up (%d)",
+                  code);
+        return PARALLAX_ERR_DEVICE_SPIN;
+    }
+    return PARALLAX_OK;
+}
