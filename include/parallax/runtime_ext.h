@@ -98,8 +98,8 @@ size_t parallax_last_count(void);
  * parallax_status.
  * The runtime allocates nothing for it: the look-back status lives in one static device
  * array of 576.25 KiB that every GPU loading this library holds until the process exits.
- * That caps count at 24576 tiles: 75,497,472 elements of a 4-byte type, 37,748,736 of an
- * 8-byte type; larger counts return PARALLAX_ERR_INVALID_ARGUMENT and touch nothing.
+ * That caps count at 24576 tiles: 301,989,888 elements of a 4-byte type, 150,994,944 of
+ * an 8-byte type; larger counts return PARALLAX_ERR_INVALID_ARGUMENT and touch nothing.
  * The first call on a device looks up that array's device address (once per device, with
  * the device current); make that first call before any stream capture. All calls share
  * the array: calls that overlap on the GPU (other streams, other threads) race and must

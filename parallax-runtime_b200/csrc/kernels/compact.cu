@@ -7,21 +7,24 @@
 // fp32 counts inexact beyond 2^24; here counts are 32-bit within a tile and 64-bit
 // across tiles.
 //
-// Here: one CTA per tile, in blockIdx order. A CTA stages its tile with one bulk copy,
-// evaluates the predicate (or the adjacent-difference test for unique) on 12 / 6
-// consecutive elements per thread, ranks the kept elements with shuffle scans, gets the
-// tile's output offset by decoupled look-back on kept counts, packs the kept elements in
-// shared memory and writes them out with coalesced stores. Traffic: n*s read + k*s
-// written.
+// Here: one CTA per 48 KiB tile, in blockIdx order, staged as four bulk-copied sub-tiles
+// (tiles.cuh). Phase 1 evaluates the predicate (or the adjacent-difference test for
+// unique) on 12 / 6 consecutive elements per thread as each sub-tile lands, keeps the
+// flags as bit masks, and ranks the kept elements with one shuffle scan per sub-tile and
+// one 32-lane scan over the (sub-tile, warp) counts; warp 0 gets the tile's output offset
+// by decoupled look-back on kept counts. Phase 2 packs the kept elements at the front of
+// the staged tile, sub-tile by sub-tile (a packed element never lands beyond the sub-tile
+// being packed), and writes them with coalesced stores. Traffic: n*s read + k*s written.
 // Partition writes every element: kept ones to [0, k), the rest in order to [k, n). The
 // rejected elements' offsets need k, so partition runs a count pass first (one read of
-// the input) and then the same kernel with two output cursors.
+// the input) and then writes both cursors straight from registers.
 #include <stdint.h>
 
 #include <type_traits>
 
 #include "../lookback.cuh"
 #include "../runtime.hpp"
+#include "../tiles.cuh"
 #include "../tma.cuh"
 
 namespace pxb {
@@ -29,12 +32,15 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kVpt = 3;
+constexpr int kSub = 4;
 
 template <typename T>
 struct Shape {
     static constexpr int V = 16 / sizeof(T);
     static constexpr int ITEMS = kVpt * V;
-    static constexpr int TILE = kBlock * ITEMS;
+    static constexpr int SUB = kBlock * ITEMS;
+    static constexpr int TILE = kSub * SUB;
+    static constexpr size_t SMEM = TILE * sizeof(T);
 };
 
 template <typename T>
@@ -42,6 +48,7 @@ struct PredDev {
     PredKind kind;
     bool negate;
     T c, m, r;
+    double inv_m;  // 1.0 / m for the fast 32-bit remainder
     __device__ __forceinline__ bool operator()(T x) const {
         bool v;
         switch (kind) {
@@ -60,141 +67,258 @@ struct PredDev {
         }
         return v != negate;
     }
+    // Flag bits of one row: the switch on the (CTA-uniform) kind is taken once per row.
+    template <int ITEMS>
+    __device__ __forceinline__ uint32_t flags(const T (&x)[ITEMS]) const {
+        uint32_t f = 0;
+        switch (kind) {
+#define PXB_ROW(KIND, EXPR)                                              \
+            case PredKind::KIND:                                          \
+                _Pragma("unroll") for (int j = 0; j < ITEMS; ++j)          \
+                    f |= (uint32_t)((EXPR) != negate) << j;                \
+                break;
+            PXB_ROW(GT, x[j] > c)
+            PXB_ROW(GE, x[j] >= c)
+            PXB_ROW(LT, x[j] < c)
+            PXB_ROW(LE, x[j] <= c)
+            PXB_ROW(EQ, x[j] == c)
+            PXB_ROW(NE, x[j] != c)
+            PXB_ROW(NONZERO, x[j] != T(0))
+            PXB_ROW(MOD, mod_eq(x[j]))
+#undef PXB_ROW
+            default: break;
+        }
+        return f;
+    }
+    // x % m == r with C semantics; 32-bit integers divide through an exact fp64 quotient
+    // estimate plus a one-step remainder correction instead of the long integer division.
+    __device__ __forceinline__ bool mod_eq(T x) const {
+        if constexpr (std::is_integral<T>::value && sizeof(T) == 4) {
+            const int64_t xi = (int64_t)x, mi = (int64_t)m;
+            const int64_t q = (int64_t)((double)xi * inv_m);
+            int64_t rr = xi - q * mi;
+            const int64_t am = mi < 0 ? -mi : mi;
+            if (xi >= 0) { if (rr < 0) rr += am; else if (rr >= am) rr -= am; }
+            else { if (rr > 0) rr -= am; else if (rr <= -am) rr += am; }
+            return rr == (int64_t)r;
+        } else if constexpr (std::is_integral<T>::value) {
+            return x % m == r;
+        } else {
+            return false;
+        }
+    }
 };
 
-// MODE: 0 select (copy_if / remove_if), 1 unique, 2 partition
+template <typename T, int ITEMS, int V>
+__device__ __forceinline__ void load_row(const T* row_ptr, T (&x)[ITEMS]) {
+    const uint4* row = reinterpret_cast<const uint4*>(row_ptr);
+#pragma unroll
+    for (int v = 0; v < ITEMS / V; ++v) {
+        const uint4 r = row[v];
+        const T* e = reinterpret_cast<const T*>(&r);
+#pragma unroll
+        for (int k = 0; k < V; ++k) x[v * V + k] = e[k];
+    }
+}
+
+// Shared state of one CTA's tile processing.
+struct CompactSmem {
+    uint32_t cnt[32];               // (sub-tile, warp) kept counts
+    uint64_t red[kBlock / 32 + 1];  // look-back scratch
+    int first[kBlock / 32];
+};
+
+// One staged tile: flags, ranks, look-back, then packed (select / unique) or scattered
+// (partition) output. MODE: 0 select (copy_if / remove_if), 1 unique, 2 partition.
+// `prev_of_tile` is the element before the tile (unique only). Ends with a barrier after
+// which the tile buffer may be refilled.
 template <typename T, int MODE, bool BULK>
-__global__ void __launch_bounds__(kBlock)
-k_compact(const T* in, T* out, uint64_t n, PredDev<T> pred,
-          TileStatus<uint64_t> ts, const unsigned long long* __restrict__ num_true,
-          unsigned long long* __restrict__ count_out) {
+__device__ __forceinline__ void compact_tile(T* buf, uint64_t* bars, uint32_t parity,
+                                             CompactSmem& sm, uint64_t tile, uint64_t base,
+                                             uint32_t cnt, T prev_of_tile, T* out, uint64_t n,
+                                             const PredDev<T>& pred,
+                                             const TileStatus<uint64_t>& ts,
+                                             const unsigned long long* num_true,
+                                             unsigned long long* count_out, bool last_tile) {
     constexpr int V = Shape<T>::V;
     constexpr int ITEMS = Shape<T>::ITEMS;
-    constexpr int TILE = Shape<T>::TILE;
-    __shared__ __align__(128) T buf[TILE];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ uint32_t s_warp[kBlock / 32];
-    __shared__ uint32_t s_wex[kBlock / 32];
-    __shared__ uint32_t s_kept;
-    __shared__ uint64_t s_prefix;
-
+    constexpr int SUB = Shape<T>::SUB;
+    constexpr int WARPS = kBlock / 32;
+    static_assert(kSub * WARPS == 32, "one lane per (sub-tile, warp)");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint64_t tile = blockIdx.x;
-    const uint64_t base = tile * (uint64_t)TILE;
-    const uint64_t rem = n - base;
-    const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
-
-    uint32_t bulk = 0;
-    if constexpr (BULK) {
-        bulk = (uint32_t)((cnt * sizeof(T)) / 16 * 16 / sizeof(T));
-        if (tid == 0) {
-            mbar_init(&bar, 1);
-            fence_mbar_init();
-            mbar_arrive_expect_tx(&bar, bulk * (uint32_t)sizeof(T));
-            if (bulk) bulk_load(buf, in + base, bulk * (uint32_t)sizeof(T), &bar);
-        }
-    }
-    for (uint32_t e = bulk + tid; e < (uint32_t)TILE; e += kBlock)
-        buf[e] = e < cnt ? in[base + e] : T(0);
-    T prev_of_tile = T(0);
-    if (MODE == 1 && tid == 0 && base > 0) prev_of_tile = in[base - 1];
-    __syncthreads();
-    if constexpr (BULK) {
-        uint32_t spins = 0;
-        while (!mbar_try_wait(&bar, 0)) {
-            if (++spins > kSpinLimit) {
-                *ts.err = 2;
-                break;
-            }
-        }
-    }
-
-    // ---- flags for ITEMS consecutive elements ----
-    T x[ITEMS];
-    {
-        const uint4* row = reinterpret_cast<const uint4*>(buf + tid * ITEMS);
-#pragma unroll
-        for (int v = 0; v < kVpt; ++v) {
-            uint4 r = row[v];
-            const T* e = reinterpret_cast<const T*>(&r);
-#pragma unroll
-            for (int k = 0; k < V; ++k) x[v * V + k] = e[k];
-        }
-    }
     const uint32_t row0 = (uint32_t)tid * ITEMS;
-    uint32_t flags = 0;
-    if constexpr (MODE == 1) {
-        T prev = tid > 0 ? buf[row0 - 1] : prev_of_tile;
-        const bool first_global = (base == 0 && tid == 0);
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            const bool keep = (j == 0 && first_global) || !(x[j] == (j ? x[j - 1] : prev));
-            if (row0 + j < cnt && keep) flags |= 1u << j;
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j)
-            if (row0 + j < cnt && pred(x[j])) flags |= 1u << j;
-    }
 
-    // ---- ranks within the tile ----
-    const uint32_t c = __popc(flags);
-    const uint32_t incl = warp_inclusive_scan(c, OpSum());
-    uint32_t texcl = shfl_up(incl, 1);
-    if (lane == 0) texcl = 0;
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t w = lane < kBlock / 32 ? s_warp[lane] : 0u;
-        const uint32_t wi = warp_inclusive_scan(w, OpSum());
-        const uint32_t agg = shfl_idx(wi, kBlock / 32 - 1);
-        uint32_t wex = shfl_up(wi, 1);
-        if (lane == 0) wex = 0;
-        const uint64_t prefix = lookback<uint64_t>(ts, tile, (uint64_t)agg);
-        if (lane < kBlock / 32) s_wex[lane] = wex;
-        if (lane == 0) {
-            s_prefix = prefix;
-            s_kept = agg;
-            if (MODE != 2 && tile == gridDim.x - 1) *count_out = prefix + agg;
+    // ---- phase 1: flags and ranks ----
+    uint32_t fl[kSub];   // bit j: element j of this thread's row in sub-tile s is kept
+    uint32_t tex[kSub];  // kept elements before this row within its warp
+#pragma unroll
+    for (int s = 0; s < kSub; ++s) {
+        if constexpr (BULK) wait_bar(&bars[s], parity, ts.err);
+        const uint32_t e0 = (uint32_t)s * SUB + row0;  // tile index of the row's first element
+        T x[ITEMS];
+        load_row<T, ITEMS, V>(buf + e0, x);
+        uint32_t f = 0;
+        if constexpr (MODE == 1) {
+            const T prev = e0 > 0 ? buf[e0 - 1] : prev_of_tile;
+            const bool first_global = base == 0 && e0 == 0;
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                const bool keep = (j == 0 && first_global) || !(x[j] == (j ? x[j - 1] : prev));
+                if (e0 + j < cnt && keep) f |= 1u << j;
+            }
+        } else {
+            f = pred.template flags<ITEMS>(x);
+            if (e0 + ITEMS > cnt) f &= e0 >= cnt ? 0u : (1u << (cnt - e0)) - 1u;
         }
+        fl[s] = f;
+        const uint32_t incl = warp_inclusive_scan((uint32_t)__popc(f), OpSum());
+        const uint32_t ex = shfl_up(incl, 1);
+        tex[s] = lane == 0 ? 0u : ex;
+        if (lane == 31) sm.cnt[s * WARPS + warp] = incl;
     }
     __syncthreads();
-    const uint32_t tile_kept = s_kept;
-    const uint64_t prefix = s_prefix;
-    uint32_t r = s_wex[warp] + texcl;  // tile-local rank of this thread's first kept element
+    // Every warp scans the 32 (sub-tile, warp) counts itself, then the whole CTA runs the
+    // look-back on kept counts.
+    uint32_t woff[kSub];  // kept elements before this warp's rows within the tile
+    uint32_t tile_kept;
+    {
+        const uint32_t v = sm.cnt[lane];
+        const uint32_t vi = warp_inclusive_scan(v, OpSum());
+        tile_kept = shfl_idx(vi, 31);
+        uint32_t vex = shfl_up(vi, 1);
+        if (lane == 0) vex = 0;
+#pragma unroll
+        for (int s = 0; s < kSub; ++s) woff[s] = shfl_idx(vex, s * WARPS + warp);
+    }
+    const uint64_t prefix =
+        lookback_cta<uint64_t, kBlock>(ts, tile, (uint64_t)tile_kept, sm.red, sm.first);
+    if (MODE != 2 && last_tile && tid == 0) *count_out = prefix + tile_kept;
 
-    // ---- pack into shared memory (all rows were read before the barrier above) ----
     if constexpr (MODE == 2) {
-        uint32_t rf = row0 - r;  // rejected elements before this thread's row, within the tile
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            if (row0 + j >= cnt) break;
-            if (flags >> j & 1u) buf[r++] = x[j];
-            else buf[tile_kept + rf++] = x[j];
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j)
-            if (flags >> j & 1u) buf[r++] = x[j];
-    }
-    __syncthreads();
-
-    // ---- coalesced stores ----
-    if constexpr (MODE == 2) {
+        // ---- partition: both cursors straight from registers ----
         const uint64_t nt = *num_true;
         const uint64_t rej_base = nt + (base - prefix);
-        for (uint32_t i = tid; i < cnt; i += kBlock) {
-            const uint64_t dst = i < tile_kept ? prefix + i : rej_base + (i - tile_kept);
-            if (dst < n) out[dst] = buf[i];
-            else *ts.err = 3;  // only reachable after a failed wait: never write out of range
+#pragma unroll
+        for (int s = 0; s < kSub; ++s) {
+            const uint32_t e0 = (uint32_t)s * SUB + row0;
+            T x[ITEMS];
+            load_row<T, ITEMS, V>(buf + e0, x);
+            uint32_t r = woff[s] + tex[s];                    // kept before this row (tile)
+            uint32_t rf = e0 - r;                             // rejected before this row
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                if (e0 + j >= cnt) break;
+                const uint64_t dst = (fl[s] >> j & 1u) ? prefix + r++ : rej_base + rf++;
+                if (dst < n) out[dst] = x[j];
+                else *ts.err = 3;  // only reachable after a failed wait: never write out of range
+            }
         }
-        if (tid == 0 && tile == gridDim.x - 1) *count_out = nt;
+        if (tid == 0 && last_tile) *count_out = nt;
     } else {
+        // ---- pack kept elements at the front of the tile, then store them ----
+#pragma unroll
+        for (int s = 0; s < kSub; ++s) {
+            T x[ITEMS];
+            load_row<T, ITEMS, V>(buf + (uint32_t)s * SUB + row0, x);
+            __syncthreads();  // every row of sub-tile s is in registers before packing
+            uint32_t r = woff[s] + tex[s];
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j)
+                if (fl[s] >> j & 1u) buf[r++] = x[j];
+        }
+        __syncthreads();
         for (uint32_t i = tid; i < tile_kept; i += kBlock) {
             if (prefix + i < n) out[prefix + i] = buf[i];
             else *ts.err = 3;
         }
     }
+    __syncthreads();  // buffer and shared state free for the next tile
+}
+
+// One CTA per tile, in blockIdx order (unaligned input).
+template <typename T, int MODE, bool BULK>
+__global__ void __launch_bounds__(kBlock, 4)
+k_compact(const T* in, T* out, uint64_t n, PredDev<T> pred, TileStatus<uint64_t> ts,
+          const unsigned long long* __restrict__ num_true,
+          unsigned long long* __restrict__ count_out) {
+    constexpr int SUB = Shape<T>::SUB;
+    constexpr int TILE = Shape<T>::TILE;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* buf = reinterpret_cast<T*>(smem_raw);
+    __shared__ __align__(8) uint64_t bars[kSub];
+    __shared__ CompactSmem sm;
+    const uint64_t tile = blockIdx.x;
+    const uint64_t base = tile * (uint64_t)TILE;
+    const uint64_t rem = n - base;
+    const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+    stage_tile<T, SUB, kSub, kBlock, BULK>(buf, bars, in, base, cnt);
+    const T prev = (MODE == 1 && base > 0) ? in[base - 1] : T(0);
+    __syncthreads();
+    compact_tile<T, MODE, BULK>(buf, bars, 0, sm, tile, base, cnt, prev, out, n, pred, ts,
+                                num_true, count_out, tile == gridDim.x - 1);
+}
+
+// Persistent CTAs (two per SM), two tile buffers each: the next claimed tile's bulk copies
+// are in flight while the current tile is compacted. Input 16-byte aligned.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kBlock, 2)
+k_compact_persistent(const T* in, T* out, uint64_t n, uint64_t num_tiles, PredDev<T> pred,
+                     TileStatus<uint64_t> ts, const unsigned long long* __restrict__ num_true,
+                     unsigned long long* __restrict__ count_out, uint32_t* counters) {
+    constexpr int SUB = Shape<T>::SUB;
+    constexpr int TILE = Shape<T>::TILE;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* const buf0 = reinterpret_cast<T*>(smem_raw);  // buffer b at buf0 + b * TILE
+    __shared__ __align__(8) uint64_t bars[2][kSub];
+    __shared__ CompactSmem sm;
+    __shared__ uint32_t s_tile[2];
+    __shared__ T s_prev[2];
+    const int tid = threadIdx.x;
+
+    auto claim_and_issue = [&](int b) {  // thread 0 only
+        const uint32_t t = atomicAdd(&counters[0], 1u);
+        s_tile[b] = t;
+        if (t < num_tiles) {
+            const uint64_t base = (uint64_t)t * TILE;
+            const uint64_t rem = n - base;
+            issue_tile<T, SUB, kSub>(buf0 + (size_t)b * TILE, bars[b], in, base,
+                                     rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE);
+            // the element before the tile (unique): its latency hides behind this round
+            s_prev[b] = (MODE == 1 && base > 0) ? in[base - 1] : T(0);
+        }
+    };
+    if (tid == 0) {
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int s = 0; s < kSub; ++s) mbar_init(&bars[b][s], 1);
+        fence_mbar_init();
+        claim_and_issue(0);
+    }
+    __syncthreads();
+    for (uint32_t it = 0;; ++it) {
+        const int b = it & 1;
+        const uint32_t parity = (it >> 1) & 1u;
+        const uint32_t cur = s_tile[b];
+        if (cur >= num_tiles) break;
+        const T prev = s_prev[b];
+        if (tid == 0) {
+            fence_proxy_async_smem();
+            claim_and_issue(b ^ 1);
+        }
+        T* buf = buf0 + (size_t)b * TILE;
+        const uint64_t base = (uint64_t)cur * TILE;
+        const uint64_t rem = n - base;
+        const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+        const uint32_t bulk = bulk_elems<T>(cnt);
+        if (cnt < (uint32_t)TILE || bulk < cnt) {  // the last tile: ragged end and padding
+            fill_ragged<T, TILE, kBlock>(buf, in, base, cnt, bulk);
+            __syncthreads();
+        }
+        compact_tile<T, MODE, true>(buf, bars[b], parity, sm, cur, base, cnt, prev, out, n,
+                                    pred, ts, num_true, count_out, cur == num_tiles - 1);
+    }
+    if (tid == 0) persistent_exit(counters);
 }
 
 template <typename T>
@@ -207,15 +331,37 @@ PredDev<T> make_pred(const Pred& p) {
     else e.c = (T)p.u;
     e.m = (T)p.mod_m;
     e.r = (T)p.mod_r;
+    e.inv_m = p.mod_m ? 1.0 / (double)p.mod_m : 0.0;
     return e;
 }
 
 template <typename T, int MODE>
-void launch_mode(dim3 grid, cudaStream_t s, bool bulk, const T* in, T* out, uint64_t n,
+bool launch_mode(uint64_t tiles, cudaStream_t s, bool bulk, const T* in, T* out, uint64_t n,
                  PredDev<T> p, TileStatus<uint64_t> ts, const unsigned long long* nt,
-                 unsigned long long* count_out) {
-    if (bulk) k_compact<T, MODE, true><<<grid, kBlock, 0, s>>>(in, out, n, p, ts, nt, count_out);
-    else k_compact<T, MODE, false><<<grid, kBlock, 0, s>>>(in, out, n, p, ts, nt, count_out);
+                 unsigned long long* count_out, uint32_t* counters) {
+    static const bool persistent = getenv("PARALLAX_PERSISTENT_TILES") != nullptr;
+    if (bulk && !persistent) {
+        if (!smem_opt_in<k_compact<T, MODE, true>>(Shape<T>::SMEM))
+            return cuda_ok(cudaGetLastError(), "k_compact shared-memory opt-in");
+        k_compact<T, MODE, true><<<(unsigned)tiles, kBlock, Shape<T>::SMEM, s>>>(
+            in, out, n, p, ts, nt, count_out);
+        return true;
+    }
+    if (bulk) {
+        constexpr size_t smem = 2 * Shape<T>::SMEM;
+        if (!smem_opt_in<k_compact_persistent<T, MODE>>(smem))
+            return cuda_ok(cudaGetLastError(), "k_compact_persistent shared-memory opt-in");
+        uint64_t grid = 2ull * device_info().sm_count;
+        if (grid > tiles) grid = tiles;
+        k_compact_persistent<T, MODE><<<(unsigned)grid, kBlock, smem, s>>>(
+            in, out, n, tiles, p, ts, nt, count_out, counters);
+        return true;
+    }
+    if (!smem_opt_in<k_compact<T, MODE, false>>(Shape<T>::SMEM))
+        return cuda_ok(cudaGetLastError(), "k_compact shared-memory opt-in");
+    k_compact<T, MODE, false><<<(unsigned)tiles, kBlock, Shape<T>::SMEM, s>>>(in, out, n, p, ts,
+                                                                              nt, count_out);
+    return true;
 }
 
 template <typename T>
@@ -241,23 +387,25 @@ bool compact_typed(Workspace& ws, CompactMode mode, const Pred& pr, const void* 
     T* out = static_cast<T*>(d_out);
     auto* cnt_out = reinterpret_cast<unsigned long long*>(d_count);
     PredDev<T> p = make_pred<T>(pr);
-    dim3 grid((unsigned)tiles);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(scratch + ScratchOff::counters);
     cudaStream_t s = ws.stream();
     // profile bytes: input read (+ the kept elements written, known only on the device)
     ProfScope prof(ws, mode == CompactMode::PARTITION ? "k_partition"
                        : mode == CompactMode::UNIQUE ? "k_unique" : "k_copy_if",
                    (mode == CompactMode::PARTITION ? 2 : 1) * n * sizeof(T));
+    bool ok = false;
     switch (mode) {
         case CompactMode::SELECT:
-            launch_mode<T, 0>(grid, s, bulk, in, out, n, p, ts, nt, cnt_out);
+            ok = launch_mode<T, 0>(tiles, s, bulk, in, out, n, p, ts, nt, cnt_out, counters);
             break;
         case CompactMode::UNIQUE:
-            launch_mode<T, 1>(grid, s, bulk, in, out, n, p, ts, nt, cnt_out);
+            ok = launch_mode<T, 1>(tiles, s, bulk, in, out, n, p, ts, nt, cnt_out, counters);
             break;
         case CompactMode::PARTITION:
-            launch_mode<T, 2>(grid, s, bulk, in, out, n, p, ts, nt, cnt_out);
+            ok = launch_mode<T, 2>(tiles, s, bulk, in, out, n, p, ts, nt, cnt_out, counters);
             break;
     }
+    if (!ok) return false;
     count_launch();
     return cuda_ok(cudaGetLastError(), "k_compact launch");
 }

@@ -6,14 +6,16 @@
 // shaders/scan_add.comp:14-19); exclusive adds a shift pass writing
 // out[i] = init + incl[i-1] (kernel_launcher.cpp:1346-1475).
 //
-// Here: one launch, one CTA per tile, in blockIdx order. Each CTA
-//   1. stages its tile (256 threads x 3 x 16 bytes = 12 KiB) in shared memory with one
-//      bulk copy (cp.async.bulk + mbarrier),
-//   2. scans 12 (4-byte) or 6 (8-byte) consecutive elements per thread in registers
+// Here: one launch, one CTA per 48 KiB tile, in blockIdx order. Each CTA
+//   1. stages its tile as four 12 KiB sub-tiles (256 threads x 3 x 16 bytes), one bulk
+//      copy (cp.async.bulk) and one mbarrier each, so 48 KiB per CTA are in flight at once
+//      and work starts when the first sub-tile lands (tiles.cuh),
+//   2. sums 12 (4-byte) or 6 (8-byte) consecutive elements per thread per sub-tile
 //      (rows of 48 bytes: conflict-free 128-bit shared loads),
-//   3. scans thread totals with warp shuffles and warp totals in one warp,
+//   3. scans row totals with warp shuffles and the 32 (sub-tile, warp) totals in one warp,
 //   4. gets the tile's exclusive prefix by decoupled look-back (lookback.cuh),
-//   5. writes results into the staged tile and stores it with one bulk copy.
+//   5. rescans each row, writes results into the staged tile and stores it with one bulk
+//      copy.
 // HBM traffic is the algorithmic minimum: n*s read + n*s written.
 // Accumulation: fp32 data is scanned per thread in fp32 (12 terms) and carried across
 // threads, warps and tiles in fp64; integers wrap around in their unsigned type.
@@ -24,6 +26,7 @@
 
 #include "../lookback.cuh"
 #include "../runtime.hpp"
+#include "../tiles.cuh"
 #include "../tma.cuh"
 
 namespace pxb {
@@ -40,94 +43,89 @@ template <> struct ScanTypes<uint32_t> { using L = uint32_t; using A = uint32_t;
 template <> struct ScanTypes<int64_t> { using L = uint64_t; using A = uint64_t; };
 template <> struct ScanTypes<uint64_t> { using L = uint64_t; using A = uint64_t; };
 
+constexpr int kSub = 4;   // sub-tiles per look-back tile; kSub x 8 warps = 32 lanes
+
 template <typename T>
 struct ScanShape {
     static constexpr int V = 16 / sizeof(T);
-    static constexpr int ITEMS = kVpt * V;
-    static constexpr int TILE = kBlock * ITEMS;
+    static constexpr int ITEMS = kVpt * V;          // elements per thread per sub-tile
+    static constexpr int SUB = kBlock * ITEMS;      // 12 KiB sub-tile
+    static constexpr int TILE = kSub * SUB;         // 48 KiB look-back tile
+    static constexpr size_t SMEM = TILE * sizeof(T);
 };
 
+// Phase 1 sums each thread's 48-byte row of every sub-tile as soon as that sub-tile lands;
+// one 32-lane scan over the (sub-tile, warp) totals - in element order - gives every
+// warp's offset and the tile aggregate; warp 0 runs the look-back. Phase 2 re-reads each
+// row from shared memory, scans it and writes the results in place. The caller has
+// staged the tile (bulk part arriving on bars[] with `parity`, ragged part filled) and
+// stores it afterwards.
 template <typename T, bool EXCL, bool BULK>
-__global__ void __launch_bounds__(kBlock)
-k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan)
-       typename ScanTypes<T>::A init, TileStatus<typename ScanTypes<T>::A> ts) {
+__device__ __forceinline__ void scan_tile(T* buf, uint64_t* bars, uint32_t parity,
+                                          typename ScanTypes<T>::A* s_tot, uint64_t tile,
+                                          typename ScanTypes<T>::A init,
+                                          const TileStatus<typename ScanTypes<T>::A>& ts,
+                                          typename ScanTypes<T>::A* red, int* first) {
     using L = typename ScanTypes<T>::L;
     using A = typename ScanTypes<T>::A;
     constexpr int V = ScanShape<T>::V;
     constexpr int ITEMS = ScanShape<T>::ITEMS;
-    constexpr int TILE = ScanShape<T>::TILE;
-    __shared__ __align__(128) T buf[TILE];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ A s_warp[kBlock / 32];
-
+    constexpr int SUB = ScanShape<T>::SUB;
+    constexpr int WARPS = kBlock / 32;
+    static_assert(kSub * WARPS == 32, "one lane per (sub-tile, warp)");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint64_t tile = blockIdx.x;
-    const uint64_t base = tile * (uint64_t)TILE;
-    const uint64_t rem = n - base;
-    const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
 
-    uint32_t bulk = 0;  // elements moved by the bulk copies
-    if constexpr (BULK) {
-        bulk = (uint32_t)((cnt * sizeof(T)) / 16 * 16 / sizeof(T));
-        if (tid == 0) {
-            mbar_init(&bar, 1);
-            fence_mbar_init();
-            mbar_arrive_expect_tx(&bar, bulk * (uint32_t)sizeof(T));
-            if (bulk) bulk_load(buf, in + base, bulk * (uint32_t)sizeof(T), &bar);
-        }
-    }
-    // ragged end of the last tile (and everything when not bulk-aligned): plain loads
-    for (uint32_t e = bulk + tid; e < (uint32_t)TILE; e += kBlock)
-        buf[e] = e < cnt ? in[base + e] : T(0);
-    __syncthreads();
-    if constexpr (BULK) {
-        uint32_t spins = 0;
-        while (!mbar_try_wait(&bar, 0)) {
-            if (++spins > kSpinLimit) {
-                *ts.err = 2;
-                break;
-            }
-        }
-    }
-
-    // ---- per-thread scan of ITEMS consecutive elements ----
-    L x[ITEMS];
-    {
-        const uint4* row = reinterpret_cast<const uint4*>(buf + tid * ITEMS);
+    // ---- phase 1: row totals of every sub-tile ----
+    A tex[kSub];  // exclusive prefix of this thread's row within its warp, per sub-tile
+#pragma unroll
+    for (int s = 0; s < kSub; ++s) {
+        if constexpr (BULK) wait_bar(&bars[s], parity, ts.err);
+        const uint4* row = reinterpret_cast<const uint4*>(buf + s * SUB + tid * ITEMS);
+        L sum = L(0);
 #pragma unroll
         for (int v = 0; v < kVpt; ++v) {
-            uint4 r = row[v];
+            const uint4 r = row[v];
+            const T* e = reinterpret_cast<const T*>(&r);
+#pragma unroll
+            for (int k = 0; k < V; ++k) sum = sum + (L)e[k];
+        }
+        const A incl = warp_inclusive_scan((A)sum, OpSum());
+        const A ex = shfl_up(incl, 1);
+        tex[s] = lane == 0 ? A(0) : ex;
+        if (lane == 31) s_tot[s * WARPS + warp] = incl;
+    }
+    __syncthreads();
+    // Every warp scans the 32 (sub-tile, warp) totals itself (identical shuffle sequence,
+    // identical result), then the whole CTA runs the look-back.
+    A woff[kSub];  // offset of this warp's rows within the tile, per sub-tile
+    A agg;
+    {
+        const A v = s_tot[lane];
+        const A vi = warp_inclusive_scan(v, OpSum());
+        agg = shfl_idx(vi, 31);
+        A vex = shfl_up(vi, 1);
+        if (lane == 0) vex = A(0);
+#pragma unroll
+        for (int s = 0; s < kSub; ++s) woff[s] = shfl_idx(vex, s * WARPS + warp);
+    }
+    const A prefix = lookback_cta<A, kBlock>(ts, tile, agg, red, first);
+
+    // ---- phase 2: scan each row and write the results in place ----
+#pragma unroll
+    for (int s = 0; s < kSub; ++s) {
+        A tb = (prefix + woff[s]) + tex[s];
+        if constexpr (EXCL) tb = init + tb;
+        uint4* row = reinterpret_cast<uint4*>(buf + s * SUB + tid * ITEMS);
+        L x[ITEMS];
+#pragma unroll
+        for (int v = 0; v < kVpt; ++v) {
+            const uint4 r = row[v];
             const T* e = reinterpret_cast<const T*>(&r);
 #pragma unroll
             for (int k = 0; k < V; ++k) x[v * V + k] = (L)e[k];
         }
-    }
 #pragma unroll
-    for (int j = 1; j < ITEMS; ++j) x[j] = x[j - 1] + x[j];
-
-    // ---- warp and block scan of thread totals ----
-    const A tot = (A)x[ITEMS - 1];
-    const A incl = warp_inclusive_scan(tot, OpSum());
-    A texcl = shfl_up(incl, 1);
-    if (lane == 0) texcl = A(0);
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        const A w = lane < kBlock / 32 ? s_warp[lane] : A(0);
-        const A wi = warp_inclusive_scan(w, OpSum());
-        const A agg = shfl_idx(wi, kBlock / 32 - 1);
-        A wex = shfl_up(wi, 1);
-        if (lane == 0) wex = A(0);
-        const A prefix = lookback(ts, tile, agg);
-        if (lane < kBlock / 32) s_warp[lane] = prefix + wex;
-    }
-    __syncthreads();
-    A tb = s_warp[warp] + texcl;
-    if constexpr (EXCL) tb = init + tb;
-
-    // ---- results back into the staged tile ----
-    {
-        uint4* row = reinterpret_cast<uint4*>(buf + tid * ITEMS);
+        for (int j = 1; j < ITEMS; ++j) x[j] = x[j - 1] + x[j];
 #pragma unroll
         for (int v = 0; v < kVpt; ++v) {
             uint4 r;
@@ -143,6 +141,31 @@ k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan
     }
     if constexpr (BULK) fence_proxy_async_smem();
     __syncthreads();
+}
+
+// One CTA per 48 KiB tile, in blockIdx order: unaligned operands (BULK = false) and the
+// allocation-free entry point.
+template <typename T, bool EXCL, bool BULK>
+__global__ void __launch_bounds__(kBlock, 4)
+k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan)
+       typename ScanTypes<T>::A init, TileStatus<typename ScanTypes<T>::A> ts) {
+    using A = typename ScanTypes<T>::A;
+    constexpr int SUB = ScanShape<T>::SUB;
+    constexpr int TILE = ScanShape<T>::TILE;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* buf = reinterpret_cast<T*>(smem_raw);
+    __shared__ __align__(8) uint64_t bars[kSub];
+    __shared__ A s_tot[32];
+    __shared__ A s_red[kBlock / 32 + 1];
+    __shared__ int s_first[kBlock / 32];
+    const int tid = threadIdx.x;
+    const uint64_t tile = blockIdx.x;
+    const uint64_t base = tile * (uint64_t)TILE;
+    const uint64_t rem = n - base;
+    const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+    const uint32_t bulk = stage_tile<T, SUB, kSub, kBlock, BULK>(buf, bars, in, base, cnt);
+    __syncthreads();
+    scan_tile<T, EXCL, BULK>(buf, bars, 0, s_tot, tile, init, ts, s_red, s_first);
     if constexpr (BULK) {
         if (tid == 0 && bulk) {
             bulk_store(out + base, buf, bulk * (uint32_t)sizeof(T));
@@ -151,8 +174,108 @@ k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan
     }
     for (uint32_t e = bulk + tid; e < cnt; e += kBlock) out[base + e] = buf[e];
     if constexpr (BULK) {
-        if (tid == 0 && bulk) bulk_wait_all();
+        if (tid == 0 && bulk) bulk_wait_read_all();
     }
+}
+
+// Persistent CTAs (two per SM) with two tile buffers each: the bulk copies of the next
+// claimed tile fill one buffer while the current tile is scanned out of the other, so
+// every SM keeps ~96 KiB of loads in flight. Operands 16-byte aligned.
+template <typename T, bool EXCL>
+__global__ void __launch_bounds__(kBlock, 2)
+k_scan_persistent(const T* in, T* out, uint64_t n, uint64_t num_tiles,
+                  typename ScanTypes<T>::A init, TileStatus<typename ScanTypes<T>::A> ts,
+                  uint32_t* counters) {
+    using A = typename ScanTypes<T>::A;
+    constexpr int SUB = ScanShape<T>::SUB;
+    constexpr int TILE = ScanShape<T>::TILE;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* const buf0 = reinterpret_cast<T*>(smem_raw);  // buffer b at buf0 + b * TILE
+    __shared__ __align__(8) uint64_t bars[2][kSub];
+    __shared__ A s_tot[32];
+    __shared__ A s_red[kBlock / 32 + 1];
+    __shared__ int s_first[kBlock / 32];
+    __shared__ uint32_t s_tile[2];
+    const int tid = threadIdx.x;
+
+    if (tid == 0) {
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int s = 0; s < kSub; ++s) mbar_init(&bars[b][s], 1);
+        fence_mbar_init();
+        const uint32_t t0 = atomicAdd(&counters[0], 1u);
+        s_tile[0] = t0;
+        if (t0 < num_tiles) {
+            const uint64_t base = (uint64_t)t0 * TILE;
+            const uint64_t rem = n - base;
+            issue_tile<T, SUB, kSub>(buf0, bars[0], in, base,
+                                     rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE);
+        }
+    }
+    __syncthreads();
+    for (uint32_t it = 0;; ++it) {
+        const int b = it & 1;
+        const uint32_t parity = (it >> 1) & 1u;
+        const uint32_t cur = s_tile[b];
+        if (cur >= num_tiles) break;
+        if (tid == 0) {  // prefetch: claim the next tile and start its copies
+            bulk_wait_read_all();  // the previous tile's store has left the other buffer
+            fence_proxy_async_smem();
+            const uint32_t nxt = atomicAdd(&counters[0], 1u);
+            s_tile[b ^ 1] = nxt;
+            if (nxt < num_tiles) {
+                const uint64_t nbase = (uint64_t)nxt * TILE;
+                const uint64_t nrem = n - nbase;
+                issue_tile<T, SUB, kSub>(buf0 + (size_t)(b ^ 1) * TILE, bars[b ^ 1], in, nbase,
+                                         nrem < (uint64_t)TILE ? (uint32_t)nrem : (uint32_t)TILE);
+            }
+        }
+        T* buf = buf0 + (size_t)b * TILE;
+        const uint64_t base = (uint64_t)cur * TILE;
+        const uint64_t rem = n - base;
+        const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+        const uint32_t bulk = bulk_elems<T>(cnt);
+        if (cnt < (uint32_t)TILE || bulk < cnt) {  // the last tile: ragged end and padding
+            fill_ragged<T, TILE, kBlock>(buf, in, base, cnt, bulk);
+            __syncthreads();
+        }
+        scan_tile<T, EXCL, true>(buf, bars[b], parity, s_tot, cur, init, ts, s_red, s_first);
+        if (tid == 0 && bulk) {
+            bulk_store(out + base, buf, bulk * (uint32_t)sizeof(T));
+            bulk_commit();
+        }
+        for (uint32_t e = bulk + tid; e < cnt; e += kBlock) out[base + e] = buf[e];
+        __syncthreads();  // s_tile / s_tot / plain reads of buf done before the next round
+    }
+    if (tid == 0) {
+        bulk_wait_read_all();
+        persistent_exit(counters);
+    }
+}
+
+template <typename T, bool EXCL, bool BULK>
+bool launch_tiles_single(const T* in, T* out, uint64_t n, typename ScanTypes<T>::A init,
+                         TileStatus<typename ScanTypes<T>::A> ts, uint64_t tiles,
+                         cudaStream_t s) {
+    if (!smem_opt_in<k_scan<T, EXCL, BULK>>(ScanShape<T>::SMEM))
+        return cuda_ok(cudaGetLastError(), "k_scan shared-memory opt-in");
+    k_scan<T, EXCL, BULK><<<(unsigned)tiles, kBlock, ScanShape<T>::SMEM, s>>>(in, out, n, init, ts);
+    return true;
+}
+
+template <typename T, bool EXCL>
+bool launch_tiles_persistent(const T* in, T* out, uint64_t n, typename ScanTypes<T>::A init,
+                             TileStatus<typename ScanTypes<T>::A> ts, uint64_t tiles,
+                             uint32_t* counters, cudaStream_t s) {
+    constexpr size_t smem = 2 * ScanShape<T>::SMEM;
+    if (!smem_opt_in<k_scan_persistent<T, EXCL>>(smem))
+        return cuda_ok(cudaGetLastError(), "k_scan_persistent shared-memory opt-in");
+    uint64_t grid = 2ull * device_info().sm_count;
+    if (grid > tiles) grid = tiles;
+    k_scan_persistent<T, EXCL><<<(unsigned)grid, kBlock, smem, s>>>(in, out, n, tiles, init, ts,
+                                                                     counters);
+    return true;
 }
 
 template <typename T>
@@ -179,16 +302,21 @@ bool scan_typed(Workspace& ws, bool exclusive, const void* d_in, void* d_out, ui
                       (reinterpret_cast<uintptr_t>(d_out) % 16 == 0);
     const T* in = static_cast<const T*>(d_in);
     T* out = static_cast<T*>(d_out);
-    dim3 grid((unsigned)tiles);
     cudaStream_t s = ws.stream();
     ProfScope prof(ws, exclusive ? "k_scan_exclusive" : "k_scan_inclusive", 2 * n * sizeof(T));
+    uint32_t* counters = reinterpret_cast<uint32_t*>(scratch + ScratchOff::counters);
+    static const bool persistent = getenv("PARALLAX_PERSISTENT_TILES") != nullptr;
+    bool ok;
     if (exclusive) {
-        if (bulk) k_scan<T, true, true><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
-        else k_scan<T, true, false><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
+        ok = !bulk ? launch_tiles_single<T, true, false>(in, out, n, init, ts, tiles, s)
+           : persistent ? launch_tiles_persistent<T, true>(in, out, n, init, ts, tiles, counters, s)
+                        : launch_tiles_single<T, true, true>(in, out, n, init, ts, tiles, s);
     } else {
-        if (bulk) k_scan<T, false, true><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
-        else k_scan<T, false, false><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
+        ok = !bulk ? launch_tiles_single<T, false, false>(in, out, n, init, ts, tiles, s)
+           : persistent ? launch_tiles_persistent<T, false>(in, out, n, init, ts, tiles, counters, s)
+                        : launch_tiles_single<T, false, true>(in, out, n, init, ts, tiles, s);
     }
+    if (!ok) return false;
     count_launch();
     return cuda_ok(cudaGetLastError(), "k_scan launch");
 }
@@ -265,14 +393,15 @@ bool noalloc_launch(const void* d_in, void* d_out, uint64_t n, const void* init_
                       (reinterpret_cast<uintptr_t>(d_out) % 16 == 0);
     const T* in = static_cast<const T*>(d_in);
     T* out = static_cast<T*>(d_out);
-    dim3 grid((unsigned)tiles);
+    bool ok;
     if (init_host) {
-        if (bulk) k_scan<T, true, true><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
-        else k_scan<T, true, false><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
+        ok = bulk ? launch_tiles_single<T, true, true>(in, out, n, init, ts, tiles, s)
+                  : launch_tiles_single<T, true, false>(in, out, n, init, ts, tiles, s);
     } else {
-        if (bulk) k_scan<T, false, true><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
-        else k_scan<T, false, false><<<grid, kBlock, 0, s>>>(in, out, n, init, ts);
+        ok = bulk ? launch_tiles_single<T, false, true>(in, out, n, init, ts, tiles, s)
+                  : launch_tiles_single<T, false, false>(in, out, n, init, ts, tiles, s);
     }
+    if (!ok) return false;
     count_launch();
     return cuda_ok(cudaGetLastError(), "parallax_scan_noalloc launch");
 }

@@ -115,6 +115,82 @@ __device__ __forceinline__ A lookback(const TileStatus<A>& ts, uint64_t tile, A 
     return excl;
 }
 
+// CTA-wide look-back: called by ALL threads of a CTA of BLOCK threads (a multiple of 32),
+// with the tile aggregate in every thread. Each round, every thread inspects one
+// predecessor (tile - 1 - tid - round offset), so one round trip to L2 covers BLOCK
+// predecessors instead of 32: when hundreds of resident tiles stand between a tile and the
+// nearest published inclusive prefix, this takes a couple of round trips instead of ten.
+// `red` is shared scratch of at least BLOCK / 32 + 1 elements of A and `first` of BLOCK / 32
+// ints. Returns the exclusive prefix in every thread; the same contribution order for the
+// same status pattern, so integer results are exact and fp results deterministic given the
+// pattern.
+template <typename A, int BLOCK>
+__device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile, A agg, A* red,
+                                          int* first) {
+    constexpr int WARPS = BLOCK / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t ep = (ts.epoch & 0x3fffffffu) << 2;
+    if (tile == 0) {
+        if (tid == 0) {
+            put_val(&ts.e[0].inc, agg);
+            st_release_u32(&ts.e[0].flag, ep | 2u);
+        }
+        return A(0);
+    }
+    if (tid == 0) {
+        put_val(&ts.e[tile].agg, agg);
+        st_release_u32(&ts.e[tile].flag, ep | 1u);
+    }
+    A excl = A(0);
+    int64_t pred = (int64_t)tile - 1;
+    for (;;) {
+        const int64_t idx = pred - tid;
+        uint32_t state = 2u;
+        A v = A(0);
+        if (idx >= 0) {
+            uint32_t f = 0, spins = 0;
+            bool gave_up = false;
+            for (;;) {
+                f = ld_acquire_u32(&ts.e[idx].flag);
+                if ((f & ~3u) == ep && (f & 3u) != 0u) break;
+                if (++spins > kSpinLimit) {
+                    *ts.err = 1;
+                    gave_up = true;
+                    break;
+                }
+                if (spins > 16) nanosleep_ns(64);
+            }
+            if (!gave_up) {
+                state = f & 3u;
+                v = state == 2u ? get_val<A>(&ts.e[idx].inc) : get_val<A>(&ts.e[idx].agg);
+            }
+        }
+        // nearest inclusive prefix = the lowest thread index holding one
+        const unsigned m = __ballot_sync(0xffffffffu, state == 2u);
+        if (lane == 0) first[warp] = m ? warp * 32 + __ffs(m) - 1 : BLOCK;
+        __syncthreads();
+        int nearest = BLOCK;
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) nearest = min(nearest, first[w]);
+        A c = tid <= nearest ? v : A(0);
+        c = warp_reduce(c, OpSum());
+        if (lane == 0) red[warp] = c;
+        __syncthreads();
+        A round = A(0);
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) round = round + red[w];
+        excl = round + excl;
+        __syncthreads();  // red / first reusable
+        if (nearest < BLOCK) break;
+        pred -= BLOCK;
+    }
+    if (tid == 0) {
+        put_val(&ts.e[tile].inc, excl + agg);
+        st_release_u32(&ts.e[tile].flag, ep | 2u);
+    }
+    return excl;
+}
+
 // Status entries live after the small scratch region.
 template <typename A>
 inline TileStatus<A> tile_status_at(char* scratch, uint32_t epoch, int32_t* err) {

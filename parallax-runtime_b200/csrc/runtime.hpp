@@ -71,6 +71,7 @@ constexpr size_t kScratchSmall = 64 << 10;
 struct ScratchOff {
     static constexpr size_t ticket = 0;        // reduce last-block ticket (self-resetting)
     static constexpr size_t num_true = 256;    // partition: count of the count pass
+    static constexpr size_t counters = 512;    // persistent launches: tile claim / exit (self-resetting)
     static constexpr size_t partials = 1024;   // reduce per-block partials (<= 48 KiB)
 };
 

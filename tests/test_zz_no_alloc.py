@@ -22,7 +22,7 @@ from cases import F32_TOL, F64_TOL
 pytestmark = pytest.mark.gpu
 
 MAX_TILES = 24576
-TILE = {4: 3072, 8: 1536}  # elements per look-back tile of the scan kernel
+TILE = {4: 12288, 8: 6144}  # elements per look-back tile of the scan kernel (48 KiB)
 
 
 def gen(ox, t, n, seed):
