@@ -87,6 +87,32 @@ int parallax_set_async(int async);
 int parallax_synchronize(void);
 size_t parallax_last_count(void);
 
+/* ---- segmented primitives (batching) --------------------------------------------- */
+/* No counterpart in the reference. `offsets` holds num_segments + 1 element offsets
+ * (offsets[0] = 0, offsets[num_segments] = count) cutting `data` into segments; all
+ * operands are DEVICE pointers (or PARALLAX_DEVICE_RESIDENT arena blocks). Each call is
+ * one persistent launch over a tile work list (plus a one-CTA planner), tile shape
+ * chosen by an autotuner on first use, captured as a CUDA graph per argument set and
+ * replayed afterwards. Return a parallax_status; synchronous unless async mode is on.
+ *   reduce: results[s] = sum of segment s (0 for an empty segment); reduce:sum handle.
+ *   exclusive_scan: per segment, output[i] = init + sum of the segment's earlier
+ *     elements; scan handle.
+ *   copy_if: the kept elements of segment s are written, in order, to
+ *     output[offsets[s] ...]; counts[s] = how many; copy_if / remove_if handle with a
+ *     comparison predicate.
+ *   sort: each segment sorted ascending in place (sort:<dtype> handle), or 8-byte
+ *     (key << 32 | value) records sorted stably by key (sort_kv:u32 handle). */
+int parallax_segmented_reduce(parallax_kernel_t kernel, const void* data, size_t count,
+                              const uint64_t* offsets, size_t num_segments, void* results);
+int parallax_segmented_exclusive_scan(parallax_kernel_t kernel, const void* input,
+                                      void* output, size_t count, const uint64_t* offsets,
+                                      size_t num_segments, const void* init);
+int parallax_segmented_copy_if(parallax_kernel_t kernel, const void* input, void* output,
+                               size_t count, const uint64_t* offsets, size_t num_segments,
+                               uint64_t* counts);
+int parallax_segmented_sort(parallax_kernel_t kernel, void* data, size_t count,
+                            const uint64_t* offsets, size_t num_segments);
+
 /* ---- allocation-free scan -------------------------------------------------------- */
 /* No counterpart in the reference. For callers that cannot allocate device memory: code
  * running inside an allocation hook (a malloc / operator new interposer that routes the

@@ -183,3 +183,52 @@ def max_rel_err(got: np.ndarray, want: np.ndarray, floor: float = 0.0) -> float:
     den = np.maximum(np.abs(w), floor) if floor else np.abs(w)
     den = np.where(den == 0, 1.0, den)
     return float(np.max(np.abs(g - w) / den)) if g.size else 0.0
+
+
+# ---- segmented primitives -----------------------------------------------------------------------
+# Each applies the per-array oracle above to every segment [offsets[s], offsets[s+1]) of x:
+# the per-segment contract is exactly the reference primitive's (stdpar.hpp:146-148 reduce,
+# :237-238 exclusive_scan, :319-321 copy_if, :178 sort).
+def seg_sum(x: np.ndarray, offsets: np.ndarray) -> np.ndarray:
+    """Per-segment sums: float64 (compensated) for fp inputs, wrapped x.dtype for integers;
+    empty segments give 0."""
+    S = offsets.size - 1
+    fp = x.dtype.kind == "f"
+    out = np.zeros(S, dtype=np.float64 if fp else x.dtype)
+    for s in range(S):
+        a, b = int(offsets[s]), int(offsets[s + 1])
+        if b > a:
+            out[s] = reduce_sum(x[a:b])
+    return out
+
+
+def seg_exscan(x: np.ndarray, offsets: np.ndarray, init=0) -> np.ndarray:
+    """Per-segment exclusive scans, each starting at init (float64 for fp inputs)."""
+    fp = x.dtype.kind == "f"
+    out = np.zeros(x.size, dtype=np.float64 if fp else x.dtype)
+    for s in range(offsets.size - 1):
+        a, b = int(offsets[s]), int(offsets[s + 1])
+        if b > a:
+            out[a:b] = scan(x[a:b], exclusive=True, init=init)
+    return out
+
+
+def seg_copy_if(x: np.ndarray, offsets: np.ndarray, kind: int, c=0.0,
+                remove: bool = False) -> tuple[list[np.ndarray], np.ndarray]:
+    """Kept elements of every segment (in order) and the kept counts."""
+    kept, counts = [], np.zeros(offsets.size - 1, dtype=np.uint64)
+    for s in range(offsets.size - 1):
+        a, b = int(offsets[s]), int(offsets[s + 1])
+        out, k = compact(x[a:b], REMOVE_IF if remove else COPY_IF, kind, c)
+        kept.append(out[:k])
+        counts[s] = k
+    return kept, counts
+
+
+def seg_sort(x: np.ndarray, offsets: np.ndarray) -> np.ndarray:
+    y = x.copy()
+    for s in range(offsets.size - 1):
+        a, b = int(offsets[s]), int(offsets[s + 1])
+        if b - a > 1:
+            y[a:b] = sort(x[a:b])
+    return y

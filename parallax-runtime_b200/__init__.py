@@ -88,6 +88,10 @@ _SIGNATURES = {
     "parallax_profile_json": (sz, [C.c_char_p, sz]),
     "parallax_profile_reset": (None, []),
     "parallax_scan_noalloc": (C.c_int, [vp, vp, vp, sz, sz, vp, vp]),
+    "parallax_segmented_reduce": (C.c_int, [vp, vp, sz, vp, sz, vp]),
+    "parallax_segmented_exclusive_scan": (C.c_int, [vp, vp, vp, sz, vp, sz, vp]),
+    "parallax_segmented_copy_if": (C.c_int, [vp, vp, vp, sz, vp, sz, vp]),
+    "parallax_segmented_sort": (C.c_int, [vp, vp, sz, vp, sz]),
     "parallax_device_info": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p, sz]),
 }
 

@@ -9,6 +9,10 @@
 
 namespace pxb {
 
+// Mapped error-word code of the segment planner: offsets not non-decreasing within
+// [0, count] (in-kernel wait timeouts use small positive codes).
+constexpr int32_t kErrSegmentOffsets = 0x5e90;
+
 enum class DType : int { F32 = 0, F64 = 1, I32 = 2, I64 = 3, U32 = 4, U64 = 5, INVALID = -1 };
 
 inline __host__ __device__ size_t dtype_size(DType t) {

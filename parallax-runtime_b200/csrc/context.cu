@@ -143,7 +143,82 @@ char* Workspace::scratch(uint64_t tiles) {
     if (!cuda_ok(cudaMemsetAsync(d_scratch, 0, cap, s), "cudaMemset(scratch)")) return nullptr;
     scratch_cap = cap;
     epoch = 1;
+    ++generation;
     return static_cast<char*>(d_scratch);
+}
+
+void* Workspace::seg(size_t bytes) {
+    if (bytes <= seg_cap) return d_seg;
+    cudaStream_t s = stream();
+    if (d_seg) {
+        if (!cuda_ok(cudaStreamSynchronize(s), "segment buffer sync")) return nullptr;
+        cudaFree(d_seg);
+        d_seg = nullptr;
+        seg_cap = 0;
+    }
+    size_t cap = 1 << 20;
+    while (cap < bytes) cap <<= 1;
+    if (!cuda_ok(cudaMalloc(&d_seg, cap), "cudaMalloc(segment buffer)")) return nullptr;
+    if (!cuda_ok(cudaMemsetAsync(d_seg, 0, cap, s), "cudaMemset(segment buffer)")) return nullptr;
+    seg_cap = cap;
+    ++generation;
+    return d_seg;
+}
+
+void* Workspace::seg_status(uint64_t entries) {
+    if (entries <= seg_status_cap) return d_seg_status;
+    cudaStream_t s = stream();
+    if (d_seg_status) {
+        if (!cuda_ok(cudaStreamSynchronize(s), "segment status sync")) return nullptr;
+        cudaFree(d_seg_status);
+        d_seg_status = nullptr;
+        seg_status_cap = 0;
+    }
+    uint64_t cap = 1 << 14;
+    while (cap < entries) cap <<= 1;
+    if (!cuda_ok(cudaMalloc(&d_seg_status, cap * kStatusEntry), "cudaMalloc(segment status)"))
+        return nullptr;
+    if (!cuda_ok(cudaMemsetAsync(d_seg_status, 0, cap * kStatusEntry, s), "cudaMemset(segment status)"))
+        return nullptr;
+    seg_status_cap = cap;
+    ++generation;
+    return d_seg_status;
+}
+
+bool graph_launch(Workspace& ws, const std::string& key, const std::function<bool()>& enqueue) {
+    static const bool enabled =
+        !(getenv("PARALLAX_GRAPHS") && atoi(getenv("PARALLAX_GRAPHS")) == 0);
+    if (!enabled || ws.user_stream) return enqueue();
+    cudaStream_t s = ws.stream();
+    auto it = ws.graphs.find(key);
+    if (it != ws.graphs.end() && it->second.first != ws.generation) {
+        cudaGraphExecDestroy(it->second.second);
+        ws.graphs.erase(it);
+        it = ws.graphs.end();
+    }
+    if (it == ws.graphs.end()) {
+        const uint64_t gen = ws.generation;
+        cudaGraph_t g = nullptr;
+        if (!cuda_ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture"))
+            return false;
+        const bool ok = enqueue();
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (!ok || !cuda_ok(e, "end capture")) {
+            if (g) cudaGraphDestroy(g);
+            return false;
+        }
+        if (ws.generation != gen) {  // a buffer moved during capture: cannot cache this graph
+            cudaGraphDestroy(g);
+            set_error(PARALLAX_ERR_CUDA, "workspace buffer reallocated during graph capture");
+            return false;
+        }
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (!cuda_ok(e, "graph instantiate")) return false;
+        it = ws.graphs.emplace(key, std::make_pair(gen, exec)).first;
+    }
+    return cuda_ok(cudaGraphLaunch(it->second.second, s), "graph launch");
 }
 
 void* Workspace::temp(size_t bytes) {
@@ -159,6 +234,7 @@ void* Workspace::temp(size_t bytes) {
     while (cap < bytes) cap <<= 1;
     if (!cuda_ok(cudaMalloc(&d_temp, cap), "cudaMalloc(temp)")) return nullptr;
     temp_cap = cap;
+    ++generation;
     return d_temp;
 }
 
@@ -175,6 +251,7 @@ void* Workspace::stage(int slot, size_t bytes) {
     while (cap < bytes) cap <<= 1;
     if (!cuda_ok(cudaMalloc(&d_stage[slot], cap), "cudaMalloc(stage)")) return nullptr;
     stage_cap[slot] = cap;
+    ++generation;
     return d_stage[slot];
 }
 
@@ -271,6 +348,11 @@ int sync_stream(Workspace& ws) {
     if (ws.h_slot->spin_error) {
         int code = ws.h_slot->spin_error;
         ws.h_slot->spin_error = 0;
+        if (code == kErrSegmentOffsets) {
+            set_error(PARALLAX_ERR_INVALID_ARGUMENT,
+                      "segment offsets must be non-decreasing and within [0, count]");
+            return PARALLAX_ERR_INVALID_ARGUMENT;
+        }
         set_error(PARALLAX_ERR_DEVICE_SPIN, "an in-kernel bounded wait gave up (code %d)", code);
         return PARALLAX_ERR_DEVICE_SPIN;
     }

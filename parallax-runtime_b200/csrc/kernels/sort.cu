@@ -18,8 +18,10 @@
 // the first load and its inverse into the last store. 8-byte records of the key-value
 // sort are (key << 32 | value) and sort as plain 64-bit keys, i.e. stably by key.
 #include <stdint.h>
+#include <stdio.h>
 
 #include "../runtime.hpp"
+#include "../segplan.cuh"
 
 namespace pxb {
 namespace {
@@ -300,6 +302,204 @@ bool sort_keys(Workspace& ws, void* d_data, uint64_t n) {
     return cuda_ok(cudaGetLastError(), "sort launch");
 }
 
+// ---- segmented sort ---------------------------------------------------------------------------
+// Work list from the planner with one item per TILE keys of a segment. A segment of m items
+// needs P = ceil(log2 m) merge passes; its tile sort writes to `data` when P is even and to
+// `tmp` when P is odd, and every pass flips the buffer, so each segment ends in `data`
+// after its own last pass with no extra copy. Passes beyond a segment's P skip it.
+__device__ __forceinline__ int passes_of(uint32_t m) {
+    int p = 0;
+    while ((1u << p) < m) ++p;
+    return p;
+}
+template <typename K>
+__device__ __forceinline__ K* seg_loc(K* data, K* tmp, int P, int q) {
+    return ((P - q) & 1) ? tmp : data;
+}
+
+struct SegGeom {
+    uint32_t seg, first, m, k;
+    uint64_t seg_off, seg_len;
+    int P;
+};
+__device__ __forceinline__ SegGeom seg_geom(const uint64_t* offsets, uint64_t S,
+                                            const uint32_t* item_start, uint32_t item) {
+    SegGeom g;
+    g.seg = find_segment(item_start, S, item);
+    g.first = item_start[g.seg];
+    g.m = item_start[g.seg + 1] - g.first;
+    g.k = item - g.first;
+    g.seg_off = offsets[g.seg];
+    g.seg_len = offsets[g.seg + 1] - g.seg_off;
+    g.P = passes_of(g.m);
+    return g;
+}
+
+template <typename K, int XF>
+__global__ void __launch_bounds__(kBlock)
+k_seg_tile_sort(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t S,
+                const uint32_t* __restrict__ item_start) {
+    constexpr int ITEMS = SortShape<K>::ITEMS;
+    constexpr int TILE = kBlock * ITEMS;
+    __shared__ K sm[TILE];
+    const uint32_t item = blockIdx.x;
+    if (item >= item_start[S]) return;
+    const SegGeom g = seg_geom(offsets, S, item_start, item);
+    const int t = threadIdx.x, lane = t & 31, row0 = t * ITEMS;
+    const uint64_t begin = g.seg_off + (uint64_t)g.k * TILE;
+    const uint64_t rem = g.seg_off + g.seg_len - begin;
+    const int cnt = rem < (uint64_t)TILE ? (int)rem : TILE;
+    K x[ITEMS];
+#pragma unroll
+    for (int r = 0; r < ITEMS; ++r)
+        x[r] = row0 + r < cnt ? to_key<K, XF>(data[begin + row0 + r]) : ~K(0);
+    bitonic_k<K, ITEMS, TILE, 2>(x, sm, t, lane, row0);
+    K* dst = seg_loc(data, tmp, g.P, 0);
+#pragma unroll
+    for (int r = 0; r < ITEMS; ++r)
+        if (row0 + r < cnt) dst[begin + row0 + r] = g.P == 0 ? from_key<K, XF>(x[r]) : x[r];
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kBlock)
+k_seg_merge_path(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t S,
+                 const uint32_t* __restrict__ item_start, int pass, uint64_t* __restrict__ splits) {
+    constexpr int TILE = kBlock * SortShape<K>::ITEMS;
+    const uint64_t wid = ((uint64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= item_start[S]) return;
+    const SegGeom g = seg_geom(offsets, S, item_start, (uint32_t)wid);
+    if (g.P < pass) return;
+    const K* src = seg_loc(data, tmp, g.P, pass - 1) + g.seg_off;
+    const uint64_t L = (uint64_t)TILE << (pass - 1);
+    const uint64_t o = (uint64_t)g.k * TILE;
+    const Pair p = pair_of(o, g.seg_len, L);
+    const uint64_t d = o - p.ps;
+    const K* A = src + p.ps;
+    const K* B = src + p.ps + p.la;
+    uint64_t lo = d > p.lb ? d - p.lb : 0;
+    uint64_t hi = d < p.la ? d : p.la;
+    while (hi - lo > 32) {
+        const uint64_t stride = (hi - lo + 31) / 32;
+        const uint64_t q = lo + (uint64_t)lane * stride;
+        const bool valid = q < hi;
+        const bool tr = valid && !(B[d - 1 - q] < A[q]);
+        const int c = __popc(__ballot_sync(0xffffffffu, tr));
+        const int nvalid = __popc(__ballot_sync(0xffffffffu, valid));
+        const uint64_t nlo = c ? lo + (uint64_t)(c - 1) * stride + 1 : lo;
+        const uint64_t nhi = c < nvalid ? lo + (uint64_t)c * stride : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    const uint64_t q = lo + lane;
+    const bool tr = q < hi && !(B[d - 1 - q] < A[q]);
+    const int c = __popc(__ballot_sync(0xffffffffu, tr));
+    if (lane == 0) splits[wid] = lo + c;
+}
+
+template <typename K, int XF>
+__global__ void __launch_bounds__(kBlock)
+k_seg_merge(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t S,
+            const uint32_t* __restrict__ item_start, int pass, const uint64_t* __restrict__ splits) {
+    constexpr int IPT = SortShape<K>::ITEMS;
+    constexpr int OT = kBlock * IPT;
+    __shared__ K sm[OT];
+    __shared__ K so[IPT * (kBlock + 1)];
+    const uint32_t item = blockIdx.x;
+    if (item >= item_start[S]) return;
+    const SegGeom g = seg_geom(offsets, S, item_start, item);
+    if (g.P < pass) return;
+    const bool final_pass = pass == g.P;
+    const K* src = seg_loc(data, tmp, g.P, pass - 1) + g.seg_off;
+    K* dst = seg_loc(data, tmp, g.P, pass) + g.seg_off;
+    const int t = threadIdx.x;
+    const uint64_t L = (uint64_t)OT << (pass - 1);
+    const uint64_t o = (uint64_t)g.k * OT;
+    const Pair p = pair_of(o, g.seg_len, L);
+    const uint64_t pair_end = p.ps + p.la + p.lb;
+    const uint64_t tile_end = o + OT < pair_end ? o + OT : pair_end;
+    const uint64_t d0 = o - p.ps, d1 = tile_end - p.ps;
+    const uint64_t a_s = splits[item];
+    const uint64_t a_e = o + OT < pair_end ? splits[item + 1] : p.la;
+    const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
+    const int na = (int)(a_e - a_s), nb = (int)(b_e - b_s);
+    const int total = na + nb;
+    const K* A = src + p.ps + a_s;
+    const K* B = src + p.ps + p.la + b_s;
+    for (int e = t; e < na; e += kBlock) sm[e] = A[e];
+    for (int e = t; e < nb; e += kBlock) sm[na + e] = B[e];
+    __syncthreads();
+    const int dt = t * IPT < total ? t * IPT : total;
+    int lo = dt > nb ? dt - nb : 0, hi = dt < na ? dt : na;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (!(sm[na + dt - 1 - mid] < sm[mid])) lo = mid + 1;
+        else hi = mid;
+    }
+    int i = lo, j = dt - lo;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        if (dt + k < total) {
+            bool take_a;
+            if (i >= na) take_a = false;
+            else if (j >= nb) take_a = true;
+            else take_a = !(sm[na + j] < sm[i]);
+            const K v = take_a ? sm[i++] : sm[na + j++];
+            so[k * (kBlock + 1) + t] = v;
+        }
+    }
+    __syncthreads();
+    for (int e = t; e < total; e += kBlock) {
+        const K v = so[(e % IPT) * (kBlock + 1) + e / IPT];
+        dst[o + e] = final_pass ? from_key<K, XF>(v) : v;
+    }
+}
+
+template <typename K, int XF>
+bool seg_sort_keys(Workspace& ws, void* d_data, uint64_t count, const uint64_t* offsets,
+                   uint64_t S) {
+    constexpr int TILE = kBlock * SortShape<K>::ITEMS;
+    const uint64_t items_cap = S + count / TILE + 1;
+    if (items_cap >= 0x7fffffffull) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "segmented sort: too many tiles");
+        return false;
+    }
+    int pass_bound = 0;
+    while ((1ull << pass_bound) < (count + TILE - 1) / TILE) ++pass_bound;
+    auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+    char* t = static_cast<char*>(ws.temp(up(count * sizeof(K)) + (items_cap + 1) * 8));
+    char* sb = static_cast<char*>(ws.seg(256 + up((S + 1) * 4)));
+    // the epoch in counters[2] is shared with the other segmented launches, so a wrap
+    // clears their status entries too
+    StatusEntry* st = static_cast<StatusEntry*>(ws.seg_status(1));
+    if (!t || !sb || !st) return false;
+    K* data = static_cast<K*>(d_data);
+    K* tmp = reinterpret_cast<K*>(t);
+    uint64_t* splits = reinterpret_cast<uint64_t*>(t + up(count * sizeof(K)));
+    uint32_t* counters = reinterpret_cast<uint32_t*>(sb);
+    uint32_t* item_start = reinterpret_cast<uint32_t*>(sb + 256);
+    char key[256];
+    snprintf(key, sizeof key, "segsort/%d/%d/%p/%p/%llu/%llu", (int)sizeof(K), XF, d_data,
+             (const void*)offsets, (unsigned long long)S, (unsigned long long)count);
+    ProfScope prof(ws, "segmented_sort", 2 * count * sizeof(K));
+    count_launch(2 + 2 * pass_bound);
+    return graph_launch(ws, key, [&] {
+        cudaStream_t s = ws.stream();
+        k_seg_plan<K, kBlock><<<1, kBlock, 0, s>>>(offsets, S, count, (uint32_t)TILE, item_start,
+                                                   counters, (K*)nullptr, K(0), nullptr, st,
+                                                   ws.seg_status_cap, &ws.d_slot->spin_error);
+        const unsigned grid = (unsigned)items_cap;
+        k_seg_tile_sort<K, XF><<<grid, kBlock, 0, s>>>(data, tmp, offsets, S, item_start);
+        for (int pass = 1; pass <= pass_bound; ++pass) {
+            const unsigned sgrid = (unsigned)((items_cap * 32 + kBlock - 1) / kBlock);
+            k_seg_merge_path<K><<<sgrid, kBlock, 0, s>>>(data, tmp, offsets, S, item_start, pass,
+                                                         splits);
+            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(data, tmp, offsets, S, item_start, pass,
+                                                       splits);
+        }
+        return cuda_ok(cudaGetLastError(), "segmented sort launch");
+    });
+}
 }  // namespace
 
 bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
@@ -318,3 +518,34 @@ bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
 }
 
 }  // namespace pxb
+
+using namespace pxb;
+
+PXB_EXPORT int parallax_segmented_sort(parallax_kernel_t kernel, void* data, size_t count,
+                                       const uint64_t* offsets, size_t num_segments) {
+    set_ok();
+    Handle* h = as_handle(kernel);
+    if (!h || (h->kind != Kind::SORT && h->kind != Kind::SORT_KV)) {
+        set_error(PARALLAX_ERR_INVALID_HANDLE, "parallax_segmented_sort: needs a sort or sort_kv handle");
+        return PARALLAX_ERR_INVALID_HANDLE;
+    }
+    Workspace* ws = workspace();
+    if (!ws) return PARALLAX_ERR_NO_DEVICE;
+    if (num_segments == 0 || count == 0) return PARALLAX_OK;
+    void* d = device_operand(data, "parallax_segmented_sort", "data");
+    const void* o = d ? device_operand(offsets, "parallax_segmented_sort", "offsets") : nullptr;
+    if (!d || !o) return PARALLAX_ERR_INVALID_ARGUMENT;
+    const uint64_t* off = static_cast<const uint64_t*>(o);
+    bool ok = false;
+    switch (h->kind == Kind::SORT_KV ? DType::U64 : h->dtype) {
+        case DType::U32: ok = seg_sort_keys<uint32_t, 0>(*ws, d, count, off, num_segments); break;
+        case DType::I32: ok = seg_sort_keys<uint32_t, 1>(*ws, d, count, off, num_segments); break;
+        case DType::F32: ok = seg_sort_keys<uint32_t, 2>(*ws, d, count, off, num_segments); break;
+        case DType::U64: ok = seg_sort_keys<uint64_t, 0>(*ws, d, count, off, num_segments); break;
+        case DType::I64: ok = seg_sort_keys<uint64_t, 1>(*ws, d, count, off, num_segments); break;
+        case DType::F64: ok = seg_sort_keys<uint64_t, 2>(*ws, d, count, off, num_segments); break;
+        default: break;
+    }
+    if (!ok) return last_error() ? last_error() : PARALLAX_ERR_CUDA;
+    return ws->async ? PARALLAX_OK : sync_stream(*ws);
+}

@@ -124,16 +124,19 @@ __device__ __forceinline__ A lookback(const TileStatus<A>& ts, uint64_t tile, A 
 // ints. Returns the exclusive prefix in every thread; the same contribution order for the
 // same status pattern, so integer results are exact and fp results deterministic given the
 // pattern.
+// `lo` is the first index of the chain (0 for a whole array, a segment's first tile for the
+// segmented kernels): that tile publishes its inclusive prefix at once, and indices below
+// it are never polled.
 template <typename A, int BLOCK>
 __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile, A agg, A* red,
-                                          int* first) {
+                                          int* first, uint64_t lo = 0) {
     constexpr int WARPS = BLOCK / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t ep = (ts.epoch & 0x3fffffffu) << 2;
-    if (tile == 0) {
+    if (tile == lo) {
         if (tid == 0) {
-            put_val(&ts.e[0].inc, agg);
-            st_release_u32(&ts.e[0].flag, ep | 2u);
+            put_val(&ts.e[tile].inc, agg);
+            st_release_u32(&ts.e[tile].flag, ep | 2u);
         }
         return A(0);
     }
@@ -147,7 +150,7 @@ __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile
         const int64_t idx = pred - tid;
         uint32_t state = 2u;
         A v = A(0);
-        if (idx >= 0) {
+        if (idx >= (int64_t)lo) {
             uint32_t f = 0, spins = 0;
             bool gave_up = false;
             for (;;) {

@@ -8,8 +8,11 @@
 #include <stddef.h>
 
 #include <atomic>
+#include <functional>
+#include <map>
 #include <mutex>
 #include <string>
+#include <utility>
 
 #include "common.cuh"
 #include "parallax/runtime.h"
@@ -94,6 +97,14 @@ struct Workspace {
 
     void* d_temp = nullptr;               // bulk temporaries (sort ping-pong buffer)
     size_t temp_cap = 0;
+    void* d_seg = nullptr;                // segmented launches: counters, work list, partials
+    size_t seg_cap = 0;
+    void* d_seg_status = nullptr;         // segmented launches: look-back status entries only
+    size_t seg_status_cap = 0;            // in entries
+    // Bumped whenever a workspace buffer is reallocated: cached graphs captured with older
+    // buffer addresses are re-captured.
+    uint64_t generation = 0;
+    std::map<std::string, std::pair<uint64_t, cudaGraphExec_t>> graphs;
 
     cudaStream_t stream() const { return user_stream ? user_stream : own_stream; }
     // Device scratch with a fixed layout (zeroed whenever it is reallocated):
@@ -102,12 +113,23 @@ struct Workspace {
     // The regions never overlap, so a status word can only ever hold a status word.
     char* scratch(uint64_t tiles);
     void* temp(size_t bytes);
+    void* seg(size_t bytes);  // zeroed on (re)allocation
+    // Status entries of segmented look-backs, which carry the device-side epoch kept in the
+    // segment buffer. A buffer of their own (zeroed on (re)allocation) so no other data
+    // ever lies where a status word is read.
+    void* seg_status(uint64_t entries);
     void* stage(int slot, size_t bytes);
     // Look-back status words carry the launch epoch, so stale words from earlier
     // launches read as "not ready" without clearing the array between launches.
     uint32_t next_epoch();
 };
 Workspace* workspace();  // nullptr when the device is unavailable
+
+// Replays the CUDA graph cached under `key` on the workspace stream, capturing it first
+// (thread-local capture of what `enqueue` puts on the stream) when it is missing or was
+// captured before a buffer reallocation. `enqueue` must not grow workspace buffers.
+// Falls back to plain enqueueing when PARALLAX_GRAPHS=0 or a user stream is set.
+bool graph_launch(Workspace& ws, const std::string& key, const std::function<bool()>& enqueue);
 
 // Waits for all work on the thread's stream with a deadline (PARALLAX_SYNC_TIMEOUT_MS,
 // default 120000) and surfaces in-kernel wait timeouts. Returns a parallax_status.
@@ -217,5 +239,9 @@ bool launch_argminmax(Workspace& ws, DType t, bool want_max, bool want_last, con
                       size_t n, uint64_t* d_index);
 bool launch_mismatch(Workspace& ws, DType t, const void* d_a, const void* d_b, size_t n,
                      uint64_t* d_index);
+
+// Device address of an operand of the segmented entry points, which take device memory or
+// PARALLAX_DEVICE_RESIDENT arena blocks only. nullptr (error recorded) otherwise.
+void* device_operand(const void* p, const char* fn, const char* what);
 
 }  // namespace pxb

@@ -84,3 +84,33 @@ def kat_relocate() -> tuple[np.ndarray, float]:
     """tests/unit/test_physptr.cpp:50-53, :116-122: 64 ones, v*2+1 through a relocated
     host pointer -> all 3.0."""
     return np.ones(64, np.float32), 3.0
+
+
+# ---- segment layouts (CSR offsets) ------------------------------------------------------
+def lognormal_offsets(seed: int, num_segments: int, median: float, sigma: float,
+                      lo: int, hi: int) -> np.ndarray:
+    """Segment lengths ~ round(lognormal(log(median), sigma)) clipped to [lo, hi], as
+    num_segments + 1 uint64 CSR offsets."""
+    rng = np.random.default_rng(seed)
+    lens = np.rint(rng.lognormal(np.log(median), sigma, num_segments))
+    lens = np.clip(lens, lo, hi).astype(np.uint64)
+    return np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+
+
+def offsets_of(lens) -> np.ndarray:
+    return np.concatenate([[0], np.cumsum(np.asarray(lens, dtype=np.uint64))]).astype(np.uint64)
+
+
+def segment_layouts() -> dict:
+    """Named segment layouts covering empty, single-element, tile-boundary and ragged cases."""
+    return {
+        "one": offsets_of([5000]),
+        "one_empty": offsets_of([0]),
+        "all_empty": offsets_of([0] * 17),
+        "ones": offsets_of([1] * 300),
+        "mixed_empty": offsets_of([0, 3, 0, 0, 1024, 1, 0, 4097, 2, 0]),
+        "tile_edges": offsets_of([1023, 1024, 1025, 2047, 2048, 2049, 4095, 4096, 4097, 8192,
+                                  16383, 16384, 16385]),
+        "big_and_small": offsets_of([1 << 20] + [7] * 100 + [300001] + [0, 1]),
+        "lognormal": lognormal_offsets(11, 500, 512, 2.0, 0, 1 << 18),
+    }
