@@ -73,37 +73,84 @@ def hbm_peak() -> tuple[float, str]:
 
 
 # ---- inputs ----------------------------------------------------------------------------------
-def make_inputs(log2n: int, log2sort: int) -> dict[str, np.ndarray]:
-    import oracle
+# u(seed, i) = splitmix64(seed * 0x9E3779B97F4A7C15 + i), the tests' and the CPU baseline's
+# counter-based generator, evaluated here with numpy (wrapping uint64 arithmetic).
+_G = 0x9E3779B97F4A7C15
+
+
+def splitmix(seed: int, n: int, start: int = 0) -> np.ndarray:
+    out = np.empty(n, dtype=np.uint64)
+    base = np.uint64((seed * _G) % (1 << 64))
+    step = 1 << 24
+    for a in range(0, n, step):
+        b = min(n, a + step)
+        x = np.arange(start + a, start + b, dtype=np.uint64) + base
+        x += np.uint64(_G)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        out[a:b] = x ^ (x >> np.uint64(31))
+    return out
+
+
+def gen(kind: str, seed: int, n: int) -> np.ndarray:
+    u = splitmix(seed, n)
+    if kind == "f32_unit":
+        return ((u >> np.uint64(40)).astype(np.float64) * 2.0 ** -24).astype(np.float32)
+    if kind == "f64_unit":
+        return (u >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    if kind == "i32_pm1000":
+        return ((u % np.uint64(2001)).astype(np.int64) - 1000).astype(np.int32)
+    if kind == "u32_full":
+        return u.astype(np.uint32)
+    if kind == "i64_full":
+        return u.view(np.int64)
+    raise ValueError(kind)
+
+
+def make_inputs(log2n: int, log2sort: int, keys=None) -> dict[str, np.ndarray]:
+    """The step's arrays (only `keys` when given)."""
     n, ns = 1 << log2n, 1 << log2sort
     t0 = time.time()
-    x = {
-        "f32": oracle.gen("f32_unit", 1, n),
-        "f64": oracle.gen("f64_unit", 2, n),
-        "i32": oracle.gen("i32_pm1000", 3, n),
-        "i64": oracle.gen("i64_full", 4, n),
-        "sort_u32": oracle.gen("u32_full", 5, ns),
-    }
-    f = oracle.gen("f32_unit", 6, ns) * np.float32(2) - np.float32(1)
-    u = oracle.gen_u64(16, 3 * (ns // 100) + 2)
+    want = (lambda k: keys is None or k in keys)
+    x = {}
+    for k, kind, seed, size in (("f32", "f32_unit", 1, n), ("f64", "f64_unit", 2, n),
+                                ("i32", "i32_pm1000", 3, n), ("i64", "i64_full", 4, n),
+                                ("sort_u32", "u32_full", 5, ns)):
+        if want(k):
+            x[k] = gen(kind, seed, size)
+    if want("sort_f32"):
+        x["sort_f32"] = sort_f32_keys(ns)
+    if want("part_i32"):
+        x["part_i32"] = gen("u32_full", 7, n).view(np.int32)
+    if want("uniq_i32"):
+        x["uniq_i32"] = unique_input(n)
+    log(f"inputs generated in {time.time() - t0:.1f}s")
+    return x
+
+
+def sort_f32_keys(ns: int) -> np.ndarray:
+    """U[-1,1) fp32 with 1% of positions overwritten by exact copies of other random
+    positions, 4096 +0.0 and 4096 -0.0."""
+    f = gen("f32_unit", 6, ns) * np.float32(2) - np.float32(1)
+    u = splitmix(16, 3 * (ns // 100) + 2)
     dup_dst = u[: ns // 100] % np.uint64(ns)
     dup_src = u[ns // 100: 2 * (ns // 100)] % np.uint64(ns)
     f[dup_dst.astype(np.int64)] = f[dup_src.astype(np.int64)]
     zpos = (u[2 * (ns // 100):] % np.uint64(ns)).astype(np.int64)[: 8192]
     f[zpos[:4096]] = np.float32(0.0)
     f[zpos[4096:8192]] = np.float32(-0.0)
-    x["sort_f32"] = f
-    x["part_i32"] = oracle.gen("u32_full", 7, n).view(np.int32)
-    # sorted int32 with geometric run lengths (p = 1/4, mean 4), value +1 per run
+    return f
+
+
+def unique_input(n: int) -> np.ndarray:
+    """Sorted int32 with geometric run lengths (p = 1/4, mean 4), value +1 per run."""
     m = n // 2 + 1024
-    ug = oracle.gen_u64(8, m)
+    ug = splitmix(8, m)
     uni = ((ug >> np.uint64(11)).astype(np.float64) + 0.5) * (1.0 / (1 << 53))
     runs = 1 + np.floor(np.log(uni) / np.log(0.75)).astype(np.int64)
     ends = np.cumsum(runs)
     k = int(np.searchsorted(ends, n)) + 1
-    x["uniq_i32"] = np.repeat(np.arange(k, dtype=np.int32), runs[:k])[:n]
-    log(f"inputs generated in {time.time() - t0:.1f}s")
-    return x
+    return np.repeat(np.arange(k, dtype=np.int32), runs[:k])[:n]
 
 
 class Op:
@@ -125,6 +172,8 @@ def build_ops(px, lib, torch, x: dict, dev: dict, aux: dict) -> list[Op]:
         return t.data_ptr()
 
     for t, s in (("f32", 4), ("f64", 8), ("i32", 4), ("i64", 8)):
+        if t not in x:
+            continue
         n = x[t].size
         for red in ("sum", "max"):
             h = px.builtin(f"reduce:{red}:{t}")
@@ -141,6 +190,8 @@ def build_ops(px, lib, torch, x: dict, dev: dict, aux: dict) -> list[Op]:
                       lambda h=hs, d=dev[t], n=n, s=s, init=init:
                       lib.parallax_exclusive_scan(h, h, h, P(d), P(out), n, s, init.ctypes.data)))
     for t, spec in (("sort_u32", "sort:u32"), ("sort_f32", "sort:f32")):
+        if t not in x:
+            continue
         n = x[t].size
         h = px.builtin(spec)
         work = aux["work"]
@@ -163,19 +214,36 @@ def build_ops(px, lib, torch, x: dict, dev: dict, aux: dict) -> list[Op]:
         op.bytes_fn, op.fn = bytes_fn, fn
         return op
 
-    ops.append(compact_op("partition_i32", "partition", "partition:i32:lt:0", "part_i32", True))
-    ops.append(compact_op("unique_i32", "unique", "unique:i32", "uniq_i32", False))
-    ops.append(compact_op("copy_if_i32", "copy_if", "copy_if:i32:mod:3:0", "i32", False))
+    for name, prim, spec, key, write_all in (
+            ("partition_i32", "partition", "partition:i32:lt:0", "part_i32", True),
+            ("unique_i32", "unique", "unique:i32", "uniq_i32", False),
+            ("copy_if_i32", "copy_if", "copy_if:i32:mod:3:0", "i32", False)):
+        if key in x:
+            ops.append(compact_op(name, prim, spec, key, write_all))
     return ops
 
 
+def op_key(name: str) -> str:
+    """Input array of a step operation, by operation name."""
+    fixed = {"sort_u32": "sort_u32", "sort_f32": "sort_f32", "partition_i32": "part_i32",
+             "unique_i32": "uniq_i32", "copy_if_i32": "i32"}
+    if name in fixed:
+        return fixed[name]
+    t = name.rsplit("_", 1)[-1]
+    if t not in ("f32", "f64", "i32", "i64"):
+        raise SystemExit(f"unknown operation {name!r}")
+    return t
+
+
 def expected_kept(x: dict) -> dict[str, int]:
-    import oracle
-    return {
-        "partition_i32": int(np.count_nonzero(x["part_i32"] < 0)),
-        "unique_i32": int(np.count_nonzero(np.diff(x["uniq_i32"])) + 1),
-        "copy_if_i32": oracle.count_if(x["i32"], oracle.P_MOD, 0, 3, 0),
-    }
+    out = {}
+    if "part_i32" in x:
+        out["partition_i32"] = int(np.count_nonzero(x["part_i32"] < 0))
+    if "uniq_i32" in x:
+        out["unique_i32"] = int(np.count_nonzero(np.diff(x["uniq_i32"])) + 1)
+    if "i32" in x:
+        out["copy_if_i32"] = int(np.count_nonzero(x["i32"] % 3 == 0))
+    return out
 
 
 # ---- clocks ----------------------------------------------------------------------------------------
@@ -354,6 +422,9 @@ def main() -> None:
     ap.add_argument("--ref-log2", type=int, default=25, help="CPU sample size (log2 elements)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ops", default="",
+                    help="comma-separated operation names to run (default: the whole step), "
+                         "e.g. sort_u32 or inclusive_scan_f32 for a small profiling case")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -375,10 +446,12 @@ def main() -> None:
 
     px = load_pkg()
     lib = px.load()
-    import oracle
-    oracle.ox()
 
-    x = make_inputs(args.log2n, args.log2sort)
+    selected = [o for o in args.ops.split(",") if o] if args.ops else None
+    if selected is not None:  # a partial step: no end-to-end or CPU legs
+        args.no_e2e = args.no_cpu = True
+    x = make_inputs(args.log2n, args.log2sort,
+                    keys=None if selected is None else {op_key(o) for o in selected})
     kept_want = expected_kept(x)
 
     def to_dev(a):
@@ -390,6 +463,8 @@ def main() -> None:
            "out": torch.empty(max_bytes, dtype=torch.uint8, device="cuda"),
            "result": torch.zeros(16, dtype=torch.uint8, device="cuda")}
     ops = build_ops(px, lib, torch, x, dev, aux)
+    if selected is not None:
+        ops = [op for op in ops if op.name in selected]
 
     stream = torch.cuda.Stream()
     lib.parallax_set_stream(C.c_void_p(stream.cuda_stream))
@@ -425,7 +500,7 @@ def main() -> None:
         collect(evs)
     for op in ops:
         op.times.clear()
-    # kept counts are deterministic: take them from the oracle-side counts, verified below
+    # kept counts are deterministic: take them from the host-side counts, verified below
     for op in ops:
         if op.name in kept_want:
             op.kept = kept_want[op.name]
@@ -448,9 +523,9 @@ def main() -> None:
     lib.parallax_profile_enable(0)
     prof = px.profile_json()
     lib.parallax_set_async(0)
-    # the compaction byte counts use the oracle's kept counts: check the device agrees
+    # the compaction byte counts use the host-side kept counts: check the device agrees
     for op in ops:
-        if op.name in kept_want:
+        if op.name in kept_want and op.name in {o.name for o in ops}:
             h = px.builtin({"partition_i32": "partition:i32:lt:0", "unique_i32": "unique:i32",
                             "copy_if_i32": "copy_if:i32:mod:3:0"}[op.name])
             key = {"partition_i32": "part_i32", "unique_i32": "uniq_i32", "copy_if_i32": "i32"}[op.name]
@@ -458,7 +533,7 @@ def main() -> None:
                                      x[key].size, 4, 0)
             px.check("kept-count check")
             if k != kept_want[op.name]:
-                raise RuntimeError(f"{op.name}: device kept {k}, oracle {kept_want[op.name]}")
+                raise RuntimeError(f"{op.name}: device kept {k}, host count {kept_want[op.name]}")
 
     step_ms = sum(statistics.fmean(op.times) for op in ops)
     bytes_step = sum(op.bytes_fn() for op in ops)
