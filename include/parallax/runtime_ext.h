@@ -134,6 +134,57 @@ int parallax_scan_noalloc(parallax_kernel_t scan_kernel, const void* input, void
                           size_t count, size_t elem_size, const void* init,
                           void* cuda_stream);
 
+/* ---- serving loop (continuous batching) --------------------------------------------
+ * No counterpart in the reference (its calls are synchronous, one at a time, and not
+ * thread-safe: src/kernel/kernel_launcher.hpp:172-176). A scheduler thread takes requests
+ * from any number of host threads, admits them in arrival order while the in-flight byte
+ * budget and the arena (for sort temporaries) allow, coalesces queued requests of the same
+ * kind into one segmented launch over per-request descriptors, and overlaps `lanes` such
+ * batches on the device. Operands stay where they are: PARALLAX_DEVICE_RESIDENT arena
+ * blocks or device memory. A request's result does not depend on what it was batched with
+ * (integers bit-exact; floating point within the primitives' tolerance). */
+typedef struct parallax_serve_config {
+    uint32_t lanes;          /* batches in flight on the device (0: 4) */
+    uint32_t max_batch;      /* requests per coalesced launch (0: 1024) */
+    uint64_t solo_elements;  /* longer requests run alone (0: 2^22) */
+    uint64_t inflight_bytes; /* admission budget: operand + temporary bytes of admitted,
+                                unfinished requests (0: half the arena capacity) */
+} parallax_serve_config;
+
+#define PARALLAX_REQ_EXCLUSIVE 1u /* scan: exclusive with `init` (else inclusive) */
+
+typedef struct parallax_request {
+    parallax_kernel_t kernel; /* reduce:<op>:<dt>, scan:<dt>, sort:<dt>, sort_kv:u32,
+                                 copy_if / remove_if / partition / unique handles */
+    const void* input;        /* sort: the data, sorted in place */
+    void* output;             /* scan (NULL: in place), compaction output */
+    size_t count;
+    const void* init;         /* exclusive scan init (element size bytes; NULL = 0) */
+    void* result;             /* host memory written on completion: the reduce value
+                                 (element size) or the kept count (uint64); may be NULL */
+    uint32_t flags;           /* PARALLAX_REQ_* */
+} parallax_request;
+
+typedef struct parallax_serve_stats {
+    uint64_t requests, batches, coalesced_requests, solo_batches, max_batch;
+    uint64_t peak_inflight_bytes, memory_waits, inflight_bytes, queued;
+} parallax_serve_stats;
+
+/* Starts the serving loop (cfg may be NULL: defaults); a no-op when it runs already. */
+int parallax_serve_start(const parallax_serve_config* cfg);
+/* Finishes every submitted request, then stops the loop. */
+int parallax_serve_stop(void);
+/* Queues a request; *ticket is waited on exactly once with parallax_serve_wait. */
+int parallax_serve_submit(const parallax_request* req, uint64_t* ticket);
+/* Blocks until the request finished; returns its parallax_status and, when done_ns is not
+ * NULL, its completion time on parallax_clock_ns()'s clock. */
+int parallax_serve_wait(uint64_t ticket, uint64_t* done_ns);
+/* submit + wait: the blocking call a client thread makes. */
+int parallax_serve_call(const parallax_request* req);
+int parallax_serve_get_stats(parallax_serve_stats* out);
+/* CLOCK_MONOTONIC in nanoseconds (the clock of parallax_serve_wait's done_ns). */
+uint64_t parallax_clock_ns(void);
+
 /* ---- instrumentation ------------------------------------------------------------- */
 /* Number of runtime kernel launches issued by this process so far. */
 uint64_t parallax_launch_count(void);

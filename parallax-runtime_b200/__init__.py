@@ -34,12 +34,34 @@ ERR_DEVICE_SPIN = 6
 ERR_UNSUPPORTED = 7
 ERR_NO_DEVICE = 8
 
+ERR_SHUTDOWN = 9
+
 COHERENT = 0
 DEVICE_RESIDENT = 1
+REQ_EXCLUSIVE = 1
 
 vp = C.c_void_p
 sz = C.c_size_t
 u64 = C.c_uint64
+
+
+class ServeConfig(C.Structure):
+    """parallax_serve_config"""
+    _fields_ = [("lanes", C.c_uint32), ("max_batch", C.c_uint32),
+                ("solo_elements", C.c_uint64), ("inflight_bytes", C.c_uint64)]
+
+
+class Request(C.Structure):
+    """parallax_request"""
+    _fields_ = [("kernel", vp), ("input", vp), ("output", vp), ("count", sz), ("init", vp),
+                ("result", vp), ("flags", C.c_uint32)]
+
+
+class ServeStats(C.Structure):
+    """parallax_serve_stats"""
+    _fields_ = [(n, C.c_uint64) for n in (
+        "requests", "batches", "coalesced_requests", "solo_batches", "max_batch",
+        "peak_inflight_bytes", "memory_waits", "inflight_bytes", "queued")]
 
 # name -> (restype, argtypes); variadic launches are declared with their fixed part only.
 _SIGNATURES = {
@@ -93,6 +115,13 @@ _SIGNATURES = {
     "parallax_segmented_copy_if": (C.c_int, [vp, vp, vp, sz, vp, sz, vp]),
     "parallax_segmented_sort": (C.c_int, [vp, vp, sz, vp, sz]),
     "parallax_device_info": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p, sz]),
+    "parallax_serve_start": (C.c_int, [C.POINTER(ServeConfig)]),
+    "parallax_serve_stop": (C.c_int, []),
+    "parallax_serve_submit": (C.c_int, [C.POINTER(Request), C.POINTER(u64)]),
+    "parallax_serve_wait": (C.c_int, [u64, C.POINTER(u64)]),
+    "parallax_serve_call": (C.c_int, [C.POINTER(Request)]),
+    "parallax_serve_get_stats": (C.c_int, [C.POINTER(ServeStats)]),
+    "parallax_clock_ns": (u64, []),
 }
 
 _lib = None

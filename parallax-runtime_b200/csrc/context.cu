@@ -93,6 +93,11 @@ static thread_local Workspace* tls_ws = nullptr;
 
 Workspace* workspace() {
     if (tls_ws) return tls_ws;
+    tls_ws = new_workspace();
+    return tls_ws;
+}
+
+Workspace* new_workspace() {
     if (!ensure_device()) {
         set_error(PARALLAX_ERR_NO_DEVICE, "no CUDA device available");
         return nullptr;
@@ -115,7 +120,6 @@ Workspace* workspace() {
         if (!g_ws_list) g_ws_list = new std::vector<Workspace*>();
         g_ws_list->push_back(ws);
     }
-    tls_ws = ws;
     return ws;
 }
 

@@ -3,22 +3,25 @@
 // No reference counterpart (the reference dispatches one primitive call per array,
 // src/kernel/kernel_launcher.cpp); this is the batching path of the B200 design.
 //
-// Layout: `offsets` (device, num_segments + 1 entries, CSR) cuts `data` into segments.
-// A one-CTA planner kernel turns the segment lengths into a tile work list (item_start[s] =
-// first work item of segment s; a segment of L elements has ceil(L / TILE) items) and
-// writes the identity results of empty segments. The persistent kernel's CTAs then claim
-// work items from an atomic counter in order, find their segment by binary search in
-// item_start, and process one tile each:
+// Segments are either CSR (`offsets`, device, num_segments + 1 entries, cut one input
+// array) or descriptors (one device-resident SegDesc per segment with its own addresses,
+// used by the serving loop to coalesce requests without moving their operands). A one-CTA
+// planner kernel turns the segment lengths into a tile work list (item_start[s] = first work
+// item of segment s; a segment of L elements has ceil(L / TILE) items) and writes the
+// results of empty segments. The persistent kernel's CTAs then claim work items from an
+// atomic counter in order, find their segment by binary search in item_start, and process
+// one tile each:
 //   reduce   tile sum -> per-item partial; the last tile of a segment to finish (per-
 //            segment ticket) folds the segment's partials in item order (deterministic)
 //   scan     tile scan + decoupled look-back that stops at the segment's first tile
+//            (exclusive with an init value, or inclusive)
 //   copy_if  flags + tile ranks + look-back on kept counts within the segment; kept
-//            elements of segment s land at out[offsets[s]...], counts[s] = kept
+//            elements of segment s land at the start of its output, its count in its slot
 // TILE = 256 threads x ITEMS; ITEMS (4, 8 or 16) is picked per (primitive, element type,
 // average segment length bucket) by timing the candidates on the first call (autotuner).
-// Every launch sequence (planner + persistent kernel) is captured once per argument set as
-// a CUDA graph and replayed; the look-back epoch lives in device memory and is advanced by
-// the planner, so a replay never reads status words of an earlier replay.
+// Every CSR launch sequence (planner + persistent kernel) is captured once per argument
+// set as a CUDA graph and replayed; the look-back epoch lives in device memory and is
+// advanced by the planner, so a replay never reads status words of an earlier replay.
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -41,9 +44,11 @@ namespace {
 constexpr int kBlock = 256;
 constexpr int kCandidates[3] = {4, 8, 16};
 
-enum SegOp : int { SEG_REDUCE = 0, SEG_SCAN = 1, SEG_COPY_IF = 2 };
+constexpr int SEG_REDUCE = (int)SegKind::REDUCE;
+constexpr int SEG_SCAN = (int)SegKind::SCAN;
+constexpr int SEG_COPY_IF = (int)SegKind::COPY_IF;
 
-// Device buffer layout of one segmented launch (all inside the workspace's segment buffer).
+// Device buffers of one segmented launch (the workspace's segment and status buffers).
 struct SegBuffers {
     uint32_t* item_start;  // num_segments + 1
     uint32_t* tickets;     // num_segments, zeroed by the planner
@@ -104,9 +109,8 @@ template <typename T> struct SegAcc { using type = typename SumAcc<T>::type; };
 // ---- the persistent kernel -------------------------------------------------------------------------
 template <typename T, int ITEMS, int OP>
 __global__ void __launch_bounds__(kBlock)
-k_segmented(const T* __restrict__ in, T* __restrict__ out, const uint64_t* __restrict__ offsets,
-            uint64_t S, SegBuffers b, void* results, unsigned long long* counts, T init,
-            SegPred<T> pred, volatile int32_t* err) {
+k_segmented(SegSrc src, uint64_t S, SegBuffers b, T init, bool inclusive, SegPred<T> pred,
+            volatile int32_t* err) {
     using A = typename SegAcc<T>::type;
     constexpr int TILE = kBlock * ITEMS;
     __shared__ __align__(16) T sm[TILE];
@@ -140,9 +144,11 @@ k_segmented(const T* __restrict__ in, T* __restrict__ out, const uint64_t* __res
         const uint32_t first_item = b.item_start[seg];
         const uint32_t seg_items = b.item_start[seg + 1] - first_item;
         const uint32_t k = item - first_item;  // tile index within the segment
-        const uint64_t seg_begin = offsets[seg], seg_end = offsets[seg + 1];
-        const uint64_t begin = seg_begin + (uint64_t)k * TILE;
-        const uint32_t len = (uint32_t)min((uint64_t)TILE, seg_end - begin);
+        const uint64_t seg_len = src.len(seg);
+        const T* in = reinterpret_cast<const T*>(src.in_addr(seg));
+        T* out = reinterpret_cast<T*>(src.out_addr(seg));
+        const uint64_t begin = (uint64_t)k * TILE;  // within the segment
+        const uint32_t len = (uint32_t)min((uint64_t)TILE, seg_len - begin);
 
         if constexpr (OP == SEG_REDUCE) {
             A acc = A(0);
@@ -152,9 +158,9 @@ k_segmented(const T* __restrict__ in, T* __restrict__ out, const uint64_t* __res
                 if (e < len) acc = acc + (A)in[begin + e];
             }
             const A sum = block_sum<T, A>(acc, red);
-            T* res = static_cast<T*>(results);
+            T* res = reinterpret_cast<T*>(src.aux_addr(seg));
             if (seg_items == 1) {
-                if (tid == 0) res[seg] = (T)sum;
+                if (tid == 0) *res = (T)sum;
             } else {
                 __shared__ bool s_last;
                 if (tid == 0) {
@@ -169,7 +175,7 @@ k_segmented(const T* __restrict__ in, T* __restrict__ out, const uint64_t* __res
                     for (uint32_t i = tid; i < seg_items; i += kBlock)
                         f = f + get_val<A>(&b.partials[first_item + i]);
                     const A t = block_sum<T, A>(f, red);
-                    if (tid == 0) res[seg] = (T)t;
+                    if (tid == 0) *res = (T)t;
                 }
                 __syncthreads();
             }
@@ -195,8 +201,13 @@ k_segmented(const T* __restrict__ in, T* __restrict__ out, const uint64_t* __res
             __syncthreads();
             const A prefix = lookback_cta<A, kBlock>(ts, item, agg, red, first, first_item);
             const A tb = (A)init + ((prefix + woff) + tex);
+            if (inclusive) {
 #pragma unroll
-            for (int j = 0; j < ITEMS; ++j) sm[tid * ITEMS + j] = (T)(j == 0 ? tb : tb + x[j - 1]);
+                for (int j = 0; j < ITEMS; ++j) sm[tid * ITEMS + j] = (T)(tb + x[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < ITEMS; ++j) sm[tid * ITEMS + j] = (T)(j == 0 ? tb : tb + x[j - 1]);
+            }
             __syncthreads();
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j) {
@@ -234,12 +245,12 @@ k_segmented(const T* __restrict__ in, T* __restrict__ out, const uint64_t* __res
             for (int j = 0; j < ITEMS; ++j)
                 if (f >> j & 1u) sm[r++] = x[j];  // rows were read before the barriers above
             __syncthreads();
-            const uint64_t dst0 = seg_begin + prefix;
             for (uint32_t i = tid; i < kept; i += kBlock) {
-                if (dst0 + i < seg_end) out[dst0 + i] = sm[i];
+                if (prefix + i < seg_len) out[prefix + i] = sm[i];
                 else *err = 3;
             }
-            if (tid == 0 && k == seg_items - 1) counts[seg] = prefix + kept;
+            if (tid == 0 && k == seg_items - 1)
+                *reinterpret_cast<uint64_t*>(src.aux_addr(seg)) = prefix + kept;
             __syncthreads();
         }
     }
@@ -268,16 +279,14 @@ bool seg_buffers(Workspace& ws, uint64_t S, uint64_t items, SegBuffers* out) {
 }
 
 struct SegCall {
-    SegOp op;
+    int op;            // SEG_REDUCE / SEG_SCAN / SEG_COPY_IF
     DType t;
-    const void* in;
-    void* out;
-    const uint64_t* offsets;
+    SegSrc src;
     uint64_t S;
-    uint64_t count;
-    void* results;
-    unsigned long long* counts;
+    uint64_t count;    // CSR: elements of the input array; descriptors: sum of lengths
     uint64_t init_bits;
+    bool inclusive;
+    bool tune;         // may time the tile candidates (launches must be idempotent)
     Pred pred;
 };
 
@@ -285,17 +294,13 @@ template <typename T, int ITEMS>
 bool enqueue_typed(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     constexpr int TILE = kBlock * ITEMS;
     cudaStream_t s = ws.stream();
-    T empty = T(0);
-    T* empty_out = c.op == SEG_REDUCE ? static_cast<T*>(c.results) : nullptr;
     volatile int32_t* err = &ws.d_slot->spin_error;
-    k_seg_plan<T, kBlock><<<1, kBlock, 0, s>>>(c.offsets, c.S, c.count, (uint32_t)TILE,
-                                               b.item_start, b.counters, empty_out, empty,
-                                               c.op == SEG_REDUCE ? b.tickets : nullptr,
-                                               b.status, b.status_cap, err);
-    if (c.op == SEG_COPY_IF) {
-        // empty segments keep nothing: zero all counts first (non-empty ones are overwritten)
-        if (!cuda_ok(cudaMemsetAsync(c.counts, 0, c.S * 8, s), "segmented counts")) return false;
-    }
+    const SegEmpty empty = c.op == SEG_REDUCE ? SegEmpty::ZERO_RESULT
+                         : c.op == SEG_COPY_IF ? SegEmpty::ZERO_COUNT : SegEmpty::NONE;
+    k_seg_plan<kBlock><<<1, kBlock, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE, b.item_start,
+                                            b.counters, empty,
+                                            c.op == SEG_REDUCE ? b.tickets : nullptr, b.status,
+                                            b.status_cap, err);
     T init;
     memcpy(&init, &c.init_bits, sizeof(T));
     SegPred<T> pr;
@@ -315,18 +320,13 @@ bool enqueue_typed(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     const unsigned grid = (unsigned)(per_sm * device_info().sm_count);
     switch (c.op) {
         case SEG_REDUCE:
-            k_segmented<T, ITEMS, SEG_REDUCE><<<grid, kBlock, 0, s>>>(
-                static_cast<const T*>(c.in), nullptr, c.offsets, c.S, b, c.results, nullptr, init, pr, err);
+            k_segmented<T, ITEMS, SEG_REDUCE><<<grid, kBlock, 0, s>>>(c.src, c.S, b, init, false, pr, err);
             break;
         case SEG_SCAN:
-            k_segmented<T, ITEMS, SEG_SCAN><<<grid, kBlock, 0, s>>>(
-                static_cast<const T*>(c.in), static_cast<T*>(c.out), c.offsets, c.S, b, nullptr,
-                nullptr, init, pr, err);
+            k_segmented<T, ITEMS, SEG_SCAN><<<grid, kBlock, 0, s>>>(c.src, c.S, b, init, c.inclusive, pr, err);
             break;
         default:
-            k_segmented<T, ITEMS, SEG_COPY_IF><<<grid, kBlock, 0, s>>>(
-                static_cast<const T*>(c.in), static_cast<T*>(c.out), c.offsets, c.S, b, nullptr,
-                c.counts, init, pr, err);
+            k_segmented<T, ITEMS, SEG_COPY_IF><<<grid, kBlock, 0, s>>>(c.src, c.S, b, init, false, pr, err);
             break;
     }
     return cuda_ok(cudaGetLastError(), "segmented launch");
@@ -404,7 +404,10 @@ int tuned_items(Workspace& ws, const SegCall& c) {
         auto it = g_tune->find(key);
         if (it != g_tune->end()) return it->second;
     }
-    if (getenv("PARALLAX_TUNE") && atoi(getenv("PARALLAX_TUNE")) == 0) return 8;
+    if (!c.tune || (getenv("PARALLAX_TUNE") && atoi(getenv("PARALLAX_TUNE")) == 0)) {
+        const uint64_t avg = c.S ? c.count / c.S : 0;  // untuned: by average segment length
+        return avg >= (16u << 10) ? 16 : avg >= (2u << 10) ? 8 : 4;
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -438,56 +441,90 @@ int tuned_items(Workspace& ws, const SegCall& c) {
 // ---- graph capture and replay -----------------------------------------------------------------
 std::string graph_key(const SegCall& c, int items) {
     char k[512];
-    snprintf(k, sizeof k, "%d/%d/%p/%p/%p/%llu/%llu/%p/%p/%llx/%d/%d/%g/%lld/%llu/%d", (int)c.op,
-             (int)c.t, c.in, c.out, (const void*)c.offsets, (unsigned long long)c.S,
-             (unsigned long long)c.count, c.results, (void*)c.counts,
-             (unsigned long long)c.init_bits, (int)c.pred.kind, (int)c.pred.negate, c.pred.f,
-             (long long)c.pred.i, (unsigned long long)c.pred.u, items);
+    snprintf(k, sizeof k, "%d/%d/%llx/%llx/%p/%llx/%llu/%llu/%llx/%d/%d/%d/%g/%lld/%llu/%d", c.op,
+             (int)c.t, (unsigned long long)c.src.in, (unsigned long long)c.src.out,
+             (const void*)c.src.offsets, (unsigned long long)c.src.aux, (unsigned long long)c.S,
+             (unsigned long long)c.count, (unsigned long long)c.init_bits, (int)c.inclusive,
+             (int)c.pred.kind, (int)c.pred.negate, c.pred.f, (long long)c.pred.i,
+             (unsigned long long)c.pred.u, items);
     return k;
 }
 
-bool run(Workspace& ws, const SegCall& c) {
+const char* op_name(int op) {
+    return op == SEG_REDUCE ? "segmented_reduce"
+         : op == SEG_SCAN ? "segmented_scan" : "segmented_copy_if";
+}
+
+// Sizes the buffers for the smallest tile before any capture (growth would invalidate a
+// captured graph).
+bool reserve(Workspace& ws, const SegCall& c) {
+    const uint64_t tile_min = (uint64_t)kBlock * kCandidates[0];
+    SegBuffers b;
+    return seg_buffers(ws, c.S, c.S + c.count / tile_min + 1, &b);
+}
+
+bool run(Workspace& ws, const SegCall& c, bool graph) {
     const int items = tuned_items(ws, c);
-    // size the buffers before any capture (growth would invalidate the graph)
-    {
-        const uint64_t tile_min = (uint64_t)kBlock * kCandidates[0];
-        SegBuffers b;
-        if (!seg_buffers(ws, c.S, c.S + c.count / tile_min + 1, &b)) return false;
-    }
+    if (!reserve(ws, c)) return false;
     const size_t es = dtype_size(c.t);
-    ProfScope prof(ws, c.op == SEG_REDUCE ? "segmented_reduce"
-                       : c.op == SEG_SCAN ? "segmented_exclusive_scan" : "segmented_copy_if",
-                   (c.op == SEG_SCAN ? 2 : 1) * c.count * es);
+    ProfScope prof(ws, op_name(c.op), (c.op == SEG_SCAN ? 2 : 1) * c.count * es);
     count_launch(2);
+    if (!graph) return enqueue(ws, c, items);
     return graph_launch(ws, graph_key(c, items), [&] { return enqueue(ws, c, items); });
 }
 
-int seg_entry(SegCall c, Handle* h, const char* fn) {
+int seg_entry(SegCall c, const void* in, void* out, const uint64_t* offsets, void* aux,
+              const char* fn) {
     set_ok();
     Workspace* ws = workspace();
     if (!ws) return PARALLAX_ERR_NO_DEVICE;
     if (c.S == 0) return PARALLAX_OK;
-    c.t = h->dtype;
     // with count == 0 every segment is empty: the data pointers are never touched and may
     // be null; offsets, results and counts are still read or written
     const bool data = c.count != 0;
-    if (data && !(c.in = device_operand(c.in, fn, "input"))) return last_error();
-    c.offsets = static_cast<const uint64_t*>(device_operand(c.offsets, fn, "offsets"));
-    if (!c.offsets) return last_error();
-    if (c.op == SEG_REDUCE && !(c.results = device_operand(c.results, fn, "results"))) return last_error();
-    if (c.op != SEG_REDUCE && data && !(c.out = device_operand(c.out, fn, "output"))) return last_error();
-    if (c.op == SEG_COPY_IF &&
-        !(c.counts = static_cast<unsigned long long*>(device_operand(c.counts, fn, "counts"))))
+    const void* d_in = nullptr;
+    void* d_out = nullptr;
+    if (data && !(d_in = device_operand(in, fn, "input"))) return last_error();
+    const void* d_off = device_operand(offsets, fn, "offsets");
+    if (!d_off) return last_error();
+    if (c.op != SEG_REDUCE && data && !(d_out = device_operand(out, fn, "output"))) return last_error();
+    void* d_aux = nullptr;  // results (reduce) or counts (copy_if); scans have none
+    if (c.op != SEG_SCAN &&
+        !(d_aux = device_operand(aux, fn, c.op == SEG_REDUCE ? "results" : "counts")))
         return last_error();
     if (c.S >= 0xffffffffull || c.count / ((uint64_t)kBlock * kCandidates[0]) + c.S >= 0xffffffffull) {
         set_error(PARALLAX_ERR_INVALID_ARGUMENT, "%s: too many segments / elements", fn);
         return PARALLAX_ERR_INVALID_ARGUMENT;
     }
-    if (!run(*ws, c)) return last_error() ? last_error() : PARALLAX_ERR_CUDA;
+    const uint32_t es = (uint32_t)dtype_size(c.t);
+    c.src = SegSrc{static_cast<const uint64_t*>(d_off), nullptr, (uint64_t)d_in, (uint64_t)d_out,
+                   (uint64_t)d_aux, c.op == SEG_COPY_IF ? 8u : es, es};
+    if (!run(*ws, c, true)) return last_error() ? last_error() : PARALLAX_ERR_CUDA;
     return ws->async ? PARALLAX_OK : sync_stream(*ws);
 }
 
 }  // namespace
+
+bool launch_segmented_descs(Workspace& ws, SegKind op, DType t, const Pred& p, bool inclusive,
+                            uint64_t init_bits, const SegDesc* d_descs, uint64_t S,
+                            uint64_t total) {
+    if (S == 0) return true;
+    if (S >= 0xffffffffull || total / ((uint64_t)kBlock * kCandidates[0]) + S >= 0xffffffffull) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "batched launch: too many segments / elements");
+        return false;
+    }
+    SegCall c{};
+    c.op = (int)op;
+    c.t = t;
+    c.src = SegSrc{nullptr, d_descs, 0, 0, 0, 0, (uint32_t)dtype_size(t)};
+    c.S = S;
+    c.count = total;
+    c.init_bits = init_bits;
+    c.inclusive = inclusive;
+    c.tune = false;
+    c.pred = p;
+    return run(ws, c, false);
+}
 
 void* device_operand(const void* p, const char* fn, const char* what) {
     if (!p) {
@@ -526,12 +563,11 @@ PXB_EXPORT int parallax_segmented_reduce(parallax_kernel_t kernel, const void* d
     }
     SegCall c{};
     c.op = SEG_REDUCE;
-    c.in = data;
+    c.t = h->dtype;
     c.count = count;
-    c.offsets = offsets;
     c.S = num_segments;
-    c.results = results;
-    return seg_entry(c, h, "parallax_segmented_reduce");
+    c.tune = true;
+    return seg_entry(c, data, nullptr, offsets, results, "parallax_segmented_reduce");
 }
 
 PXB_EXPORT int parallax_segmented_exclusive_scan(parallax_kernel_t kernel, const void* input,
@@ -545,13 +581,12 @@ PXB_EXPORT int parallax_segmented_exclusive_scan(parallax_kernel_t kernel, const
     }
     SegCall c{};
     c.op = SEG_SCAN;
-    c.in = input;
-    c.out = output;
+    c.t = h->dtype;
     c.count = count;
-    c.offsets = offsets;
     c.S = num_segments;
+    c.tune = input != output;  // timing the candidates in place would scan twice
     if (init) memcpy(&c.init_bits, init, dtype_size(h->dtype));
-    return seg_entry(c, h, "parallax_segmented_exclusive_scan");
+    return seg_entry(c, input, output, offsets, nullptr, "parallax_segmented_exclusive_scan");
 }
 
 PXB_EXPORT int parallax_segmented_copy_if(parallax_kernel_t kernel, const void* input,
@@ -565,13 +600,11 @@ PXB_EXPORT int parallax_segmented_copy_if(parallax_kernel_t kernel, const void* 
     }
     SegCall c{};
     c.op = SEG_COPY_IF;
-    c.in = input;
-    c.out = output;
+    c.t = h->dtype;
     c.count = count;
-    c.offsets = offsets;
     c.S = num_segments;
-    c.counts = reinterpret_cast<unsigned long long*>(counts);
+    c.tune = true;
     c.pred = h->pred;
     if (h->remove) c.pred.negate = !c.pred.negate;
-    return seg_entry(c, h, "parallax_segmented_copy_if");
+    return seg_entry(c, input, output, offsets, counts, "parallax_segmented_copy_if");
 }

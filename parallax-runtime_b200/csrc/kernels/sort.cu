@@ -304,79 +304,83 @@ bool sort_keys(Workspace& ws, void* d_data, uint64_t n) {
 
 // ---- segmented sort ---------------------------------------------------------------------------
 // Work list from the planner with one item per TILE keys of a segment. A segment of m items
-// needs P = ceil(log2 m) merge passes; its tile sort writes to `data` when P is even and to
-// `tmp` when P is odd, and every pass flips the buffer, so each segment ends in `data`
-// after its own last pass with no extra copy. Passes beyond a segment's P skip it.
+// needs P = ceil(log2 m) merge passes; its tile sort writes to the segment's data when P is
+// even and to its temporary when P is odd, and every pass flips the buffer, so each segment
+// ends in its data after its own last pass with no extra copy. Passes beyond a segment's P
+// skip it. Segments are CSR (one array, temporary at the same offsets of one buffer) or
+// descriptors (each with its own data and temporary addresses).
 __device__ __forceinline__ int passes_of(uint32_t m) {
     int p = 0;
     while ((1u << p) < m) ++p;
     return p;
 }
-template <typename K>
-__device__ __forceinline__ K* seg_loc(K* data, K* tmp, int P, int q) {
-    return ((P - q) & 1) ? tmp : data;
-}
 
+template <typename K>
 struct SegGeom {
     uint32_t seg, first, m, k;
-    uint64_t seg_off, seg_len;
+    uint64_t len;
+    K* data;
+    K* tmp;
     int P;
+    // buffer holding the segment after q merge passes
+    __device__ __forceinline__ K* loc(int q) const { return ((P - q) & 1) ? tmp : data; }
 };
-__device__ __forceinline__ SegGeom seg_geom(const uint64_t* offsets, uint64_t S,
-                                            const uint32_t* item_start, uint32_t item) {
-    SegGeom g;
+template <typename K>
+__device__ __forceinline__ SegGeom<K> seg_geom(const SegSrc& src, uint64_t S,
+                                               const uint32_t* item_start, uint32_t item) {
+    SegGeom<K> g;
     g.seg = find_segment(item_start, S, item);
     g.first = item_start[g.seg];
     g.m = item_start[g.seg + 1] - g.first;
     g.k = item - g.first;
-    g.seg_off = offsets[g.seg];
-    g.seg_len = offsets[g.seg + 1] - g.seg_off;
+    g.len = src.len(g.seg);
+    g.data = reinterpret_cast<K*>(src.in_addr(g.seg));
+    g.tmp = reinterpret_cast<K*>(src.aux_addr(g.seg));
     g.P = passes_of(g.m);
     return g;
 }
 
 template <typename K, int XF>
 __global__ void __launch_bounds__(kBlock)
-k_seg_tile_sort(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t S,
-                const uint32_t* __restrict__ item_start) {
+k_seg_tile_sort(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start) {
     constexpr int ITEMS = SortShape<K>::ITEMS;
     constexpr int TILE = kBlock * ITEMS;
     __shared__ K sm[TILE];
     const uint32_t item = blockIdx.x;
     if (item >= item_start[S]) return;
-    const SegGeom g = seg_geom(offsets, S, item_start, item);
+    const SegGeom<K> g = seg_geom<K>(src, S, item_start, item);
     const int t = threadIdx.x, lane = t & 31, row0 = t * ITEMS;
-    const uint64_t begin = g.seg_off + (uint64_t)g.k * TILE;
-    const uint64_t rem = g.seg_off + g.seg_len - begin;
+    const uint64_t begin = (uint64_t)g.k * TILE;
+    const uint64_t rem = g.len - begin;
     const int cnt = rem < (uint64_t)TILE ? (int)rem : TILE;
+    const K* in = g.data + begin;
     K x[ITEMS];
 #pragma unroll
-    for (int r = 0; r < ITEMS; ++r)
-        x[r] = row0 + r < cnt ? to_key<K, XF>(data[begin + row0 + r]) : ~K(0);
+    for (int r = 0; r < ITEMS; ++r) x[r] = row0 + r < cnt ? to_key<K, XF>(in[row0 + r]) : ~K(0);
     bitonic_k<K, ITEMS, TILE, 2>(x, sm, t, lane, row0);
-    K* dst = seg_loc(data, tmp, g.P, 0);
+    K* dst = g.loc(0) + begin;
 #pragma unroll
     for (int r = 0; r < ITEMS; ++r)
-        if (row0 + r < cnt) dst[begin + row0 + r] = g.P == 0 ? from_key<K, XF>(x[r]) : x[r];
+        if (row0 + r < cnt) dst[row0 + r] = g.P == 0 ? from_key<K, XF>(x[r]) : x[r];
 }
 
 template <typename K>
 __global__ void __launch_bounds__(kBlock)
-k_seg_merge_path(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t S,
-                 const uint32_t* __restrict__ item_start, int pass, uint64_t* __restrict__ splits) {
+k_seg_merge_path(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start, int pass,
+                 uint64_t* __restrict__ splits) {
     constexpr int TILE = kBlock * SortShape<K>::ITEMS;
     const uint64_t wid = ((uint64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (wid >= item_start[S]) return;
-    const SegGeom g = seg_geom(offsets, S, item_start, (uint32_t)wid);
+    const SegGeom<K> g = seg_geom<K>(src, S, item_start, (uint32_t)wid);
     if (g.P < pass) return;
-    const K* src = seg_loc(data, tmp, g.P, pass - 1) + g.seg_off;
+    const K* srcb = g.loc(pass - 1);
     const uint64_t L = (uint64_t)TILE << (pass - 1);
     const uint64_t o = (uint64_t)g.k * TILE;
-    const Pair p = pair_of(o, g.seg_len, L);
+    const Pair p = pair_of(o, g.len, L);
     const uint64_t d = o - p.ps;
-    const K* A = src + p.ps;
-    const K* B = src + p.ps + p.la;
+    const K* A = srcb + p.ps;
+    const K* B = srcb + p.ps + p.la;
     uint64_t lo = d > p.lb ? d - p.lb : 0;
     uint64_t hi = d < p.la ? d : p.la;
     while (hi - lo > 32) {
@@ -399,23 +403,23 @@ k_seg_merge_path(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t
 
 template <typename K, int XF>
 __global__ void __launch_bounds__(kBlock)
-k_seg_merge(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t S,
-            const uint32_t* __restrict__ item_start, int pass, const uint64_t* __restrict__ splits) {
+k_seg_merge(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start, int pass,
+            const uint64_t* __restrict__ splits) {
     constexpr int IPT = SortShape<K>::ITEMS;
     constexpr int OT = kBlock * IPT;
     __shared__ K sm[OT];
     __shared__ K so[IPT * (kBlock + 1)];
     const uint32_t item = blockIdx.x;
     if (item >= item_start[S]) return;
-    const SegGeom g = seg_geom(offsets, S, item_start, item);
+    const SegGeom<K> g = seg_geom<K>(src, S, item_start, item);
     if (g.P < pass) return;
     const bool final_pass = pass == g.P;
-    const K* src = seg_loc(data, tmp, g.P, pass - 1) + g.seg_off;
-    K* dst = seg_loc(data, tmp, g.P, pass) + g.seg_off;
+    const K* srcb = g.loc(pass - 1);
+    K* dst = g.loc(pass);
     const int t = threadIdx.x;
     const uint64_t L = (uint64_t)OT << (pass - 1);
     const uint64_t o = (uint64_t)g.k * OT;
-    const Pair p = pair_of(o, g.seg_len, L);
+    const Pair p = pair_of(o, g.len, L);
     const uint64_t pair_end = p.ps + p.la + p.lb;
     const uint64_t tile_end = o + OT < pair_end ? o + OT : pair_end;
     const uint64_t d0 = o - p.ps, d1 = tile_end - p.ps;
@@ -424,8 +428,8 @@ k_seg_merge(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t S,
     const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
     const int na = (int)(a_e - a_s), nb = (int)(b_e - b_s);
     const int total = na + nb;
-    const K* A = src + p.ps + a_s;
-    const K* B = src + p.ps + p.la + b_s;
+    const K* A = srcb + p.ps + a_s;
+    const K* B = srcb + p.ps + p.la + b_s;
     for (int e = t; e < na; e += kBlock) sm[e] = A[e];
     for (int e = t; e < nb; e += kBlock) sm[na + e] = B[e];
     __syncthreads();
@@ -455,9 +459,12 @@ k_seg_merge(K* data, K* tmp, const uint64_t* __restrict__ offsets, uint64_t S,
     }
 }
 
+// Plans and sorts S segments: CSR (`src.offsets`; `count` = elements of the array) or
+// descriptors (`count` = sum of the lengths). `max_len` bounds every segment's length.
+// The temporaries come from `src` (CSR: aux = base of a count-element buffer).
 template <typename K, int XF>
-bool seg_sort_keys(Workspace& ws, void* d_data, uint64_t count, const uint64_t* offsets,
-                   uint64_t S) {
+bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64_t max_len,
+                   bool graph) {
     constexpr int TILE = kBlock * SortShape<K>::ITEMS;
     const uint64_t items_cap = S + count / TILE + 1;
     if (items_cap >= 0x7fffffffull) {
@@ -465,41 +472,61 @@ bool seg_sort_keys(Workspace& ws, void* d_data, uint64_t count, const uint64_t* 
         return false;
     }
     int pass_bound = 0;
-    while ((1ull << pass_bound) < (count + TILE - 1) / TILE) ++pass_bound;
+    while ((1ull << pass_bound) < (max_len + TILE - 1) / TILE) ++pass_bound;
     auto up = [](size_t v) { return (v + 255) / 256 * 256; };
-    char* t = static_cast<char*>(ws.temp(up(count * sizeof(K)) + (items_cap + 1) * 8));
+    const bool csr_tmp = src.offsets != nullptr;
+    const size_t tmp_bytes = csr_tmp ? up(count * sizeof(K)) : 0;
+    char* t = static_cast<char*>(ws.temp(tmp_bytes + (items_cap + 1) * 8));
     char* sb = static_cast<char*>(ws.seg(256 + up((S + 1) * 4)));
     // the epoch in counters[2] is shared with the other segmented launches, so a wrap
     // clears their status entries too
     StatusEntry* st = static_cast<StatusEntry*>(ws.seg_status(1));
     if (!t || !sb || !st) return false;
-    K* data = static_cast<K*>(d_data);
-    K* tmp = reinterpret_cast<K*>(t);
-    uint64_t* splits = reinterpret_cast<uint64_t*>(t + up(count * sizeof(K)));
+    if (csr_tmp) src.aux = reinterpret_cast<uint64_t>(t);
+    src.aux_stride = 0;
+    src.elem = sizeof(K);
+    uint64_t* splits = reinterpret_cast<uint64_t*>(t + tmp_bytes);
     uint32_t* counters = reinterpret_cast<uint32_t*>(sb);
     uint32_t* item_start = reinterpret_cast<uint32_t*>(sb + 256);
-    char key[256];
-    snprintf(key, sizeof key, "segsort/%d/%d/%p/%p/%llu/%llu", (int)sizeof(K), XF, d_data,
-             (const void*)offsets, (unsigned long long)S, (unsigned long long)count);
     ProfScope prof(ws, "segmented_sort", 2 * count * sizeof(K));
     count_launch(2 + 2 * pass_bound);
-    return graph_launch(ws, key, [&] {
+    auto enqueue = [&] {
         cudaStream_t s = ws.stream();
-        k_seg_plan<K, kBlock><<<1, kBlock, 0, s>>>(offsets, S, count, (uint32_t)TILE, item_start,
-                                                   counters, (K*)nullptr, K(0), nullptr, st,
-                                                   ws.seg_status_cap, &ws.d_slot->spin_error);
+        k_seg_plan<kBlock><<<1, kBlock, 0, s>>>(src, S, count, (uint32_t)TILE, item_start, counters,
+                                                SegEmpty::NONE, nullptr, st, ws.seg_status_cap,
+                                                &ws.d_slot->spin_error);
         const unsigned grid = (unsigned)items_cap;
-        k_seg_tile_sort<K, XF><<<grid, kBlock, 0, s>>>(data, tmp, offsets, S, item_start);
+        k_seg_tile_sort<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start);
         for (int pass = 1; pass <= pass_bound; ++pass) {
             const unsigned sgrid = (unsigned)((items_cap * 32 + kBlock - 1) / kBlock);
-            k_seg_merge_path<K><<<sgrid, kBlock, 0, s>>>(data, tmp, offsets, S, item_start, pass,
-                                                         splits);
-            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(data, tmp, offsets, S, item_start, pass,
-                                                       splits);
+            k_seg_merge_path<K><<<sgrid, kBlock, 0, s>>>(src, S, item_start, pass, splits);
+            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, pass, splits);
         }
         return cuda_ok(cudaGetLastError(), "segmented sort launch");
-    });
+    };
+    if (!graph) return enqueue();
+    char key[256];
+    snprintf(key, sizeof key, "segsort/%d/%d/%p/%p/%llu/%llu/%llu", (int)sizeof(K), XF,
+             (const void*)src.in, (const void*)src.offsets, (unsigned long long)S,
+             (unsigned long long)count, (unsigned long long)max_len);
+    return graph_launch(ws, key, enqueue);
 }
+
+bool seg_sort_dispatch(Workspace& ws, DType t, const SegSrc& src, uint64_t count, uint64_t S,
+                       uint64_t max_len, bool graph) {
+    switch (t) {
+        case DType::U32: return seg_sort_keys<uint32_t, 0>(ws, src, count, S, max_len, graph);
+        case DType::I32: return seg_sort_keys<uint32_t, 1>(ws, src, count, S, max_len, graph);
+        case DType::F32: return seg_sort_keys<uint32_t, 2>(ws, src, count, S, max_len, graph);
+        case DType::U64: return seg_sort_keys<uint64_t, 0>(ws, src, count, S, max_len, graph);
+        case DType::I64: return seg_sort_keys<uint64_t, 1>(ws, src, count, S, max_len, graph);
+        case DType::F64: return seg_sort_keys<uint64_t, 2>(ws, src, count, S, max_len, graph);
+        default: break;
+    }
+    set_error(PARALLAX_ERR_INVALID_ARGUMENT, "segmented sort: unsupported element type");
+    return false;
+}
+
 }  // namespace
 
 bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
@@ -515,6 +542,13 @@ bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
     }
     set_error(PARALLAX_ERR_INVALID_ARGUMENT, "sort: unsupported element type");
     return false;
+}
+
+bool launch_segmented_sort_descs(Workspace& ws, DType t, const SegDesc* d_descs, uint64_t S,
+                                 uint64_t total, uint64_t max_len) {
+    if (S == 0 || total == 0) return true;
+    const SegSrc src{nullptr, d_descs, 0, 0, 0, 0, (uint32_t)dtype_size(t)};
+    return seg_sort_dispatch(ws, t, src, total, S, max_len, false);
 }
 
 }  // namespace pxb
@@ -535,17 +569,11 @@ PXB_EXPORT int parallax_segmented_sort(parallax_kernel_t kernel, void* data, siz
     void* d = device_operand(data, "parallax_segmented_sort", "data");
     const void* o = d ? device_operand(offsets, "parallax_segmented_sort", "offsets") : nullptr;
     if (!d || !o) return PARALLAX_ERR_INVALID_ARGUMENT;
-    const uint64_t* off = static_cast<const uint64_t*>(o);
-    bool ok = false;
-    switch (h->kind == Kind::SORT_KV ? DType::U64 : h->dtype) {
-        case DType::U32: ok = seg_sort_keys<uint32_t, 0>(*ws, d, count, off, num_segments); break;
-        case DType::I32: ok = seg_sort_keys<uint32_t, 1>(*ws, d, count, off, num_segments); break;
-        case DType::F32: ok = seg_sort_keys<uint32_t, 2>(*ws, d, count, off, num_segments); break;
-        case DType::U64: ok = seg_sort_keys<uint64_t, 0>(*ws, d, count, off, num_segments); break;
-        case DType::I64: ok = seg_sort_keys<uint64_t, 1>(*ws, d, count, off, num_segments); break;
-        case DType::F64: ok = seg_sort_keys<uint64_t, 2>(*ws, d, count, off, num_segments); break;
-        default: break;
-    }
+    const DType t = h->kind == Kind::SORT_KV ? DType::U64 : h->dtype;
+    const SegSrc src{static_cast<const uint64_t*>(o), nullptr, reinterpret_cast<uint64_t>(d), 0, 0,
+                     0, (uint32_t)dtype_size(t)};
+    // CSR: every segment lies within the array, so `count` bounds the longest one
+    const bool ok = seg_sort_dispatch(*ws, t, src, count, num_segments, count, true);
     if (!ok) return last_error() ? last_error() : PARALLAX_ERR_CUDA;
     return ws->async ? PARALLAX_OK : sync_stream(*ws);
 }

@@ -123,7 +123,8 @@ struct Workspace {
     // launches read as "not ready" without clearing the array between launches.
     uint32_t next_epoch();
 };
-Workspace* workspace();  // nullptr when the device is unavailable
+Workspace* workspace();  // the calling thread's; nullptr when the device is unavailable
+Workspace* new_workspace();  // an independent one (own stream and buffers), never freed
 
 // Replays the CUDA graph cached under `key` on the workspace stream, capturing it first
 // (thread-local capture of what `enqueue` puts on the stream) when it is missing or was
@@ -239,6 +240,19 @@ bool launch_argminmax(Workspace& ws, DType t, bool want_max, bool want_last, con
                       size_t n, uint64_t* d_index);
 bool launch_mismatch(Workspace& ws, DType t, const void* d_a, const void* d_b, size_t n,
                      uint64_t* d_index);
+
+// Segmented launches over per-segment descriptors (SegDesc, segplan.cuh; a device-resident
+// table of S entries whose lengths sum to `total`): one planner + one persistent kernel,
+// asynchronous on the workspace stream, no graph capture. Used by the serving loop.
+enum class SegKind : int { REDUCE = 0, SCAN = 1, COPY_IF = 2 };
+struct SegDesc;
+bool launch_segmented_descs(Workspace& ws, SegKind op, DType t, const Pred& p, bool inclusive,
+                            uint64_t init_bits, const SegDesc* d_descs, uint64_t S,
+                            uint64_t total);
+// Sorts every descriptor's segment in place (aux = an n-element device temporary);
+// `max_len` bounds the segment lengths. `t` is U64 for sort_kv records.
+bool launch_segmented_sort_descs(Workspace& ws, DType t, const SegDesc* d_descs, uint64_t S,
+                                 uint64_t total, uint64_t max_len);
 
 // Device address of an operand of the segmented entry points, which take device memory or
 // PARALLAX_DEVICE_RESIDENT arena blocks only. nullptr (error recorded) otherwise.

@@ -1,17 +1,59 @@
 // Segment work lists shared by the segmented kernels (segmented.cu, sort.cu).
 //
-// `offsets` (device, S + 1 entries, CSR) cut the data into segments. The one-CTA planner
-// turns segment lengths into a tile work list: item_start[s] = first work item of segment
-// s, item_start[S] = total items; a segment of L elements owns ceil(L / tile) items. It
-// also writes a caller-chosen value for every empty segment, zeroes a per-segment counter
-// array (`seg_zero`, optional), and advances the launch epoch kept in device memory (so a
-// replayed CUDA graph gets a fresh epoch every time).
+// Segments come in one of two forms:
+//   CSR         `offsets` (device, S + 1 entries) cut one input array (and the output array
+//               at the same offsets) into segments: the segmented ABI entry points;
+//   descriptors one SegDesc per segment with its own device addresses: the serving loop's
+//               coalesced launches, where every request keeps its operands where they are.
+// The one-CTA planner turns segment lengths into a tile work list: item_start[s] = first
+// work item of segment s, item_start[S] = total items; a segment of L elements owns
+// ceil(L / tile) items. It also writes the results of empty segments (a reduce identity or
+// a zero kept count), zeroes a per-segment counter array (optional), and advances the
+// launch epoch kept in device memory (so a replayed CUDA graph gets a fresh epoch every
+// time).
 #pragma once
 
 #include "common.cuh"
 #include "lookback.cuh"
 
 namespace pxb {
+
+// One segment of a descriptor-form launch (device-resident table, 32 bytes).
+struct SegDesc {
+    uint64_t in;   // device address of the segment's input
+    uint64_t out;  // device address of its output (scan, copy_if); 0 otherwise
+    uint64_t n;    // elements
+    uint64_t aux;  // reduce: result address; copy_if: kept-count address (uint64);
+                   // sort: address of an n-element temporary
+};
+
+// Where segment s lives. CSR: in/out are the arrays' bases, results/counts per-segment
+// arrays (aux of a CSR sort is the temporary's base, at the same offsets).
+struct SegSrc {
+    const uint64_t* offsets;  // CSR form when non-null
+    const SegDesc* descs;     // descriptor form otherwise
+    uint64_t in, out, aux;    // CSR bases (addresses)
+    uint32_t aux_stride;      // CSR: bytes per segment of the aux array (result / count)
+    uint32_t elem;            // element bytes
+
+    __device__ __forceinline__ uint64_t begin(uint64_t s) const {
+        return offsets ? __ldg(&offsets[s]) : 0;
+    }
+    __device__ __forceinline__ uint64_t len(uint64_t s) const {
+        return offsets ? __ldg(&offsets[s + 1]) - __ldg(&offsets[s]) : descs[s].n;
+    }
+    __device__ __forceinline__ uint64_t in_addr(uint64_t s) const {
+        return offsets ? in + begin(s) * elem : descs[s].in;
+    }
+    __device__ __forceinline__ uint64_t out_addr(uint64_t s) const {
+        return offsets ? out + begin(s) * elem : descs[s].out;
+    }
+    // reduce result / copy_if count slot, or the sort temporary of the segment
+    __device__ __forceinline__ uint64_t aux_addr(uint64_t s) const {
+        if (!offsets) return descs[s].aux;
+        return aux_stride ? aux + s * aux_stride : aux + begin(s) * elem;
+    }
+};
 
 // Largest s with item_start[s] <= item (item_start non-decreasing).
 __device__ __forceinline__ uint32_t find_segment(const uint32_t* item_start, uint64_t S,
@@ -25,16 +67,19 @@ __device__ __forceinline__ uint32_t find_segment(const uint32_t* item_start, uin
     return (uint32_t)lo;
 }
 
-// Offsets that are not non-decreasing within [0, count] write kErrSegmentOffsets to the
+// What the planner writes for an empty segment.
+enum class SegEmpty : int { NONE = 0, ZERO_RESULT = 1, ZERO_COUNT = 2 };
+
+// counters[2] is the epoch; status (status_cap entries) is cleared when it wraps.
+// CSR offsets that are not non-decreasing within [0, count] write kErrSegmentOffsets to the
 // mapped error word; such segments get no work items, so no kernel touches memory outside
 // the caller's buffers.
-// counters[2] is the epoch; status (status_cap entries) is cleared when it wraps.
-template <typename R, int BLOCK>
+template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
-k_seg_plan(const uint64_t* __restrict__ offsets, uint64_t S, uint64_t count, uint32_t tile,
-           uint32_t* __restrict__ item_start, uint32_t* __restrict__ counters, R* empty_out,
-           R empty_value, uint32_t* __restrict__ seg_zero, StatusEntry* status,
-           uint64_t status_cap, volatile int32_t* err) {
+k_seg_plan(SegSrc src, uint64_t S, uint64_t count, uint32_t tile,
+           uint32_t* __restrict__ item_start, uint32_t* __restrict__ counters, SegEmpty empty,
+           uint32_t* __restrict__ seg_zero, StatusEntry* status, uint64_t status_cap,
+           volatile int32_t* err) {
     __shared__ uint32_t s_warp[BLOCK / 32];
     __shared__ uint32_t s_carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -44,12 +89,22 @@ k_seg_plan(const uint64_t* __restrict__ offsets, uint64_t S, uint64_t count, uin
         const uint64_t s = base + tid;
         uint32_t items = 0;
         if (s < S) {
-            const uint64_t a = offsets[s], b = offsets[s + 1];
-            const bool bad = b < a || b > count;
-            if (bad) *err = kErrSegmentOffsets;
-            const uint64_t len = bad ? 0 : b - a;
+            uint64_t len;
+            if (src.offsets) {
+                const uint64_t a = src.offsets[s], b = src.offsets[s + 1];
+                const bool bad = b < a || b > count;
+                if (bad) *err = kErrSegmentOffsets;
+                len = bad ? 0 : b - a;
+            } else {
+                len = src.descs[s].n;
+            }
             items = (uint32_t)((len + tile - 1) / tile);
-            if (len == 0 && empty_out) empty_out[s] = empty_value;
+            if (len == 0 && empty != SegEmpty::NONE) {
+                void* slot = reinterpret_cast<void*>(src.aux_addr(s));
+                if (empty == SegEmpty::ZERO_COUNT) *static_cast<uint64_t*>(slot) = 0;
+                else if (src.elem == 8) *static_cast<uint64_t*>(slot) = 0;  // +0.0 / 0
+                else *static_cast<uint32_t*>(slot) = 0;
+            }
             if (seg_zero) seg_zero[s] = 0;
         }
         const uint32_t incl = warp_inclusive_scan(items, OpSum());

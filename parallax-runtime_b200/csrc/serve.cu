@@ -1,0 +1,520 @@
+// Serving loop: continuous batching of primitive requests from many host threads.
+//
+// No reference counterpart: the reference runs one synchronous call at a time on a single
+// command buffer and fence and is not thread-safe (src/kernel/kernel_launcher.hpp:172-176,
+// src/kernel/kernel_launcher.cpp:438-443).
+//
+// Clients submit requests (reduce / scan / sort / copy_if over operands already resident on
+// the device: PARALLAX_DEVICE_RESIDENT arena blocks or device memory) from any number of
+// threads. One scheduler thread owns `lanes` independent device lanes (a workspace each:
+// stream, scratch, descriptor table, pinned result slots) and keeps them busy:
+//   * completion: a lane whose batch finished (event query) hands every request its result
+//     and releases the request's admitted bytes and arena temporaries;
+//   * admission: requests are taken in arrival order while the in-flight byte budget
+//     allows and their temporaries (sort) can be carved out of the arena; the head request
+//     that does not fit waits for completions (no overtaking, so no starvation);
+//   * coalescing: the head request and every queued request of the same kind (operation,
+//     element type, predicate, scan flavour) up to `solo_elements` long become ONE
+//     segmented launch over per-request descriptors (segmented.cu, sort.cu): a planner plus
+//     one persistent kernel, or the per-segment merge passes of the segmented sort. Longer
+//     requests, and kinds without a segmented form (reduce max/min, modulo predicates,
+//     unique, partition), run alone through the plain launchers.
+// Requests that arrive while others are on the device are admitted into the next free
+// lane, so batches overlap on the device; a request's result does not depend on what it
+// was batched with (integer results are bit-exact, floating-point ones are within the
+// primitives' stated tolerance of the fp64 oracle either way).
+#include <stdint.h>
+#include <string.h>
+#include <time.h>
+
+#include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "runtime.hpp"
+#include "segplan.cuh"
+
+namespace pxb {
+namespace {
+
+enum class ReqOp : int { REDUCE, SCAN, SORT, COMPACT };
+
+uint64_t now_ns() {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (uint64_t)ts.tv_sec * 1000000000ull + (uint64_t)ts.tv_nsec;
+}
+
+struct Request {
+    ReqOp op = ReqOp::REDUCE;
+    DType t = DType::INVALID;  // U64 for sort_kv records
+    RedOp red = RedOp::SUM;
+    CompactMode mode = CompactMode::SELECT;
+    Pred pred;                 // negate folded in (remove_if)
+    bool exclusive = false;
+    uint64_t init_bits = 0;
+    const void* d_in = nullptr;
+    void* d_out = nullptr;
+    uint64_t n = 0;
+    size_t es = 0;
+    void* result = nullptr;    // caller's host memory: reduce value / kept count
+    uint64_t footprint = 0;    // admitted bytes (operands + temporaries)
+    void* tmp = nullptr;       // sort temporary: arena block (host-side address)
+    bool coalescible = false;
+    // completion
+    int status = PARALLAX_OK;
+    uint64_t done_ns = 0;
+    bool done = false;         // guarded by the server mutex
+};
+
+bool same_kind(const Request& a, const Request& b) {
+    return a.op == b.op && a.t == b.t && a.red == b.red && a.mode == b.mode &&
+           a.exclusive == b.exclusive && a.init_bits == b.init_bits &&
+           a.pred.kind == b.pred.kind && a.pred.negate == b.pred.negate &&
+           a.pred.i == b.pred.i && a.pred.u == b.pred.u &&
+           (a.pred.f == b.pred.f || (a.pred.f != a.pred.f && b.pred.f != b.pred.f));
+}
+
+struct Lane {
+    Workspace* ws = nullptr;
+    cudaEvent_t done = nullptr;
+    SegDesc* h_desc = nullptr;   // pinned
+    SegDesc* d_desc = nullptr;   // device
+    uint64_t* h_res = nullptr;   // pinned, mapped: one 8-byte result slot per request
+    uint64_t* d_res = nullptr;   // device alias of h_res
+    std::vector<Request*> reqs;
+    bool busy = false;
+};
+
+class Server {
+  public:
+    parallax_serve_config cfg{};
+    std::vector<Lane> lanes;
+    std::thread thr;
+    std::mutex mu;
+    std::condition_variable cv_sched, cv_done;
+    std::deque<Request*> queue;
+    bool stopping = false;
+    uint64_t inflight = 0;
+    parallax_serve_stats stats{};
+
+    bool init(const parallax_serve_config* c) {
+        if (c) cfg = *c;
+        if (cfg.lanes == 0) cfg.lanes = 4;
+        if (cfg.max_batch == 0) cfg.max_batch = 1024;
+        if (cfg.solo_elements == 0) cfg.solo_elements = 1ull << 22;
+        if (cfg.inflight_bytes == 0) cfg.inflight_bytes = parallax_arena_capacity() / 2;
+        lanes.resize(cfg.lanes);
+        for (Lane& l : lanes) {
+            l.ws = new_workspace();
+            if (!l.ws) return false;
+            if (!cuda_ok(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming), "serve event") ||
+                !cuda_ok(cudaHostAlloc((void**)&l.h_desc, cfg.max_batch * sizeof(SegDesc), 0),
+                         "serve descriptors (host)") ||
+                !cuda_ok(cudaMalloc((void**)&l.d_desc, cfg.max_batch * sizeof(SegDesc)),
+                         "serve descriptors (device)") ||
+                !cuda_ok(cudaHostAlloc((void**)&l.h_res, cfg.max_batch * 8, cudaHostAllocMapped),
+                         "serve results") ||
+                !cuda_ok(cudaHostGetDevicePointer((void**)&l.d_res, l.h_res, 0), "serve results"))
+                return false;
+        }
+        thr = std::thread([this] { loop(); });
+        return true;
+    }
+
+    void submit(Request* r) {
+        r->coalescible = r->coalescible && r->n <= cfg.solo_elements;
+        {
+            std::lock_guard<std::mutex> g(mu);
+            queue.push_back(r);
+            ++stats.requests;
+        }
+        cv_sched.notify_one();
+    }
+
+    int wait(Request* r, uint64_t* done_ns) {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_done.wait(lk, [&] { return r->done; });
+        if (done_ns) *done_ns = r->done_ns;
+        return r->status;
+    }
+
+    void stop() {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            stopping = true;
+        }
+        cv_sched.notify_one();
+        if (thr.joinable()) thr.join();
+    }
+
+  private:
+    // ---- admission (mutex held) ----------------------------------------------------------------
+    bool admit(Request* r) {
+        const bool idle = inflight == 0;
+        if (!idle && inflight + r->footprint > cfg.inflight_bytes) return false;
+        if (r->op == ReqOp::SORT && r->coalescible && r->n > 1) {
+            void* p = parallax_arena_alloc(r->n * r->es, 256);
+            if (!p) {
+                if (!idle) return false;
+                finish_locked(r, PARALLAX_ERR_OUT_OF_MEMORY);  // cannot fit even alone
+                return true;
+            }
+            parallax_arena_set_residency(p, PARALLAX_DEVICE_RESIDENT);
+            r->tmp = p;
+        }
+        inflight += r->footprint;
+        if (inflight > stats.peak_inflight_bytes) stats.peak_inflight_bytes = inflight;
+        return true;
+    }
+
+    // Takes the next batch off the queue (mutex held); empty when the head must wait.
+    std::vector<Request*> form_batch() {
+        std::vector<Request*> b;
+        while (!queue.empty()) {
+            Request* head = queue.front();
+            if (!admit(head)) {
+                ++stats.memory_waits;
+                return b;
+            }
+            queue.pop_front();
+            if (head->done) continue;  // rejected at admission
+            b.push_back(head);
+            break;
+        }
+        if (b.empty() || !b[0]->coalescible) return b;
+        for (auto it = queue.begin(); it != queue.end() && b.size() < cfg.max_batch;) {
+            Request* r = *it;
+            if (!r->coalescible || !same_kind(*r, *b[0])) {
+                ++it;
+                continue;
+            }
+            if (!admit(r)) break;  // keep arrival order for what does not fit
+            it = queue.erase(it);
+            if (!r->done) b.push_back(r);
+        }
+        return b;
+    }
+
+    void finish_locked(Request* r, int status) {
+        r->status = status;
+        r->done_ns = now_ns();
+        r->done = true;
+    }
+
+    // ---- launch (no mutex) ---------------------------------------------------------------------
+    bool launch(Lane& l) {
+        Workspace& ws = *l.ws;
+        const Request& h = *l.reqs[0];
+        const size_t S = l.reqs.size();
+        cudaStream_t s = ws.stream();
+        if (!h.coalescible) {
+            l.h_res[0] = 0;
+            switch (h.op) {
+                case ReqOp::REDUCE: return launch_reduce(ws, h.t, h.red, h.d_in, h.n, l.d_res);
+                case ReqOp::SCAN:
+                    return launch_scan(ws, h.t, h.exclusive, h.d_in, h.d_out ? h.d_out : (void*)h.d_in,
+                                       h.n, h.exclusive ? &h.init_bits : nullptr);
+                case ReqOp::SORT: return launch_sort(ws, h.t, const_cast<void*>(h.d_in), h.n);
+                case ReqOp::COMPACT:
+                    return launch_compact(ws, h.t, h.mode, h.pred, h.d_in, h.d_out, h.n, l.d_res);
+            }
+            return false;
+        }
+        uint64_t total = 0, max_len = 0;
+        for (size_t i = 0; i < S; ++i) {
+            const Request& r = *l.reqs[i];
+            SegDesc& d = l.h_desc[i];
+            l.h_res[i] = 0;
+            d.in = reinterpret_cast<uint64_t>(r.d_in);
+            d.out = reinterpret_cast<uint64_t>(r.d_out ? r.d_out : (void*)r.d_in);
+            d.n = r.n;
+            d.aux = r.op == ReqOp::SORT ? reinterpret_cast<uint64_t>(r.tmp ? arena_dev(r.tmp) : nullptr)
+                                        : reinterpret_cast<uint64_t>(l.d_res + i);
+            total += r.n;
+            if (r.n > max_len) max_len = r.n;
+        }
+        if (!cuda_ok(cudaMemcpyAsync(l.d_desc, l.h_desc, S * sizeof(SegDesc), cudaMemcpyHostToDevice, s),
+                     "serve descriptor upload"))
+            return false;
+        switch (h.op) {
+            case ReqOp::REDUCE:
+                return launch_segmented_descs(ws, SegKind::REDUCE, h.t, h.pred, false, 0, l.d_desc, S, total);
+            case ReqOp::SCAN:
+                return launch_segmented_descs(ws, SegKind::SCAN, h.t, h.pred, !h.exclusive,
+                                              h.exclusive ? h.init_bits : 0, l.d_desc, S, total);
+            case ReqOp::COMPACT:
+                return launch_segmented_descs(ws, SegKind::COPY_IF, h.t, h.pred, false, 0, l.d_desc, S, total);
+            case ReqOp::SORT:
+                return launch_segmented_sort_descs(ws, h.t, l.d_desc, S, total, max_len);
+        }
+        return false;
+    }
+
+    // ---- completion (no mutex while reading results) ------------------------------------------------
+    void complete(Lane& l, int status) {
+        int32_t spin = l.ws->h_slot->spin_error;
+        if (spin) {
+            l.ws->h_slot->spin_error = 0;
+            if (status == PARALLAX_OK) status = PARALLAX_ERR_DEVICE_SPIN;
+        }
+        for (size_t i = 0; i < l.reqs.size(); ++i) {
+            Request* r = l.reqs[i];
+            if (status == PARALLAX_OK && r->result) {
+                const uint64_t v = l.h_res[r->coalescible ? i : 0];
+                if (r->op == ReqOp::REDUCE) memcpy(r->result, &v, r->es);
+                else if (r->op == ReqOp::COMPACT) memcpy(r->result, &v, 8);
+            }
+            if (r->tmp) {
+                parallax_arena_free(r->tmp);
+                r->tmp = nullptr;
+            }
+        }
+        {
+            std::lock_guard<std::mutex> g(mu);
+            for (Request* r : l.reqs) {
+                inflight -= r->footprint;
+                finish_locked(r, status);
+            }
+        }
+        l.reqs.clear();
+        l.busy = false;
+        cv_done.notify_all();
+    }
+
+    void loop() {
+        ensure_device();
+        for (;;) {
+            bool progress = false;
+            bool any_busy = false;
+            for (Lane& l : lanes) {
+                if (!l.busy) continue;
+                const cudaError_t e = cudaEventQuery(l.done);
+                if (e == cudaErrorNotReady) {
+                    any_busy = true;
+                    continue;
+                }
+                complete(l, e == cudaSuccess ? PARALLAX_OK : PARALLAX_ERR_CUDA);
+                if (e != cudaSuccess) cudaGetLastError();
+                progress = true;
+            }
+            std::unique_lock<std::mutex> lk(mu);
+            for (Lane& l : lanes) {
+                if (l.busy || queue.empty()) continue;
+                std::vector<Request*> b = form_batch();
+                cv_done.notify_all();  // requests rejected at admission are finished
+                if (b.empty()) break;
+                l.reqs = std::move(b);
+                l.busy = true;
+                ++stats.batches;
+                if (l.reqs.size() > stats.max_batch) stats.max_batch = l.reqs.size();
+                if (l.reqs[0]->coalescible) stats.coalesced_requests += l.reqs.size();
+                else ++stats.solo_batches;
+                lk.unlock();
+                set_ok();
+                const bool ok = launch(l) &&
+                                cuda_ok(cudaEventRecord(l.done, l.ws->stream()), "serve event record");
+                if (!ok) {
+                    // drain what the failed launch enqueued before its buffers are reused
+                    const int st = last_error() ? last_error() : PARALLAX_ERR_CUDA;
+                    cudaStreamSynchronize(l.ws->stream());
+                    cudaGetLastError();
+                    complete(l, st);
+                }
+                lk.lock();
+                progress = true;
+                any_busy = true;
+            }
+            if (stopping && queue.empty() && !any_busy) {
+                bool busy = false;
+                for (Lane& l : lanes) busy |= l.busy;
+                if (!busy) break;
+            }
+            if (progress) continue;
+            if (any_busy) {
+                lk.unlock();
+                std::this_thread::yield();  // poll the lanes' events
+            } else {
+                cv_sched.wait(lk, [&] { return stopping || !queue.empty(); });
+            }
+        }
+    }
+};
+
+std::mutex g_srv_mu;
+Server* g_srv = nullptr;
+
+// Builds a request from the public description; returns a parallax_status.
+int make_request(const parallax_request* q, Request* r) {
+    static const char* fn = "parallax_serve_submit";
+    Handle* h = q ? as_handle(q->kernel) : nullptr;
+    if (!h) {
+        set_error(PARALLAX_ERR_INVALID_HANDLE, "%s: invalid kernel handle", fn);
+        return PARALLAX_ERR_INVALID_HANDLE;
+    }
+    r->t = h->kind == Kind::SORT_KV ? DType::U64 : h->dtype;
+    r->es = dtype_size(r->t);
+    r->n = q->count;
+    r->result = q->result;
+    switch (h->kind) {
+        case Kind::REDUCE:
+            r->op = ReqOp::REDUCE;
+            r->red = h->op;
+            r->coalescible = h->op == RedOp::SUM;
+            break;
+        case Kind::SCAN:
+            r->op = ReqOp::SCAN;
+            r->exclusive = (q->flags & PARALLAX_REQ_EXCLUSIVE) != 0;
+            if (r->exclusive && q->init) memcpy(&r->init_bits, q->init, r->es);
+            r->coalescible = true;
+            break;
+        case Kind::SORT:
+        case Kind::SORT_KV:
+            r->op = ReqOp::SORT;
+            r->coalescible = true;
+            break;
+        case Kind::COMPACT_FLAGS:
+        case Kind::UNIQUE_FLAGS:
+        case Kind::PARTITION_SCATTER:
+            r->op = ReqOp::COMPACT;
+            r->pred = h->pred;
+            if (h->kind == Kind::COMPACT_FLAGS && h->remove) r->pred.negate = !r->pred.negate;
+            r->mode = h->kind == Kind::UNIQUE_FLAGS ? CompactMode::UNIQUE
+                    : h->kind == Kind::PARTITION_SCATTER ? CompactMode::PARTITION
+                                                         : CompactMode::SELECT;
+            r->coalescible = r->mode == CompactMode::SELECT && h->pred.kind != PredKind::MOD;
+            break;
+        default:
+            set_error(PARALLAX_ERR_INVALID_HANDLE, "%s: no served form for this kernel", fn);
+            return PARALLAX_ERR_INVALID_HANDLE;
+    }
+    if (r->n == 0) return PARALLAX_OK;
+    if (!(r->d_in = device_operand(q->input, fn, "input"))) return last_error();
+    const bool has_out = r->op == ReqOp::COMPACT || (r->op == ReqOp::SCAN && q->output);
+    if (has_out && !(r->d_out = device_operand(q->output, fn, "output"))) return last_error();
+    r->footprint = r->n * r->es * (has_out ? 2 : 1) + (r->op == ReqOp::SORT ? r->n * r->es : 0);
+    return PARALLAX_OK;
+}
+
+}  // namespace
+}  // namespace pxb
+
+using namespace pxb;
+
+PXB_EXPORT int parallax_serve_start(const parallax_serve_config* cfg) {
+    set_ok();
+    if (!ensure_device()) {
+        set_error(PARALLAX_ERR_NO_DEVICE, "no CUDA device available");
+        return PARALLAX_ERR_NO_DEVICE;
+    }
+    std::lock_guard<std::mutex> g(g_srv_mu);
+    if (g_srv) return PARALLAX_OK;
+    auto* s = new Server();
+    if (!s->init(cfg)) {
+        delete s;  // lanes' workspaces stay in the global list (never freed by design)
+        return last_error() ? last_error() : PARALLAX_ERR_CUDA;
+    }
+    g_srv = s;
+    return PARALLAX_OK;
+}
+
+PXB_EXPORT int parallax_serve_stop(void) {
+    Server* s;
+    {
+        std::lock_guard<std::mutex> g(g_srv_mu);
+        s = g_srv;
+        g_srv = nullptr;
+    }
+    if (!s) return PARALLAX_OK;
+    s->stop();
+    delete s;
+    return PARALLAX_OK;
+}
+
+PXB_EXPORT int parallax_serve_submit(const parallax_request* req, uint64_t* ticket) {
+    set_ok();
+    if (!ticket) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "parallax_serve_submit: ticket is null");
+        return PARALLAX_ERR_INVALID_ARGUMENT;
+    }
+    *ticket = 0;
+    Server* s;
+    {
+        std::lock_guard<std::mutex> g(g_srv_mu);
+        s = g_srv;
+    }
+    if (!s) {
+        set_error(PARALLAX_ERR_SHUTDOWN, "parallax_serve_submit: the serving loop is not running");
+        return PARALLAX_ERR_SHUTDOWN;
+    }
+    auto* r = new Request();
+    const int st = make_request(req, r);
+    if (st != PARALLAX_OK) {
+        delete r;
+        return st;
+    }
+    if (r->n == 0) {  // nothing to do on the device
+        if (r->result && (r->op == ReqOp::REDUCE || r->op == ReqOp::COMPACT))
+            memset(r->result, 0, r->op == ReqOp::REDUCE ? r->es : 8);
+        r->done = true;
+        r->done_ns = now_ns();
+    } else {
+        s->submit(r);
+    }
+    *ticket = reinterpret_cast<uint64_t>(r);
+    return PARALLAX_OK;
+}
+
+PXB_EXPORT int parallax_serve_wait(uint64_t ticket, uint64_t* done_ns) {
+    set_ok();
+    auto* r = reinterpret_cast<Request*>(ticket);
+    if (!r) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "parallax_serve_wait: null ticket");
+        return PARALLAX_ERR_INVALID_ARGUMENT;
+    }
+    int st;
+    if (r->done && r->n == 0) {
+        st = r->status;
+        if (done_ns) *done_ns = r->done_ns;
+    } else {
+        Server* s;
+        {
+            std::lock_guard<std::mutex> g(g_srv_mu);
+            s = g_srv;
+        }
+        if (!s) {
+            set_error(PARALLAX_ERR_SHUTDOWN, "parallax_serve_wait: the serving loop is not running");
+            return PARALLAX_ERR_SHUTDOWN;
+        }
+        st = s->wait(r, done_ns);
+    }
+    delete r;
+    if (st != PARALLAX_OK) set_error(st, "served request failed (status %d)", st);
+    return st;
+}
+
+PXB_EXPORT int parallax_serve_call(const parallax_request* req) {
+    uint64_t t = 0;
+    const int st = parallax_serve_submit(req, &t);
+    if (st != PARALLAX_OK) return st;
+    return parallax_serve_wait(t, nullptr);
+}
+
+PXB_EXPORT int parallax_serve_get_stats(parallax_serve_stats* out) {
+    if (!out) return PARALLAX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(g_srv_mu);
+    if (!g_srv) {
+        memset(out, 0, sizeof *out);
+        return PARALLAX_ERR_SHUTDOWN;
+    }
+    std::lock_guard<std::mutex> g2(g_srv->mu);
+    *out = g_srv->stats;
+    out->inflight_bytes = g_srv->inflight;
+    out->queued = g_srv->queue.size();
+    return PARALLAX_OK;
+}
+
+PXB_EXPORT uint64_t parallax_clock_ns(void) { return now_ns(); }
