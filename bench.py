@@ -422,6 +422,9 @@ def main() -> None:
     ap.add_argument("--ref-log2", type=int, default=25, help="CPU sample size (log2 elements)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the segmented, map and serving workloads")
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--ops", default="",
                     help="comma-separated operation names to run (default: the whole step), "
                          "e.g. sort_u32 or inclusive_scan_f32 for a small profiling case")
@@ -565,6 +568,16 @@ def main() -> None:
                     "alg_bytes_per_launch": int(alg), "ms_per_launch": round(per_launch_ms, 4),
                     "share_of_step": round(dom["ms"] / args.steps / step_ms, 3)}
 
+    workloads = {}
+    if selected is None and not args.no_workloads:
+        lib.parallax_set_async(1)
+        workloads["segmented"] = run_segmented(px, lib, torch, stream, args.steps, args.warmup, peak)
+        workloads["map"] = run_map(px, lib, torch, stream, args.steps, args.warmup, peak)
+    lib.parallax_set_async(0)
+    lib.parallax_set_stream(None)
+    if selected is None and not args.no_workloads and rank == 0:
+        workloads["serving"] = run_serving(px, lib, args.serve_seconds)
+
     e2e = None
     if not args.no_e2e and rank == 0:
         e2e = run_e2e(px, lib, x, kept_want, args.e2e_steps)
@@ -582,7 +595,7 @@ def main() -> None:
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk,
             "wall_ms_per_step": round(1e3 * wall / args.steps, 3),
-            "per_primitive": per_prim, "kernels": prof,
+            "per_primitive": per_prim, "kernels": prof, "workloads": workloads,
             "notes": ("value and ms_per_step cover the ABI calls only; the device copies that "
                       "restore in-place operands (scan, sort) between steps are excluded and "
                       "appear in wall_ms_per_step"),
@@ -607,6 +620,220 @@ def traffic_from_profiles(kernel: str, alg_bytes: float):
             except ValueError:
                 return None
     return None
+
+
+def lognormal_offsets(seed: int, num_segments: int, median: float, sigma: float,
+                      lo: int, hi: int) -> np.ndarray:
+    """Segment lengths ~ round(lognormal(log(median), sigma)) clipped to [lo, hi], as
+    num_segments + 1 uint64 CSR offsets."""
+    rng = np.random.default_rng(seed)
+    lens = np.clip(np.rint(rng.lognormal(np.log(median), sigma, num_segments)), lo, hi)
+    return np.concatenate([[0], np.cumsum(lens.astype(np.uint64))]).astype(np.uint64)
+
+
+def timed_calls(torch, stream, fn, steps: int, warmup: int, restore=None) -> float:
+    """Mean device ms of fn() over `steps` calls (CUDA events on the launch stream)."""
+    times = []
+    for i in range(warmup + steps):
+        if restore:
+            with torch.cuda.stream(stream):
+                restore()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        stream.synchronize()
+        if i >= warmup:
+            times.append(e0.elapsed_time(e1))
+    return statistics.fmean(times)
+
+
+def run_segmented(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dict:
+    """Batched segmented primitives: 4096 segments, lognormal sizes (median 4096, sigma 2,
+    clipped to [1, 2^22], seed 11); each call is one replayed CUDA graph."""
+    off = lognormal_offsets(11, 4096, 4096, 2.0, 1, 1 << 22)
+    total = int(off[-1])
+    S = off.size - 1
+    f32 = gen("f32_unit", 11, total)
+    i32 = gen("i32_pm1000", 12, total)
+    keys = gen("u32_full", 13, total).astype(np.uint64)
+    within = np.arange(total, dtype=np.uint64) - np.repeat(off[:-1], np.diff(off).astype(np.int64))
+    recs = (keys << np.uint64(32)) | within
+    del keys, within
+
+    def put(a):
+        return torch.from_numpy(a.view(np.uint8)).cuda()
+
+    d_off, d_f32, d_i32, d_recs = put(off), put(f32), put(i32), put(recs)
+    work = torch.empty_like(d_recs)
+    out = torch.empty(total * 4, dtype=torch.uint8, device="cuda")
+    res = torch.empty(S * 8, dtype=torch.uint8, device="cuda")
+    cnt = torch.empty(S * 8, dtype=torch.uint8, device="cuda")
+    zero = np.zeros(1, np.int64)
+    P = lambda t: t.data_ptr()  # noqa: E731
+    kept = {"f32": int(np.count_nonzero(f32 > np.float32(0.5))),
+            "i32": int(np.count_nonzero(i32 > 0))}
+    ops = []
+    for t, d in (("f32", d_f32), ("i32", d_i32)):
+        ops.append((f"segmented_reduce_{t}", total * 4, None, lambda t=t, d=d:
+                    lib.parallax_segmented_reduce(px.builtin(f"reduce:sum:{t}"), P(d), total,
+                                                  P(d_off), S, P(res))))
+        ops.append((f"segmented_exclusive_scan_{t}", 2 * total * 4, None, lambda t=t, d=d:
+                    lib.parallax_segmented_exclusive_scan(px.builtin(f"exclusive_scan:{t}"), P(d),
+                                                          P(out), total, P(d_off), S,
+                                                          zero.ctypes.data)))
+        spec = "copy_if:f32:gt:0.5" if t == "f32" else "copy_if:i32:gt:0"
+        ops.append((f"segmented_copy_if_{t}", (total + kept[t]) * 4, None, lambda spec=spec, d=d:
+                    lib.parallax_segmented_copy_if(px.builtin(spec), P(d), P(out), total,
+                                                   P(d_off), S, P(cnt))))
+    ops.append(("segmented_sort_kv_u32", 2 * total * 8, lambda: work.copy_(d_recs, non_blocking=True),
+                lambda: lib.parallax_segmented_sort(px.builtin("sort_kv:u32"), P(work), total,
+                                                    P(d_off), S)))
+    per_op, tot_bytes, tot_ms = {}, 0, 0.0
+    for name, nbytes, restore, fn in ops:
+        ms = timed_calls(torch, stream, fn, steps, warmup, restore)
+        px.check(name)
+        per_op[name] = {"ms": round(ms, 4), "GB_s": round(nbytes / ms / 1e6, 1),
+                        "frac_of_peak": round(nbytes / ms / 1e6 / peak, 3)}
+        tot_bytes += nbytes
+        tot_ms += ms
+    # parity spot check of the sorted records (stable by key within each segment)
+    got = work.cpu().numpy().view(np.uint64)
+    for s_ in (0, S // 2, S - 1):
+        a, b = int(off[s_]), int(off[s_ + 1])
+        seg = recs[a:b]
+        want = seg[np.argsort(seg >> np.uint64(32), kind="stable")]
+        if not np.array_equal(got[a:b], want):
+            raise RuntimeError(f"segmented sort_kv mismatch in segment {s_}")
+    return {"workload": (f"{S} segments, lognormal sizes (median 4096, sigma 2, clipped to "
+                         f"[1, 2^22], seed 11): {total} elements of fp32 U[0,1) and int32 "
+                         f"U[-1000,1000]; key-value records u32 key | u32 index"),
+            "elements": total, "GB_s": round(tot_bytes / tot_ms / 1e6, 1),
+            "frac_of_peak": round(tot_bytes / tot_ms / 1e6 / peak, 3), "ms": round(tot_ms, 3),
+            "per_op": per_op}
+
+
+def run_map(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dict:
+    """Map with captures and in-kernel relocation: 2^24 {float x; u32 pad; float* p}
+    records whose p are HOST arena addresses of a 2^24 fp32 target (seed 7), y = 1.5*x + *p,
+    then a reduce of y; all three arrays device-resident arena blocks."""
+    n = 1 << 24
+    tgt_h = gen("f32_unit", 7, n)
+    idx = splitmix(8, n) % np.uint64(n)
+    xs = gen("f32_unit", 9, n)
+    blocks = []
+
+    def arena_array(a):
+        p = lib.parallax_arena_alloc(a.nbytes, 256)
+        if not p:
+            raise RuntimeError("arena allocation failed")
+        blocks.append(p)
+        v = np.ctypeslib.as_array((C.c_ubyte * a.nbytes).from_address(p)).view(a.dtype)
+        v[:] = a
+        return p
+
+    try:
+        tgt = arena_array(tgt_h)
+        rec = np.zeros(n * 4, np.uint32)
+        rec[0::4] = xs.view(np.uint32)
+        rec.view(np.uint64)[1::2] = np.uint64(tgt) + idx * np.uint64(4)
+        recs = arena_array(rec)
+        y = arena_array(np.zeros(n, np.float32))
+        for p, nb in ((tgt, n * 4), (recs, n * 16), (y, n * 4)):
+            lib.parallax_arena_set_residency(p, px.DEVICE_RESIDENT)
+            lib.parallax_arena_sync_to_device(p, nb)
+        a = np.array([1.5], np.float32)
+        hm = px.builtin("map:saxpy_gather_f32")
+        hr = px.builtin("reduce:sum:f32")
+        res = torch.zeros(8, dtype=torch.uint8, device="cuda")
+        ms_map = timed_calls(torch, stream, lambda: lib.parallax_kernel_launch_transform2_captures(
+            hm, recs, y, n, 16, 4, a.ctypes.data, 4), steps, warmup)
+        ms_red = timed_calls(torch, stream, lambda: lib.parallax_reduce(hr, y, n, 4, res.data_ptr()),
+                             steps, warmup)
+        px.check("map workload")
+        # bit-exact spot check of y (fp32 products and sums, no contraction)
+        lib.parallax_arena_sync_to_host(y, n * 4)
+        lib.parallax_synchronize()  # async mode: the copy above is only enqueued
+        yv = np.ctypeslib.as_array((C.c_ubyte * (n * 4)).from_address(y)).view(np.float32)
+        sel = np.arange(0, n, 9973)
+        prod = (np.float32(1.5) * xs[sel]).astype(np.float32)
+        want = (prod + tgt_h[idx[sel].astype(np.int64)]).astype(np.float32)
+        if not np.array_equal(yv[sel], want):
+            raise RuntimeError("map workload: y differs from the host fp32 formula")
+    finally:
+        for p in blocks:
+            lib.parallax_arena_free(p)
+    b_map, b_red = 24 * n, 4 * n
+    return {"workload": "2^24 records {float x; u32 pad; float* p}, y = 1.5f*x + *p (host "
+                        "pointers relocated in-kernel), then reduce(y); seed 7",
+            "elements": n,
+            "map": {"ms": round(ms_map, 4), "GB_s": round(b_map / ms_map / 1e6, 1),
+                    "frac_of_peak": round(b_map / ms_map / 1e6 / peak, 3)},
+            "reduce": {"ms": round(ms_red, 4), "GB_s": round(b_red / ms_red / 1e6, 1)},
+            "GB_s": round((b_map + b_red) / (ms_map + ms_red) / 1e6, 1),
+            "frac_of_peak": round((b_map + b_red) / (ms_map + ms_red) / 1e6 / peak, 3)}
+
+
+class LoadgenConfig(C.Structure):
+    _fields_ = [("threads", C.c_uint32), ("mode", C.c_uint32), ("rate", C.c_double),
+                ("seconds", C.c_double), ("seed", C.c_uint64), ("log2_min", C.c_uint32),
+                ("log2_max", C.c_uint32), ("max_inflight", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class LoadgenResult(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("errors", C.c_uint64), ("seconds", C.c_double),
+                ("req_s", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double), ("max_ms", C.c_double), ("gbytes", C.c_double),
+                ("gb_s", C.c_double), ("per_op", C.c_uint64 * 4)]
+
+
+def run_serving(px, lib, seconds: float) -> dict:
+    """Serving mix: 16 client threads, Poisson arrivals, 40/30/20/10 reduce / exclusive scan /
+    sort / copy_if, n log-uniform 2^10..2^26, dtypes uniform over fp32/fp64/int32/int64,
+    operands in device-resident arena blocks (seed 13). Per-call (one synchronous ABI call
+    per request) against the serving loop, back-to-back (saturation; the served clients keep
+    up to 8 requests each outstanding) and at 70 % of the per-call saturation rate."""
+    lg = C.CDLL(str(ROOT / "parallax-runtime_b200" / "lib" / "libparallax-loadgen.so"))
+    lg.px_loadgen_prepare.argtypes = [C.c_uint64]
+    lg.px_loadgen_run.argtypes = [C.POINTER(LoadgenConfig), C.POINTER(LoadgenResult)]
+    if lg.px_loadgen_prepare(13) != px.OK:
+        raise RuntimeError("loadgen prepare failed")
+
+    def one(mode, rate):
+        cfg = LoadgenConfig(threads=16, mode=mode, rate=rate, seconds=seconds, seed=13,
+                            log2_min=10, log2_max=26, max_inflight=8 if rate <= 0 else 64)
+        r = LoadgenResult()
+        if lg.px_loadgen_run(C.byref(cfg), C.byref(r)) != px.OK:
+            raise RuntimeError("loadgen run failed")
+        if r.errors:
+            raise RuntimeError(f"serving mix: {r.errors} failed requests")
+        return {"req_s": round(r.req_s, 1), "p50_ms": round(r.p50_ms, 3),
+                "p99_ms": round(r.p99_ms, 3), "mean_ms": round(r.mean_ms, 3),
+                "GB_s": round(r.gb_s, 1), "completed": int(r.completed),
+                "offered_req_s": rate if rate > 0 else "back-to-back"}
+
+    try:
+        out = {"per_call_saturation": one(0, 0.0)}
+        assert lib.parallax_serve_start(None) == px.OK
+        out["served_saturation"] = one(1, 0.0)
+        rate = round(0.7 * out["per_call_saturation"]["req_s"], 1)
+        out["served_at_rate"] = one(1, rate)
+        st = px.ServeStats()
+        lib.parallax_serve_get_stats(C.byref(st))
+        lib.parallax_serve_stop()
+        out["per_call_at_rate"] = one(0, rate)
+        out["serve_stats"] = {"requests": st.requests, "batches": st.batches,
+                              "coalesced_requests": st.coalesced_requests,
+                              "max_batch": st.max_batch, "memory_waits": st.memory_waits}
+        out["throughput_ratio_saturation"] = round(
+            out["served_saturation"]["req_s"] / out["per_call_saturation"]["req_s"], 3)
+    finally:
+        lib.parallax_serve_stop()
+        lg.px_loadgen_release()
+    out["workload"] = ("16 threads, Poisson arrivals, 40/30/20/10 reduce / exclusive scan / sort / "
+                       "copy_if, n log-uniform 2^10..2^26, dtype uniform over fp32/fp64/int32/int64, "
+                       f"operands in device-resident arena blocks, seed 13, {seconds:g} s per point")
+    return out
 
 
 def run_e2e(px, lib, x: dict, kept_want: dict, steps: int) -> dict:
@@ -649,13 +876,16 @@ def run_e2e(px, lib, x: dict, kept_want: dict, steps: int) -> dict:
         h = px.builtin(spec)
         plan.append((key, lambda h=h, n=n: lib.parallax_copy_if(h, h, h, h, pin, pout, n, 4, 0),
                      alg, n * 4, w * 4))
-    for _ in range(steps):
+    for step in range(steps + 1):  # step 0 warms up (the first copies page-lock the blocks)
         for key, fn, alg, up, down in plan:
             view(pin, x[key])[:] = x[key]  # host-side staging of the step's input (untimed)
             t0 = time.perf_counter()
             fn()
-            total_s += time.perf_counter() - t0
+            dt = time.perf_counter() - t0
             px.check("e2e call")
+            if step == 0:
+                continue
+            total_s += dt
             total_bytes += alg
             h2d += up
             d2h += down

@@ -2,7 +2,9 @@
 
 Compiles every CUDA/C++ source under csrc/ with nvcc for sm_100a and links one shared
 library, lib/libparallax-runtime.so, that exports the parallax C ABI. Objects go to
-_build/ and are rebuilt when a source or any header is newer than the object.
+_build/ and are rebuilt when a source or any header is newer than the object. The
+serving-mix load generator (loadgen/loadgen.cpp, host C++ over the public ABI) is linked
+against it as lib/libparallax-loadgen.so.
 
     python parallax-runtime_b200/build.py [--force] [--jobs N]
 """
@@ -89,7 +91,29 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False,
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_loadgen(force)
     return LIB
+
+
+LOADGEN_SRC = PKG / "loadgen" / "loadgen.cpp"
+LOADGEN = LIB_DIR / "libparallax-loadgen.so"
+
+
+def build_loadgen(force: bool = False) -> Path:
+    """The serving-mix load generator: host C++ over the public C ABI only."""
+    newest = max(LOADGEN_SRC.stat().st_mtime, LIB.stat().st_mtime,
+                 *(h.stat().st_mtime for h in (ROOT / "include").rglob("*.h")))
+    if not force and LOADGEN.exists() and LOADGEN.stat().st_mtime >= newest:
+        return LOADGEN
+    tmp = LOADGEN.with_suffix(".so.tmp")
+    cmd = ["g++", "-std=c++17", "-O2", "-shared", "-fPIC", "-fvisibility=hidden", "-Wall",
+           "-I", str(ROOT / "include"), str(LOADGEN_SRC), "-o", str(tmp),
+           "-L", str(LIB_DIR), "-lparallax-runtime", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"loadgen build failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LOADGEN)
+    return LOADGEN
 
 
 def main() -> None:

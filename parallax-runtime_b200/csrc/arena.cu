@@ -7,8 +7,9 @@
 //   * device side: one contiguous virtual range (cuMemAddressReserve) whose physical
 //     HBM is mapped in 512 MiB chunks as the arena grows, so a 64 GiB capacity costs
 //     nothing until used;
-//   * host side: one contiguous anonymous mapping of the same size; every mapped chunk
-//     is page-locked so host<->device copies run at full link speed;
+//   * host side: one contiguous anonymous mapping of the same size; a chunk's pages are
+//     locked the first time a copy touches it (host<->device copies then run at full
+//     link speed), so device-resident blocks cost no host memory;
 //   * the relocation formula of the reference stays exact: the device address of a
 //     host arena pointer p is dev_base + (p - host_base);
 //   * blocks carry a residency mode; ABI calls move only the byte ranges they name
@@ -62,13 +63,29 @@ struct Arena {
     char* host_base = nullptr;
     CUdeviceptr dev_base = 0;
     size_t chunk = 512ull << 20;
-    size_t mapped = 0;     // bytes with device memory mapped and host pages locked
+    size_t mapped = 0;     // bytes with device memory mapped
     size_t bump = 0;       // first never-used offset
     size_t used = 0;       // bytes in live blocks
     std::map<size_t, size_t> free_blocks;       // offset -> size, coalesced
     std::map<size_t, ArenaBlock> live;          // offset -> block
     DriverFns drv;
     std::vector<CUmemGenericAllocationHandle> handles;
+    std::vector<uint8_t> pinned;  // per chunk: host mirror page-locked yet
+
+    // Page-locks the host mirror of every chunk that [off, off + bytes) touches, on first
+    // use: blocks that only ever live on the device never pin host memory.
+    void pin_range(size_t off, size_t bytes) {
+        std::lock_guard<std::mutex> g(mu);
+        for (size_t c = off / chunk; c * chunk < off + bytes && c < pinned.size(); ++c) {
+            if (pinned[c]) continue;
+            if (cudaHostRegister(host_base + c * chunk, chunk, cudaHostRegisterDefault) !=
+                cudaSuccess) {
+                cudaGetLastError();  // copies from this chunk stay pageable (slower, correct)
+                continue;
+            }
+            pinned[c] = 1;
+        }
+    }
 
     static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -133,12 +150,8 @@ struct Arena {
             acc.location = prop.location;
             acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
             if (drv.set_access(dev_base + mapped, chunk, &acc, 1) != CUDA_SUCCESS) return false;
-            if (cudaHostRegister(host_base + mapped, chunk, cudaHostRegisterDefault) !=
-                cudaSuccess) {
-                cudaGetLastError();
-                return false;
-            }
             handles.push_back(hdl);
+            pinned.push_back(0);
             mapped += chunk;
         }
         return true;
@@ -268,14 +281,15 @@ uint64_t arena_mapped_bytes() {
     return a.mapped;
 }
 
-// The host mirror is page-locked chunk by chunk, and one copy may not span two
-// registrations, so arena copies are split at chunk boundaries (which are also the
+// The host mirror is page-locked chunk by chunk on first copy, and one copy may not span
+// two registrations, so arena copies are split at chunk boundaries (which are also the
 // boundaries of the device-side physical allocations).
 bool arena_copy_async(void* dst, const void* src, size_t bytes, bool to_device,
                       cudaStream_t s) {
     Arena& a = arena();
     const char* h = static_cast<const char*>(to_device ? src : dst);
     size_t off = static_cast<size_t>(h - a.host_base);
+    a.pin_range(off, bytes);
     size_t done = 0;
     while (done < bytes) {
         size_t room = a.chunk - (off + done) % a.chunk;

@@ -192,8 +192,15 @@ void* Workspace::seg_status(uint64_t entries) {
 bool graph_launch(Workspace& ws, const std::string& key, const std::function<bool()>& enqueue) {
     static const bool enabled =
         !(getenv("PARALLAX_GRAPHS") && atoi(getenv("PARALLAX_GRAPHS")) == 0);
-    if (!enabled || ws.user_stream) return enqueue();
+    if (!enabled) return enqueue();
     cudaStream_t s = ws.stream();
+    if (ws.user_stream) {  // the caller may be capturing its own stream: launch into that
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) {
+            cudaGetLastError();
+            return enqueue();
+        }
+    }
     auto it = ws.graphs.find(key);
     if (it != ws.graphs.end() && it->second.first != ws.generation) {
         cudaGraphExecDestroy(it->second.second);

@@ -9,9 +9,10 @@
 // 2048 8-byte keys per 256-thread CTA): stages whose partner distance j is below the
 // per-thread run use registers, j up to 32 runs uses warp shuffles, larger j goes through
 // shared memory. Sorted tiles are then merged pairwise, doubling the run length each
-// pass, with a merge-path split per 16 KiB output tile (one warp per split, 32-ary
-// search) and a stable in-shared-memory merge. Any n is accepted (the last tile is padded
-// with the largest key in registers only).
+// pass: a CTA finds its output tiles' spans on the merge path (one warp per split, 32-ary
+// search over HBM), stages the two input spans in shared memory and merges stably, each
+// thread producing its 16 (8) contiguous outputs in registers. Any n is accepted (the
+// last tile is padded with the largest key in registers only).
 // Keys are sorted as unsigned integers after an order-preserving transform: signed
 // integers flip the sign bit; IEEE floats flip all bits when negative and the sign bit
 // otherwise (the IEEE total order: -0.0 sorts before +0.0). The transform is fused into
@@ -19,6 +20,7 @@
 // sort are (key << 32 | value) and sort as plain 64-bit keys, i.e. stably by key.
 #include <stdint.h>
 #include <stdio.h>
+#include <string.h>
 
 #include "../runtime.hpp"
 #include "../segplan.cuh"
@@ -169,22 +171,16 @@ __device__ __forceinline__ Pair pair_of(uint64_t o, uint64_t n, uint64_t L) {
     return p;
 }
 
-// One warp per output tile: number of A elements among the first d outputs of the
-// stable merge (A wins ties): the first i with !(A[i] <= B[d-1-i]).
+// Warp-collective merge-path search: the number of A elements among the first d outputs
+// of the stable merge of A[0, la) and B[0, lb) (A wins ties): the number of i < d with
+// B[d-1-i] >= A[i] (a monotone predicate), found by a 32-ary search (32 probes a round).
 template <typename K>
-__global__ void __launch_bounds__(kBlock)
-k_merge_path(const K* __restrict__ src, uint64_t n, uint64_t L, uint64_t OT, uint64_t tiles,
-             uint64_t* __restrict__ splits) {
-    const uint64_t tile = ((uint64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
+__device__ __forceinline__ uint64_t warp_merge_split(const K* __restrict__ A, uint64_t la,
+                                                     const K* __restrict__ B, uint64_t lb,
+                                                     uint64_t d) {
     const int lane = threadIdx.x & 31;
-    if (tile >= tiles) return;
-    const uint64_t o = tile * OT;
-    const Pair p = pair_of(o, n, L);
-    const uint64_t d = o - p.ps;
-    const K* A = src + p.ps;
-    const K* B = src + p.ps + p.la;
-    uint64_t lo = d > p.lb ? d - p.lb : 0;
-    uint64_t hi = d < p.la ? d : p.la;
+    uint64_t lo = d > lb ? d - lb : 0;
+    uint64_t hi = d < la ? d : la;
     while (hi - lo > 32) {
         const uint64_t stride = (hi - lo + 31) / 32;
         const uint64_t q = lo + (uint64_t)lane * stride;
@@ -199,58 +195,132 @@ k_merge_path(const K* __restrict__ src, uint64_t n, uint64_t L, uint64_t OT, uin
     }
     const uint64_t q = lo + lane;
     const bool tr = q < hi && !(B[d - 1 - q] < A[q]);
-    const int c = __popc(__ballot_sync(0xffffffffu, tr));
-    if (lane == 0) splits[tile] = lo + c;
+    return lo + __popc(__ballot_sync(0xffffffffu, tr));
 }
 
-template <typename K, int XF, bool FINAL>
-__global__ void __launch_bounds__(kBlock)
-k_merge(const K* __restrict__ src, K* __restrict__ dst, uint64_t n, uint64_t L,
-        const uint64_t* __restrict__ splits) {
-    constexpr int IPT = SortShape<K>::ITEMS;
-    constexpr int OT = kBlock * IPT;
-    __shared__ K sm[OT];
-    __shared__ K so[IPT * (kBlock + 1)];
-    const int t = threadIdx.x;
-    const uint64_t o = (uint64_t)blockIdx.x * OT;
-    const Pair p = pair_of(o, n, L);
-    const uint64_t pair_end = p.ps + p.la + p.lb;
-    const uint64_t tile_end = o + OT < pair_end ? o + OT : pair_end;
-    const uint64_t d0 = o - p.ps, d1 = tile_end - p.ps;
-    const uint64_t a_s = splits[blockIdx.x];
-    const uint64_t a_e = o + OT < pair_end ? splits[blockIdx.x + 1] : p.la;
-    const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
-    const int na = (int)(a_e - a_s), nb = (int)(b_e - b_s);
-    const int total = na + nb;
-    const K* A = src + p.ps + a_s;
-    const K* B = src + p.ps + p.la + b_s;
-    for (int e = t; e < na; e += kBlock) sm[e] = A[e];
-    for (int e = t; e < nb; e += kBlock) sm[na + e] = B[e];
-    __syncthreads();
+// Shared-memory position of element i of a staged span: one padding slot per 32 elements.
+// Threads walk their merge-path segments at strides of about IPT / 2 to IPT elements
+// (8 or 16 for 4-byte keys), which would put a warp's loads in 2-4 banks; the padding
+// spreads those strides over all 32.
+__device__ __forceinline__ int pad32(int i) { return i + (i >> 5); }
+constexpr int staged_elems(int ot) { return ot + ot / 32 + 4; }
 
-    const int dt = t * IPT < total ? t * IPT : total;
+// Merges the sorted spans As and Bs (shared memory, padded positions, na + nb <= OT, A
+// wins ties) into dst[0, na + nb): every thread finds its start on the merge path by
+// binary search and merges its IPT outputs in registers (one shared load per output),
+// then stores them as 16-byte vectors (a thread's outputs are contiguous). Positions
+// pad32(na) of As and pad32(nb) of Bs must be readable (their values are ignored).
+template <typename K, int XF>
+__device__ __forceinline__ void merge_spans(const K* As, int na, const K* Bs, int nb,
+                                            K* __restrict__ dst, bool final_pass) {
+    constexpr int IPT = SortShape<K>::ITEMS;
+    constexpr int V = 16 / sizeof(K);
+    const int total = na + nb;
+    const int dt = threadIdx.x * IPT < total ? threadIdx.x * IPT : total;
     int lo = dt > nb ? dt - nb : 0, hi = dt < na ? dt : na;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (!(sm[na + dt - 1 - mid] < sm[mid])) lo = mid + 1;
+        if (!(Bs[pad32(dt - 1 - mid)] < As[pad32(mid)])) lo = mid + 1;
         else hi = mid;
     }
     int i = lo, j = dt - lo;
+    K a = As[pad32(i)];
+    K b = Bs[pad32(j)];
+    K out[IPT];
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
-        if (dt + k < total) {
-            bool take_a;
-            if (i >= na) take_a = false;
-            else if (j >= nb) take_a = true;
-            else take_a = !(sm[na + j] < sm[i]);
-            const K v = take_a ? sm[i++] : sm[na + j++];
-            so[k * (kBlock + 1) + t] = v;
+        const bool take_a = j >= nb || (i < na && !(b < a));
+        out[k] = take_a ? a : b;
+        i += take_a;
+        j += !take_a;
+        const K x = take_a ? As[pad32(i)] : Bs[pad32(j)];
+        a = take_a ? x : a;
+        b = take_a ? b : x;
+    }
+    if (final_pass) {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) out[k] = from_key<K, XF>(out[k]);
+    }
+    if (dt + IPT <= total && (reinterpret_cast<uintptr_t>(dst) % 16 == 0)) {
+        uint4* d = reinterpret_cast<uint4*>(dst + dt);
+#pragma unroll
+        for (int v = 0; v < IPT / V; ++v) {
+            uint4 r;
+            memcpy(&r, &out[v * V], 16);
+            d[v] = r;
         }
+    } else {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k)
+            if (dt + k < total) dst[dt + k] = out[k];
+    }
+}
+
+// Stages A[0, na) and B[0, nb) in sm (staged_elems(OT) elements, padded positions) with
+// coalesced plain loads, four independent loads per thread in flight, then merges them.
+template <typename K, int XF>
+__device__ __forceinline__ void merge_tile(const K* __restrict__ A, int na, const K* __restrict__ B,
+                                           int nb, K* __restrict__ dst, bool final_pass, K* sm) {
+    const int t = threadIdx.x;
+    K* Bs = sm + pad32(na) + 1;
+    int e = t;
+    for (; e + 3 * kBlock < na; e += 4 * kBlock) {
+        const K x0 = A[e], x1 = A[e + kBlock], x2 = A[e + 2 * kBlock], x3 = A[e + 3 * kBlock];
+        sm[pad32(e)] = x0;
+        sm[pad32(e + kBlock)] = x1;
+        sm[pad32(e + 2 * kBlock)] = x2;
+        sm[pad32(e + 3 * kBlock)] = x3;
+    }
+    for (; e < na; e += kBlock) sm[pad32(e)] = A[e];
+    e = t;
+    for (; e + 3 * kBlock < nb; e += 4 * kBlock) {
+        const K x0 = B[e], x1 = B[e + kBlock], x2 = B[e + 2 * kBlock], x3 = B[e + 3 * kBlock];
+        Bs[pad32(e)] = x0;
+        Bs[pad32(e + kBlock)] = x1;
+        Bs[pad32(e + 2 * kBlock)] = x2;
+        Bs[pad32(e + 3 * kBlock)] = x3;
+    }
+    for (; e < nb; e += kBlock) Bs[pad32(e)] = B[e];
+    __syncthreads();
+    merge_spans<K, XF>(sm, na, Bs, nb, dst, final_pass);
+}
+
+// One CTA per kTilesPerCta output tiles of OT keys. Each of the first 2 x kTilesPerCta
+// warps finds one tile start or end on the merge path of the tile's run pair (a 32-ary
+// search over HBM, all searches in parallel, so the latency is paid once per four tiles);
+// the CTA then stages and merges its tiles in turn.
+constexpr int kTilesPerCta = 4;
+static_assert(2 * kTilesPerCta <= kBlock / 32, "one warp per split");
+
+template <typename K, int XF, bool FINAL>
+__global__ void __launch_bounds__(kBlock)
+k_merge(const K* __restrict__ src, K* __restrict__ dst, uint64_t n, uint64_t L, uint64_t tiles) {
+    constexpr int OT = kBlock * SortShape<K>::ITEMS;
+    __shared__ __align__(16) K sm[staged_elems(OT)];
+    __shared__ uint64_t s_split[2 * kTilesPerCta];
+    const uint64_t tile0 = (uint64_t)blockIdx.x * kTilesPerCta;
+    const int ntiles = (int)(tiles - tile0 < (uint64_t)kTilesPerCta ? tiles - tile0 : kTilesPerCta);
+    const int warp = threadIdx.x >> 5;
+    if (warp < 2 * ntiles) {
+        const uint64_t o = (tile0 + warp / 2) * OT;
+        const Pair p = pair_of(o, n, L);
+        const uint64_t pair_end = p.ps + p.la + p.lb;
+        const uint64_t d = (warp & 1) ? (o + OT < pair_end ? o + OT : pair_end) - p.ps : o - p.ps;
+        const uint64_t v = ((warp & 1) && d == p.la + p.lb) ? p.la
+                         : warp_merge_split(src + p.ps, p.la, src + p.ps + p.la, p.lb, d);
+        if ((threadIdx.x & 31) == 0) s_split[warp] = v;
     }
     __syncthreads();
-    for (int e = t; e < total; e += kBlock) {
-        const K v = so[(e % IPT) * (kBlock + 1) + e / IPT];
-        dst[o + e] = FINAL ? from_key<K, XF>(v) : v;
+    for (int k = 0; k < ntiles; ++k) {
+        const uint64_t o = (tile0 + k) * OT;
+        const Pair p = pair_of(o, n, L);
+        const uint64_t pair_end = p.ps + p.la + p.lb;
+        const uint64_t d0 = o - p.ps, d1 = (o + OT < pair_end ? o + OT : pair_end) - p.ps;
+        const uint64_t a_s = s_split[2 * k], a_e = s_split[2 * k + 1];
+        const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
+        if (k) __syncthreads();  // the previous tile's shared-memory reads are done
+        merge_tile<K, XF>(src + p.ps + a_s, (int)(a_e - a_s), src + p.ps + p.la + b_s,
+                          (int)(b_e - b_s), dst + o, FINAL, sm);
     }
 }
 
@@ -266,13 +336,9 @@ bool sort_keys(Workspace& ws, void* d_data, uint64_t n) {
     while ((uint64_t(1) << passes) < tiles) ++passes;
     K* data = static_cast<K*>(d_data);
     K* tmp = nullptr;
-    uint64_t* splits = nullptr;
     if (passes) {
-        const size_t key_bytes = (n * sizeof(K) + 255) / 256 * 256;
-        char* t = static_cast<char*>(ws.temp(key_bytes + (tiles + 1) * sizeof(uint64_t)));
-        if (!t) return false;
-        tmp = reinterpret_cast<K*>(t);
-        splits = reinterpret_cast<uint64_t*>(t + key_bytes);
+        tmp = static_cast<K*>(ws.temp(n * sizeof(K)));
+        if (!tmp) return false;
     }
     cudaStream_t s = ws.stream();
     K* cur = (passes % 2 == 0) ? data : tmp;
@@ -284,19 +350,15 @@ bool sort_keys(Workspace& ws, void* d_data, uint64_t n) {
     for (int pass = 1; pass <= passes; ++pass) {
         const uint64_t L = (uint64_t)TILE << (pass - 1);
         K* nxt = cur == data ? tmp : data;
-        const unsigned search_blocks = (unsigned)((tiles * 32 + kBlock - 1) / kBlock);
-        {
-            ProfScope prof(ws, "k_merge_path", 0);
-            k_merge_path<K><<<search_blocks, kBlock, 0, s>>>(cur, n, L, TILE, tiles, splits);
-        }
         {
             ProfScope prof(ws, "k_merge", 2 * n * sizeof(K));
+            const unsigned grid = (unsigned)((tiles + kTilesPerCta - 1) / kTilesPerCta);
             if (pass == passes)
-                k_merge<K, XF, true><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, splits);
+                k_merge<K, XF, true><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles);
             else
-                k_merge<K, XF, false><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, splits);
+                k_merge<K, XF, false><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles);
         }
-        count_launch(2);
+        count_launch(1);
         cur = nxt;
     }
     return cuda_ok(cudaGetLastError(), "sort launch");
@@ -364,99 +426,37 @@ k_seg_tile_sort(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start)
         if (row0 + r < cnt) dst[row0 + r] = g.P == 0 ? from_key<K, XF>(x[r]) : x[r];
 }
 
-template <typename K>
-__global__ void __launch_bounds__(kBlock)
-k_seg_merge_path(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start, int pass,
-                 uint64_t* __restrict__ splits) {
-    constexpr int TILE = kBlock * SortShape<K>::ITEMS;
-    const uint64_t wid = ((uint64_t)blockIdx.x * kBlock + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (wid >= item_start[S]) return;
-    const SegGeom<K> g = seg_geom<K>(src, S, item_start, (uint32_t)wid);
-    if (g.P < pass) return;
-    const K* srcb = g.loc(pass - 1);
-    const uint64_t L = (uint64_t)TILE << (pass - 1);
-    const uint64_t o = (uint64_t)g.k * TILE;
-    const Pair p = pair_of(o, g.len, L);
-    const uint64_t d = o - p.ps;
-    const K* A = srcb + p.ps;
-    const K* B = srcb + p.ps + p.la;
-    uint64_t lo = d > p.lb ? d - p.lb : 0;
-    uint64_t hi = d < p.la ? d : p.la;
-    while (hi - lo > 32) {
-        const uint64_t stride = (hi - lo + 31) / 32;
-        const uint64_t q = lo + (uint64_t)lane * stride;
-        const bool valid = q < hi;
-        const bool tr = valid && !(B[d - 1 - q] < A[q]);
-        const int c = __popc(__ballot_sync(0xffffffffu, tr));
-        const int nvalid = __popc(__ballot_sync(0xffffffffu, valid));
-        const uint64_t nlo = c ? lo + (uint64_t)(c - 1) * stride + 1 : lo;
-        const uint64_t nhi = c < nvalid ? lo + (uint64_t)c * stride : hi;
-        lo = nlo;
-        hi = nhi;
-    }
-    const uint64_t q = lo + lane;
-    const bool tr = q < hi && !(B[d - 1 - q] < A[q]);
-    const int c = __popc(__ballot_sync(0xffffffffu, tr));
-    if (lane == 0) splits[wid] = lo + c;
-}
-
+// One CTA per work item (output tile of OT keys) of every segment still merging in this
+// pass; like k_merge, warps 0 and 1 find the tile's span on the merge path first.
 template <typename K, int XF>
 __global__ void __launch_bounds__(kBlock)
-k_seg_merge(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start, int pass,
-            const uint64_t* __restrict__ splits) {
-    constexpr int IPT = SortShape<K>::ITEMS;
-    constexpr int OT = kBlock * IPT;
-    __shared__ K sm[OT];
-    __shared__ K so[IPT * (kBlock + 1)];
+k_seg_merge(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start, int pass) {
+    constexpr int OT = kBlock * SortShape<K>::ITEMS;
+    __shared__ __align__(16) K sm[staged_elems(OT)];
+    __shared__ uint64_t s_split[2];
     const uint32_t item = blockIdx.x;
     if (item >= item_start[S]) return;
     const SegGeom<K> g = seg_geom<K>(src, S, item_start, item);
     if (g.P < pass) return;
-    const bool final_pass = pass == g.P;
     const K* srcb = g.loc(pass - 1);
-    K* dst = g.loc(pass);
-    const int t = threadIdx.x;
     const uint64_t L = (uint64_t)OT << (pass - 1);
     const uint64_t o = (uint64_t)g.k * OT;
     const Pair p = pair_of(o, g.len, L);
     const uint64_t pair_end = p.ps + p.la + p.lb;
     const uint64_t tile_end = o + OT < pair_end ? o + OT : pair_end;
     const uint64_t d0 = o - p.ps, d1 = tile_end - p.ps;
-    const uint64_t a_s = splits[item];
-    const uint64_t a_e = o + OT < pair_end ? splits[item + 1] : p.la;
+    const int warp = threadIdx.x >> 5;
+    if (warp < 2) {
+        const uint64_t d = warp ? d1 : d0;
+        const uint64_t v = (warp && d1 == p.la + p.lb) ? p.la
+                         : warp_merge_split(srcb + p.ps, p.la, srcb + p.ps + p.la, p.lb, d);
+        if ((threadIdx.x & 31) == 0) s_split[warp] = v;
+    }
+    __syncthreads();
+    const uint64_t a_s = s_split[0], a_e = s_split[1];
     const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
-    const int na = (int)(a_e - a_s), nb = (int)(b_e - b_s);
-    const int total = na + nb;
-    const K* A = srcb + p.ps + a_s;
-    const K* B = srcb + p.ps + p.la + b_s;
-    for (int e = t; e < na; e += kBlock) sm[e] = A[e];
-    for (int e = t; e < nb; e += kBlock) sm[na + e] = B[e];
-    __syncthreads();
-    const int dt = t * IPT < total ? t * IPT : total;
-    int lo = dt > nb ? dt - nb : 0, hi = dt < na ? dt : na;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (!(sm[na + dt - 1 - mid] < sm[mid])) lo = mid + 1;
-        else hi = mid;
-    }
-    int i = lo, j = dt - lo;
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-        if (dt + k < total) {
-            bool take_a;
-            if (i >= na) take_a = false;
-            else if (j >= nb) take_a = true;
-            else take_a = !(sm[na + j] < sm[i]);
-            const K v = take_a ? sm[i++] : sm[na + j++];
-            so[k * (kBlock + 1) + t] = v;
-        }
-    }
-    __syncthreads();
-    for (int e = t; e < total; e += kBlock) {
-        const K v = so[(e % IPT) * (kBlock + 1) + e / IPT];
-        dst[o + e] = final_pass ? from_key<K, XF>(v) : v;
-    }
+    merge_tile<K, XF>(srcb + p.ps + a_s, (int)(a_e - a_s), srcb + p.ps + p.la + b_s,
+                      (int)(b_e - b_s), g.loc(pass) + o, pass == g.P, sm);
 }
 
 // Plans and sorts S segments: CSR (`src.offsets`; `count` = elements of the array) or
@@ -476,7 +476,7 @@ bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64
     auto up = [](size_t v) { return (v + 255) / 256 * 256; };
     const bool csr_tmp = src.offsets != nullptr;
     const size_t tmp_bytes = csr_tmp ? up(count * sizeof(K)) : 0;
-    char* t = static_cast<char*>(ws.temp(tmp_bytes + (items_cap + 1) * 8));
+    char* t = static_cast<char*>(ws.temp(tmp_bytes + 256));
     char* sb = static_cast<char*>(ws.seg(256 + up((S + 1) * 4)));
     // the epoch in counters[2] is shared with the other segmented launches, so a wrap
     // clears their status entries too
@@ -485,11 +485,10 @@ bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64
     if (csr_tmp) src.aux = reinterpret_cast<uint64_t>(t);
     src.aux_stride = 0;
     src.elem = sizeof(K);
-    uint64_t* splits = reinterpret_cast<uint64_t*>(t + tmp_bytes);
     uint32_t* counters = reinterpret_cast<uint32_t*>(sb);
     uint32_t* item_start = reinterpret_cast<uint32_t*>(sb + 256);
     ProfScope prof(ws, "segmented_sort", 2 * count * sizeof(K));
-    count_launch(2 + 2 * pass_bound);
+    count_launch(2 + pass_bound);
     auto enqueue = [&] {
         cudaStream_t s = ws.stream();
         k_seg_plan<kBlock><<<1, kBlock, 0, s>>>(src, S, count, (uint32_t)TILE, item_start, counters,
@@ -497,11 +496,8 @@ bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64
                                                 &ws.d_slot->spin_error);
         const unsigned grid = (unsigned)items_cap;
         k_seg_tile_sort<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start);
-        for (int pass = 1; pass <= pass_bound; ++pass) {
-            const unsigned sgrid = (unsigned)((items_cap * 32 + kBlock - 1) / kBlock);
-            k_seg_merge_path<K><<<sgrid, kBlock, 0, s>>>(src, S, item_start, pass, splits);
-            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, pass, splits);
-        }
+        for (int pass = 1; pass <= pass_bound; ++pass)
+            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, pass);
         return cuda_ok(cudaGetLastError(), "segmented sort launch");
     };
     if (!graph) return enqueue();

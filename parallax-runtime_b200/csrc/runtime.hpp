@@ -129,7 +129,8 @@ Workspace* new_workspace();  // an independent one (own stream and buffers), nev
 // Replays the CUDA graph cached under `key` on the workspace stream, capturing it first
 // (thread-local capture of what `enqueue` puts on the stream) when it is missing or was
 // captured before a buffer reallocation. `enqueue` must not grow workspace buffers.
-// Falls back to plain enqueueing when PARALLAX_GRAPHS=0 or a user stream is set.
+// Falls back to plain enqueueing when PARALLAX_GRAPHS=0 or the stream is being captured
+// by the caller (a parallax_set_stream stream inside the caller's own capture).
 bool graph_launch(Workspace& ws, const std::string& key, const std::function<bool()>& enqueue);
 
 // Waits for all work on the thread's stream with a deadline (PARALLAX_SYNC_TIMEOUT_MS,
