@@ -158,12 +158,13 @@ k_tile_sort(const K* in, K* out, uint64_t n, bool apply_inverse) {
 
 // ---- merge path ---------------------------------------------------------------------------
 // Pair geometry of output tile `o`: runs A = [ps, ps+la) and B = [ps+la, ps+la+lb).
+// L (the run length) is a power of two.
 struct Pair {
     uint64_t ps, la, lb;
 };
 __device__ __forceinline__ Pair pair_of(uint64_t o, uint64_t n, uint64_t L) {
     Pair p;
-    p.ps = o / (2 * L) * (2 * L);
+    p.ps = o & ~(2 * L - 1);
     const uint64_t r = n - p.ps;
     p.la = r < L ? r : L;
     const uint64_t r2 = r - p.la;
