@@ -20,6 +20,8 @@
 //   unique            stdpar.hpp:392-393
 //   argminmax / find / mismatch   src/kernel/kernel_launcher.cpp:987-1278 (first index
 //                                 of the extremum / match, `count` when none)
+// The modulo predicate x % m == r follows C (the remainder takes the sign of x) with m and
+// r converted to the element type; x % -1 is taken as 0 (C leaves MIN % -1 undefined).
 // Floating-point sums and prefixes are computed in fp64 with Neumaier compensation, the
 // reference against which fp32 results are held to 1e-5 and fp64 results to 1e-12
 // relative error (the fallback's own fp32 left fold stalls at 2^24 and is not used).
@@ -75,8 +77,13 @@ bool pred_eval(int kind, double c, int64_t ci, int64_t m, int64_t r, T x) {
         case P_NE: return x != cc;
         case P_NONZERO: return x != T(0);
         case P_MOD:
-            if constexpr (std::is_integral<T>::value) return x % (T)m == (T)r;
-            else return false;
+            if constexpr (std::is_integral<T>::value) {
+                // x % -1 is 0; the C expression overflows (traps) for the minimum value
+                if (std::is_signed<T>::value && (T)m == T(-1)) return T(0) == (T)r;
+                return x % (T)m == (T)r;
+            } else {
+                return false;
+            }
         default: return false;
     }
 }

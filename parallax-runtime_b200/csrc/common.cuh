@@ -13,6 +13,46 @@ namespace pxb {
 // [0, count] (in-kernel wait timeouts use small positive codes).
 constexpr int32_t kErrSegmentOffsets = 0x5e90;
 
+// x % m == r for 32-bit integers with C semantics (the remainder takes the sign of x),
+// dividing |x| by |m| as an invariant divisor: one multiply-high and two shifts
+// (Granlund & Montgomery 1994, "Division by invariant integers using multiplication",
+// Fig. 4.1: q = (t + ((n - t) >> sh1)) >> sh2, t = mulhi(magic, n)). am == 0 stands for a
+// modulus that is zero in the element type; nothing matches it.
+struct FastMod32 {
+    uint32_t am = 0, magic = 0, sh1 = 0, sh2 = 0;
+    static FastMod32 make(int64_t m) {  // m already converted to the element type
+        FastMod32 f;
+        const uint64_t d = (uint64_t)(m < 0 ? -m : m);
+        if (d == 0 || d > 0xffffffffull) return f;
+        uint32_t l = 0;
+        while (l < 32 && (1ull << l) < d) ++l;  // l = ceil(log2 d)
+        const unsigned __int128 num =
+            ((unsigned __int128)1 << 32) * (((unsigned __int128)1 << l) - d);
+        f.am = (uint32_t)d;
+        f.magic = (uint32_t)(num / d + 1);
+        f.sh1 = l < 1 ? l : 1;
+        f.sh2 = l > 1 ? l - 1 : 0;
+        return f;
+    }
+    __device__ __forceinline__ uint32_t rem(uint32_t n) const {
+        const uint32_t t = __umulhi(magic, n);
+        const uint32_t q = (t + ((n - t) >> sh1)) >> sh2;
+        return n - q * am;
+    }
+    template <typename T>
+    __device__ __forceinline__ bool eq(T x, T r) const {
+        static_assert(sizeof(T) == 4, "32-bit integers");
+        if (am == 0) return false;
+        if constexpr (T(-1) < T(0)) {  // signed
+            const bool neg = x < T(0);
+            const uint32_t ra = rem(neg ? 0u - (uint32_t)x : (uint32_t)x);
+            return (neg ? -(int64_t)ra : (int64_t)ra) == (int64_t)r;
+        } else {
+            return rem((uint32_t)x) == (uint32_t)r;
+        }
+    }
+};
+
 enum class DType : int { F32 = 0, F64 = 1, I32 = 2, I64 = 3, U32 = 4, U64 = 5, INVALID = -1 };
 
 inline __host__ __device__ size_t dtype_size(DType t) {

@@ -17,7 +17,8 @@
 // being packed), and writes them with coalesced stores. Traffic: n*s read + k*s written.
 // Partition writes every element: kept ones to [0, k), the rest in order to [k, n). The
 // rejected elements' offsets need k, so partition runs a count pass first (one read of
-// the input) and then writes both cursors straight from registers.
+// the input); each sub-tile is then permuted in shared memory (kept run, rejected run)
+// and both runs are written with coalesced stores.
 #include <stdint.h>
 
 #include <type_traits>
@@ -48,7 +49,7 @@ struct PredDev {
     PredKind kind;
     bool negate;
     T c, m, r;
-    double inv_m;  // 1.0 / m for the fast 32-bit remainder
+    FastMod32 fm;  // 32-bit element types: m as an invariant divisor
     __device__ __forceinline__ bool operator()(T x) const {
         bool v;
         switch (kind) {
@@ -90,19 +91,13 @@ struct PredDev {
         }
         return f;
     }
-    // x % m == r with C semantics; 32-bit integers divide through an exact fp64 quotient
-    // estimate plus a one-step remainder correction instead of the long integer division.
+    // x % m == r with C semantics; 32-bit integers divide by the precomputed invariant
+    // divisor instead of the long division.
     __device__ __forceinline__ bool mod_eq(T x) const {
         if constexpr (std::is_integral<T>::value && sizeof(T) == 4) {
-            const int64_t xi = (int64_t)x, mi = (int64_t)m;
-            const int64_t q = (int64_t)((double)xi * inv_m);
-            int64_t rr = xi - q * mi;
-            const int64_t am = mi < 0 ? -mi : mi;
-            if (xi >= 0) { if (rr < 0) rr += am; else if (rr >= am) rr -= am; }
-            else { if (rr > 0) rr -= am; else if (rr <= -am) rr += am; }
-            return rr == (int64_t)r;
-        } else if constexpr (std::is_integral<T>::value) {
-            return x % m == r;
+            return fm.eq(x, r);
+        } else if constexpr (std::is_integral<T>::value) {  // x % -1 == 0, no overflow
+            return (std::is_signed<T>::value && m == T(-1)) ? r == T(0) : x % m == r;
         } else {
             return false;
         }
@@ -195,21 +190,46 @@ __device__ __forceinline__ void compact_tile(T* buf, uint64_t* bars, uint32_t pa
     if (MODE != 2 && last_tile && tid == 0) *count_out = prefix + tile_kept;
 
     if constexpr (MODE == 2) {
-        // ---- partition: both cursors straight from registers ----
+        // ---- partition: per sub-tile, kept elements are packed at its front and the
+        // rejected ones after them (an in-place permutation of the sub-tile, done from
+        // registers after a barrier), then both runs are stored with coalesced writes:
+        // kept to [prefix + kept before the sub-tile, ...), rejected to
+        // [num_true + rejected before the sub-tile, ...).
         const uint64_t nt = *num_true;
         const uint64_t rej_base = nt + (base - prefix);
+        uint32_t sub_before[kSub + 1];  // kept elements of the tile before each sub-tile
+        {
+            const uint32_t v = sm.cnt[lane];
+            const uint32_t vi = warp_inclusive_scan(v, OpSum());
+            uint32_t vex = shfl_up(vi, 1);
+            if (lane == 0) vex = 0;
+#pragma unroll
+            for (int s = 0; s < kSub; ++s) sub_before[s] = shfl_idx(vex, s * WARPS);
+            sub_before[kSub] = tile_kept;
+        }
 #pragma unroll
         for (int s = 0; s < kSub; ++s) {
-            const uint32_t e0 = (uint32_t)s * SUB + row0;
+            const uint32_t s0 = (uint32_t)s * SUB;
+            const uint32_t ks = sub_before[s + 1] - sub_before[s];      // kept in sub-tile
+            const uint32_t valid = cnt > s0 ? (cnt - s0 < (uint32_t)SUB ? cnt - s0 : (uint32_t)SUB) : 0u;
+            T* sb = buf + s0;
             T x[ITEMS];
-            load_row<T, ITEMS, V>(buf + e0, x);
-            uint32_t r = woff[s] + tex[s];                    // kept before this row (tile)
-            uint32_t rf = e0 - r;                             // rejected before this row
+            load_row<T, ITEMS, V>(sb + row0, x);
+            __syncthreads();  // every row of sub-tile s is in registers before permuting
+            uint32_t rk = woff[s] + tex[s] - sub_before[s];  // kept before this row (sub-tile)
+            uint32_t rr = row0 - rk;                          // rejected before this row
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j) {
-                if (e0 + j >= cnt) break;
-                const uint64_t dst = (fl[s] >> j & 1u) ? prefix + r++ : rej_base + rf++;
-                if (dst < n) out[dst] = x[j];
+                if (row0 + j >= valid) break;
+                if (fl[s] >> j & 1u) sb[rk++] = x[j];
+                else sb[ks + rr++] = x[j];
+            }
+            __syncthreads();
+            const uint64_t kdst = prefix + sub_before[s];
+            const uint64_t rdst = rej_base + (s0 - sub_before[s]);
+            for (uint32_t i = tid; i < valid; i += kBlock) {
+                const uint64_t dst = i < ks ? kdst + i : rdst + (i - ks);
+                if (dst < n) out[dst] = sb[i];
                 else *ts.err = 3;  // only reachable after a failed wait: never write out of range
             }
         }
@@ -331,7 +351,7 @@ PredDev<T> make_pred(const Pred& p) {
     else e.c = (T)p.u;
     e.m = (T)p.mod_m;
     e.r = (T)p.mod_r;
-    e.inv_m = p.mod_m ? 1.0 / (double)p.mod_m : 0.0;
+    if (std::is_integral<T>::value && sizeof(T) == 4) e.fm = FastMod32::make((int64_t)e.m);
     return e;
 }
 

@@ -75,6 +75,7 @@ struct PredEval {
     bool negate;
     T c;
     T m, r;
+    FastMod32 fm;  // 32-bit element types: m as an invariant divisor
     __device__ __forceinline__ bool operator()(T x) const {
         bool v;
         switch (kind) {
@@ -92,7 +93,9 @@ struct PredEval {
     }
     template <typename U = T>
     __device__ __forceinline__ bool mod_eq(U x) const {
-        if constexpr (std::is_integral<U>::value) return x % m == r;
+        if constexpr (std::is_integral<U>::value && sizeof(U) == 4) return fm.eq(x, r);
+        else if constexpr (std::is_integral<U>::value)  // x % -1 == 0 (no overflowing division)
+            return (std::is_signed<U>::value && m == U(-1)) ? r == U(0) : x % m == r;
         else return false;
     }
 };
@@ -266,6 +269,7 @@ PredEval<T> make_pred(const Pred& p) {
     else e.c = (T)p.u;
     e.m = (T)p.mod_m;
     e.r = (T)p.mod_r;
+    if (std::is_integral<T>::value && sizeof(T) == 4) e.fm = FastMod32::make((int64_t)e.m);
     return e;
 }
 

@@ -282,6 +282,10 @@ Handle* parse_spec(const std::string& spec) {
         if (h.pred.kind == PredKind::MOD &&
             (h.dtype == DType::F32 || h.dtype == DType::F64))
             return nullptr;
+        // a modulus that is zero in a 32-bit element type (x % 0 has no meaning)
+        if (h.pred.kind == PredKind::MOD && (h.dtype == DType::I32 || h.dtype == DType::U32) &&
+            (uint32_t)h.pred.mod_m == 0)
+            return nullptr;
         h.kind = op == "copy_if" ? Kind::COMPACT_FLAGS
                : op == "remove_if" ? Kind::COMPACT_FLAGS
                : op == "partition" ? Kind::PARTITION_SCATTER

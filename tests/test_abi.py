@@ -111,6 +111,8 @@ def test_registered_spirv_for_fixed_funnel_still_resolves(lib):
     ("mismatch:i32", True), ("map:saxpy_gather_f32", True), ("map:affine_f32", True),
     ("reduce:avg:f32", False), ("scan:f16", False), ("copy_if:f32:mod:3:0", False),
     ("copy_if:i32:between:1", False), ("sort_kv:u64", False), ("map:nope", False), ("", False),
+    ("copy_if:i32:mod:4294967296:0", False), ("count_if:u32:mod:0:0", False),
+    ("copy_if:i64:mod:4294967296:0", True),
 ])
 def test_builtin_specs(lib, spec, ok):
     h = lib.parallax_builtin_kernel(spec.encode())

@@ -141,6 +141,29 @@ PREDS = [  # (spec tail, oracle kind, c, m, r)
 ]
 
 
+@pytest.mark.parametrize("t", ["i32", "u32", "i64"])
+@pytest.mark.parametrize("m", [1, 2, 3, 5, 7, 10, 641, 65537, 6700417, 2**31 - 1, -1, -3, -7,
+                               -(2**31) + 1, 2**31, 2**32 - 1, -(2**32) + 5])
+def test_modulo_predicate_divisors(lib, px, ox, dev, t, m):
+    """x % m == r through the multiply-high remainder (compaction and the count pass of
+    partition): every divisor class, both signs, the extreme values of the type."""
+    x = make(ox, t, 100003, seed=23)
+    info = np.iinfo(x.dtype)
+    x[:6] = np.array([0, 1, info.max, info.min, info.max - 1, info.min + 1]).astype(x.dtype)
+    if t == "i32":
+        x[6:8] = np.array([-1, -2], dtype=np.int32)
+    for r in (0, 1, 2, -1):
+        spec = f"copy_if:{t}:mod:{m}:{r}"
+        got, k = compact_dev(lib, px, dev, spec, x)
+        want, wk = ox.compact(x, ox.COPY_IF, ox.P_MOD, 0.0, m, r)
+        assert k == wk, (spec, k, wk)
+        assert np.array_equal(got[:k], want[:k]), spec
+        # partition counts with the count_if kernel first, then scatters both sides
+        got, k = compact_dev(lib, px, dev, f"partition:{t}:mod:{m}:{r}", x)
+        want, wk = ox.compact(x, ox.PARTITION, ox.P_MOD, 0.0, m, r)
+        assert k == wk and np.array_equal(got, want), f"partition {spec}"
+
+
 @pytest.mark.parametrize("t", list(DTYPES))
 @pytest.mark.parametrize("n", [1, 2, 33, 3072, 3073, 4097, 65543, (1 << 20) + 7])
 @pytest.mark.parametrize("mode", ["copy_if", "remove_if", "partition"])
