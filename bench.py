@@ -777,7 +777,7 @@ def run_map(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dic
 class LoadgenConfig(C.Structure):
     _fields_ = [("threads", C.c_uint32), ("mode", C.c_uint32), ("rate", C.c_double),
                 ("seconds", C.c_double), ("seed", C.c_uint64), ("log2_min", C.c_uint32),
-                ("log2_max", C.c_uint32), ("max_inflight", C.c_uint32), ("pad", C.c_uint32)]
+                ("log2_max", C.c_uint32), ("max_inflight", C.c_uint32), ("warmup", C.c_uint32)]
 
 
 class LoadgenResult(C.Structure):
@@ -792,7 +792,8 @@ def run_serving(px, lib, seconds: float) -> dict:
     sort / copy_if, n log-uniform 2^10..2^26, dtypes uniform over fp32/fp64/int32/int64,
     operands in device-resident arena blocks (seed 13). Per-call (one synchronous ABI call
     per request) against the serving loop, back-to-back (saturation; the served clients keep
-    up to 8 requests each outstanding) and at 70 % of the per-call saturation rate."""
+    up to 8 requests each outstanding) and at 70 % of the per-call saturation rate. Every
+    point starts with an untimed warm-up (one largest request of each operation per client)."""
     lg = C.CDLL(str(ROOT / "parallax-runtime_b200" / "lib" / "libparallax-loadgen.so"))
     lg.px_loadgen_prepare.argtypes = [C.c_uint64]
     lg.px_loadgen_run.argtypes = [C.POINTER(LoadgenConfig), C.POINTER(LoadgenResult)]
@@ -801,7 +802,8 @@ def run_serving(px, lib, seconds: float) -> dict:
 
     def one(mode, rate):
         cfg = LoadgenConfig(threads=16, mode=mode, rate=rate, seconds=seconds, seed=13,
-                            log2_min=10, log2_max=26, max_inflight=8 if rate <= 0 else 64)
+                            log2_min=10, log2_max=26, max_inflight=8 if rate <= 0 else 64,
+                            warmup=1)
         r = LoadgenResult()
         if lg.px_loadgen_run(C.byref(cfg), C.byref(r)) != px.OK:
             raise RuntimeError("loadgen run failed")

@@ -8,9 +8,9 @@
 // used by the serving loop to coalesce requests without moving their operands). A one-CTA
 // planner kernel turns the segment lengths into a tile work list (item_start[s] = first work
 // item of segment s; a segment of L elements has ceil(L / TILE) items) and writes the
-// results of empty segments. The persistent kernel's CTAs then claim work items from an
-// atomic counter in order, find their segment by binary search in item_start, and process
-// one tile each:
+// results of empty segments; a second small kernel inverts it (item -> segment). The
+// persistent kernel's CTAs then claim work items from an atomic counter in order, look up
+// their segment, and process one tile each:
 //   reduce   tile sum -> per-item partial; the last tile of a segment to finish (per-
 //            segment ticket) folds the segment's partials in item order (deterministic)
 //   scan     tile scan + decoupled look-back that stops at the segment's first tile
@@ -51,6 +51,7 @@ constexpr int SEG_COPY_IF = (int)SegKind::COPY_IF;
 // Device buffers of one segmented launch (the workspace's segment and status buffers).
 struct SegBuffers {
     uint32_t* item_start;  // num_segments + 1
+    uint32_t* item_seg;    // one per work item: its segment (k_seg_map)
     uint32_t* tickets;     // num_segments, zeroed by the planner
     uint64_t* partials;    // one per work item
     StatusEntry* status;   // one per work item (a buffer of its own)
@@ -134,7 +135,7 @@ k_segmented(SegSrc src, uint64_t S, SegBuffers b, T init, bool inclusive, SegPre
         if (tid == 0) {
             const uint32_t item = atomicAdd(&b.counters[0], 1u);
             s_item = item;
-            s_seg = item < total ? find_segment(b.item_start, S, item) : 0u;
+            s_seg = item < total ? b.item_seg[item] : 0u;
         }
         __syncthreads();
         const uint32_t item = s_item;
@@ -263,7 +264,8 @@ size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 // Carves the buffers for S segments and at most `items` work items out of the workspace's
 // segment buffer (zeroed when it is (re)allocated).
 bool seg_buffers(Workspace& ws, uint64_t S, uint64_t items, SegBuffers* out) {
-    const size_t need = 256 + up256((S + 1) * 4) + up256(S * 4) + up256(items * 8);
+    const size_t need = 256 + up256((S + 1) * 4) + up256(S * 4) + up256(items * 8) +
+                        up256(items * 4);
     char* p = static_cast<char*>(ws.seg(need));
     out->status = static_cast<StatusEntry*>(ws.seg_status(items));
     if (!p || !out->status) return false;
@@ -275,6 +277,8 @@ bool seg_buffers(Workspace& ws, uint64_t S, uint64_t items, SegBuffers* out) {
     out->tickets = reinterpret_cast<uint32_t*>(p);
     p += up256(S * 4);
     out->partials = reinterpret_cast<uint64_t*>(p);
+    p += up256(items * 8);
+    out->item_seg = reinterpret_cast<uint32_t*>(p);
     return true;
 }
 
@@ -301,6 +305,7 @@ bool enqueue_typed(Workspace& ws, const SegCall& c, const SegBuffers& b) {
                                             b.counters, empty,
                                             c.op == SEG_REDUCE ? b.tickets : nullptr, b.status,
                                             b.status_cap, err);
+    k_seg_map<256><<<seg_map_grid(c.S), 256, 0, s>>>(b.item_start, c.S, b.item_seg);
     T init;
     memcpy(&init, &c.init_bits, sizeof(T));
     SegPred<T> pr;
@@ -468,7 +473,7 @@ bool run(Workspace& ws, const SegCall& c, bool graph) {
     if (!reserve(ws, c)) return false;
     const size_t es = dtype_size(c.t);
     ProfScope prof(ws, op_name(c.op), (c.op == SEG_SCAN ? 2 : 1) * c.count * es);
-    count_launch(2);
+    count_launch(3);
     if (!graph) return enqueue(ws, c, items);
     return graph_launch(ws, graph_key(c, items), [&] { return enqueue(ws, c, items); });
 }

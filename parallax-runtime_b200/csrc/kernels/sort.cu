@@ -389,10 +389,10 @@ struct SegGeom {
     __device__ __forceinline__ K* loc(int q) const { return ((P - q) & 1) ? tmp : data; }
 };
 template <typename K>
-__device__ __forceinline__ SegGeom<K> seg_geom(const SegSrc& src, uint64_t S,
-                                               const uint32_t* item_start, uint32_t item) {
+__device__ __forceinline__ SegGeom<K> seg_geom(const SegSrc& src, const uint32_t* item_start,
+                                               const uint32_t* item_seg, uint32_t item) {
     SegGeom<K> g;
-    g.seg = find_segment(item_start, S, item);
+    g.seg = item_seg[item];
     g.first = item_start[g.seg];
     g.m = item_start[g.seg + 1] - g.first;
     g.k = item - g.first;
@@ -405,13 +405,14 @@ __device__ __forceinline__ SegGeom<K> seg_geom(const SegSrc& src, uint64_t S,
 
 template <typename K, int XF>
 __global__ void __launch_bounds__(kBlock)
-k_seg_tile_sort(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start) {
+k_seg_tile_sort(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start,
+                const uint32_t* __restrict__ item_seg) {
     constexpr int ITEMS = SortShape<K>::ITEMS;
     constexpr int TILE = kBlock * ITEMS;
     __shared__ K sm[TILE];
     const uint32_t item = blockIdx.x;
     if (item >= item_start[S]) return;
-    const SegGeom<K> g = seg_geom<K>(src, S, item_start, item);
+    const SegGeom<K> g = seg_geom<K>(src, item_start, item_seg, item);
     const int t = threadIdx.x, lane = t & 31, row0 = t * ITEMS;
     const uint64_t begin = (uint64_t)g.k * TILE;
     const uint64_t rem = g.len - begin;
@@ -431,13 +432,14 @@ k_seg_tile_sort(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start)
 // pass; like k_merge, warps 0 and 1 find the tile's span on the merge path first.
 template <typename K, int XF>
 __global__ void __launch_bounds__(kBlock)
-k_seg_merge(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start, int pass) {
+k_seg_merge(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start,
+            const uint32_t* __restrict__ item_seg, int pass) {
     constexpr int OT = kBlock * SortShape<K>::ITEMS;
     __shared__ __align__(16) K sm[staged_elems(OT)];
     __shared__ uint64_t s_split[2];
     const uint32_t item = blockIdx.x;
     if (item >= item_start[S]) return;
-    const SegGeom<K> g = seg_geom<K>(src, S, item_start, item);
+    const SegGeom<K> g = seg_geom<K>(src, item_start, item_seg, item);
     if (g.P < pass) return;
     const K* srcb = g.loc(pass - 1);
     const uint64_t L = (uint64_t)OT << (pass - 1);
@@ -478,7 +480,7 @@ bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64
     const bool csr_tmp = src.offsets != nullptr;
     const size_t tmp_bytes = csr_tmp ? up(count * sizeof(K)) : 0;
     char* t = static_cast<char*>(ws.temp(tmp_bytes + 256));
-    char* sb = static_cast<char*>(ws.seg(256 + up((S + 1) * 4)));
+    char* sb = static_cast<char*>(ws.seg(256 + up((S + 1) * 4) + up(items_cap * 4)));
     // the epoch in counters[2] is shared with the other segmented launches, so a wrap
     // clears their status entries too
     StatusEntry* st = static_cast<StatusEntry*>(ws.seg_status(1));
@@ -488,17 +490,19 @@ bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64
     src.elem = sizeof(K);
     uint32_t* counters = reinterpret_cast<uint32_t*>(sb);
     uint32_t* item_start = reinterpret_cast<uint32_t*>(sb + 256);
+    uint32_t* item_seg = reinterpret_cast<uint32_t*>(sb + 256 + up((S + 1) * 4));
     ProfScope prof(ws, "segmented_sort", 2 * count * sizeof(K));
-    count_launch(2 + pass_bound);
+    count_launch(3 + pass_bound);
     auto enqueue = [&] {
         cudaStream_t s = ws.stream();
         k_seg_plan<kBlock><<<1, kBlock, 0, s>>>(src, S, count, (uint32_t)TILE, item_start, counters,
                                                 SegEmpty::NONE, nullptr, st, ws.seg_status_cap,
                                                 &ws.d_slot->spin_error);
         const unsigned grid = (unsigned)items_cap;
-        k_seg_tile_sort<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start);
+        k_seg_map<256><<<seg_map_grid(S), 256, 0, s>>>(item_start, S, item_seg);
+        k_seg_tile_sort<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, item_seg);
         for (int pass = 1; pass <= pass_bound; ++pass)
-            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, pass);
+            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, item_seg, pass);
         return cuda_ok(cudaGetLastError(), "segmented sort launch");
     };
     if (!graph) return enqueue();

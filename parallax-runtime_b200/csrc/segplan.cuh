@@ -67,6 +67,23 @@ __device__ __forceinline__ uint32_t find_segment(const uint32_t* item_start, uin
     return (uint32_t)lo;
 }
 
+// Inverse of the work list: item_seg[i] = the segment of work item i, so a kernel finds
+// its segment with one load instead of a binary search. One thread per segment writes
+// that segment's items (grid-stride over segments).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_seg_map(const uint32_t* __restrict__ item_start, uint64_t S, uint32_t* __restrict__ item_seg) {
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < S;
+         s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = item_start[s], b = item_start[s + 1];
+        for (uint32_t i = a; i < b; ++i) item_seg[i] = (uint32_t)s;
+    }
+}
+inline unsigned seg_map_grid(uint64_t S) {  // for BLOCK = 256
+    const uint64_t g = (S + 255) / 256;
+    return (unsigned)(g < 1024 ? (g ? g : 1) : 1024);
+}
+
 // What the planner writes for an empty segment.
 enum class SegEmpty : int { NONE = 0, ZERO_RESULT = 1, ZERO_COUNT = 2 };
 

@@ -13,6 +13,9 @@
 // and freed when it completes (a request waits for its thread's oldest one when the arena is
 // full). Sort requests sort whatever the freshly allocated block holds (earlier requests'
 // bytes); this measures time only, results are checked by the tests.
+// With `warmup`, each client first runs one largest request of each operation untimed (so
+// per-thread and per-lane buffers that grow on first use are in place), then all clients
+// start one shared measured window.
 // Latency = completion - arrival time. The per-call path issues a thread's requests in
 // order, so a request that arrives while its thread is busy waits, as it would in a client
 // with one connection; the served path submits at arrival and collects completions on a
@@ -45,7 +48,9 @@ typedef struct px_loadgen_config {
     uint64_t seed;
     uint32_t log2_min, log2_max;
     uint32_t max_inflight;   /* served mode: outstanding requests per thread (64) */
-    uint32_t pad;
+    uint32_t warmup;         /* nonzero: every thread first runs one largest request of each
+                                operation (fp64), untimed, so buffers grown on first use are
+                                in place before the measured window */
 } px_loadgen_config;
 
 typedef struct px_loadgen_result {
@@ -217,7 +222,47 @@ struct ThreadOut {
     std::vector<Item> items;
 };
 
-void client(const px_loadgen_config& c, int tid, uint64_t t0, uint64_t t_end, ThreadOut* out) {
+// Start line: every client finishes its warm-up, then all share one measured window.
+struct StartLine {
+    std::mutex mu;
+    std::condition_variable cv;
+    uint32_t arrived = 0, expected = 0;
+    uint64_t t0 = 0, t_end = 0;
+    double seconds = 0;
+    void arrive_and_wait(uint64_t* t0_out, uint64_t* t_end_out) {
+        std::unique_lock<std::mutex> lk(mu);
+        if (++arrived == expected) {
+            t0 = now_ns() + 2000000;  // 2 ms for the clients to wake
+            t_end = t0 + (uint64_t)(seconds * 1e9);
+            cv.notify_all();
+        } else {
+            cv.wait(lk, [&] { return arrived == expected; });
+        }
+        *t0_out = t0;
+        *t_end_out = t_end;
+    }
+};
+
+void warm_up(const px_loadgen_config& c) {
+    for (int op = 0; op < 4; ++op) {
+        Item it;
+        it.op = op;
+        it.t = 1;  // fp64: the largest buffers
+        it.n = std::min<uint64_t>(1ull << c.log2_max, kPoolElems);
+        while (!alloc_buf(it)) std::this_thread::yield();
+        if (c.mode == 0) {
+            run_call(it);
+        } else if (submit(it) == PARALLAX_OK) {
+            parallax_serve_wait(it.ticket, nullptr);
+        }
+        free_buf(it);
+    }
+}
+
+void client(const px_loadgen_config& c, int tid, StartLine* line, ThreadOut* out) {
+    if (c.warmup) warm_up(c);
+    uint64_t t0, t_end;
+    line->arrive_and_wait(&t0, &t_end);
     Rng r{c.seed * 1000003ull + (uint64_t)tid * 7919ull};
     const double per_thread_rate = c.rate > 0 ? c.rate / c.threads : 0.0;
     uint64_t next_arrival = t0;
@@ -383,10 +428,11 @@ LG_EXPORT int px_loadgen_run(const px_loadgen_config* cfg, px_loadgen_result* re
     if (c.log2_min == 0) c.log2_min = 10;
     std::vector<ThreadOut> outs(c.threads);
     std::vector<std::thread> th;
-    const uint64_t t0 = now_ns() + 2000000;  // 2 ms for the threads to start
-    const uint64_t t_end = t0 + (uint64_t)(c.seconds * 1e9);
+    StartLine line;
+    line.expected = c.threads;
+    line.seconds = c.seconds;
     for (uint32_t i = 0; i < c.threads; ++i)
-        th.emplace_back(client, std::cref(c), (int)i, t0, t_end, &outs[i]);
+        th.emplace_back(client, std::cref(c), (int)i, &line, &outs[i]);
     for (auto& x : th) x.join();
     memset(res, 0, sizeof *res);
     std::vector<double> lat;
