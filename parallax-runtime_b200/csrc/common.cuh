@@ -12,6 +12,10 @@ namespace pxb {
 // Mapped error-word code of the segment planner: offsets not non-decreasing within
 // [0, count] (in-kernel wait timeouts use small positive codes).
 constexpr int32_t kErrSegmentOffsets = 0x5e90;
+// Mapped error-word code of the merge passes: a tile's two input spans on the merge path
+// were inconsistent (only possible if a run was not sorted); the tile is skipped instead of
+// staging outside its shared-memory buffer.
+constexpr int32_t kErrMergeSpan = 0x5e91;
 
 // x % m == r for 32-bit integers with C semantics (the remainder takes the sign of x),
 // dividing |x| by |m| as an invariant divisor: one multiply-high and two shifts

@@ -359,6 +359,10 @@ int sync_stream(Workspace& ws) {
     if (ws.h_slot->spin_error) {
         int code = ws.h_slot->spin_error;
         ws.h_slot->spin_error = 0;
+        if (code == kErrMergeSpan) {
+            set_error(PARALLAX_ERR_CUDA, "sort: a merge pass met an unsorted run (tile skipped)");
+            return PARALLAX_ERR_CUDA;
+        }
         if (code == kErrSegmentOffsets) {
             set_error(PARALLAX_ERR_INVALID_ARGUMENT,
                       "segment offsets must be non-decreasing and within [0, count]");

@@ -199,18 +199,26 @@ __device__ __forceinline__ uint64_t warp_merge_split(const K* __restrict__ A, ui
     return lo + __popc(__ballot_sync(0xffffffffu, tr));
 }
 
-// Shared-memory position of element i of a staged span: one padding slot per 32 elements.
-// Threads walk their merge-path segments at strides of about IPT / 2 to IPT elements
-// (8 or 16 for 4-byte keys), which would put a warp's loads in 2-4 banks; the padding
-// spreads those strides over all 32.
-__device__ __forceinline__ int pad32(int i) { return i + (i >> 5); }
-constexpr int staged_elems(int ot) { return ot + ot / 32 + 4; }
+// The spans of one output tile: [a_s, a_e) of run A and [b_s, b_e) of run B, at most ot
+// elements together. Sorted runs always give consistent spans; anything else is refused
+// before a single element is staged.
+__device__ __forceinline__ bool spans_ok(uint64_t a_s, uint64_t a_e, uint64_t b_s, uint64_t b_e,
+                                         int ot) {
+    return a_s <= a_e && b_s <= b_e && (a_e - a_s) + (b_e - b_s) <= (uint64_t)ot;
+}
 
-// Merges the sorted spans As and Bs (shared memory, padded positions, na + nb <= OT, A
-// wins ties) into dst[0, na + nb): every thread finds its start on the merge path by
-// binary search and merges its IPT outputs in registers (one shared load per output),
-// then stores them as 16-byte vectors (a thread's outputs are contiguous). Positions
-// pad32(na) of As and pad32(nb) of Bs must be readable (their values are ignored).
+// Staged layout of a tile's two spans in shared memory: A at [0, na), IPT sentinel keys
+// (all ones, the largest transformed key), B at [na + IPT, na + IPT + nb), IPT sentinels.
+// A thread whose run in one span is exhausted keeps reading sentinels, which never win
+// against a real key (a real key equal to the sentinel has the same bits, so either choice
+// writes the same output), so the merge loop needs no bounds checks.
+template <typename K>
+constexpr int staged_elems(int ot) { return ot + 2 * SortShape<K>::ITEMS + 8; }
+
+// Merges the sorted spans As[0, na) and Bs[0, nb) (shared memory, sentinels after each,
+// na + nb <= OT, A wins ties) into dst[0, na + nb): every thread finds its start on the
+// merge path by binary search and merges its IPT outputs in registers (one shared load per
+// output), then stores them as 16-byte vectors (a thread's outputs are contiguous).
 template <typename K, int XF>
 __device__ __forceinline__ void merge_spans(const K* As, int na, const K* Bs, int nb,
                                             K* __restrict__ dst, bool final_pass) {
@@ -221,20 +229,21 @@ __device__ __forceinline__ void merge_spans(const K* As, int na, const K* Bs, in
     int lo = dt > nb ? dt - nb : 0, hi = dt < na ? dt : na;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (!(Bs[pad32(dt - 1 - mid)] < As[pad32(mid)])) lo = mid + 1;
+        if (!(Bs[dt - 1 - mid] < As[mid])) lo = mid + 1;
         else hi = mid;
     }
-    int i = lo, j = dt - lo;
-    K a = As[pad32(i)];
-    K b = Bs[pad32(j)];
+    const K* pa = As + lo;
+    const K* pb = Bs + (dt - lo);
+    K a = *pa;
+    K b = *pb;
     K out[IPT];
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
-        const bool take_a = j >= nb || (i < na && !(b < a));
+        const bool take_a = !(b < a);
         out[k] = take_a ? a : b;
-        i += take_a;
-        j += !take_a;
-        const K x = take_a ? As[pad32(i)] : Bs[pad32(j)];
+        pa += take_a;
+        pb += !take_a;
+        const K x = *(take_a ? pa : pb);
         a = take_a ? x : a;
         b = take_a ? b : x;
     }
@@ -257,31 +266,34 @@ __device__ __forceinline__ void merge_spans(const K* As, int na, const K* Bs, in
     }
 }
 
-// Stages A[0, na) and B[0, nb) in sm (staged_elems(OT) elements, padded positions) with
+// Stages A[0, na) and B[0, nb) in sm (staged_elems(OT) elements, the layout above) with
 // coalesced plain loads, four independent loads per thread in flight, then merges them.
 template <typename K, int XF>
 __device__ __forceinline__ void merge_tile(const K* __restrict__ A, int na, const K* __restrict__ B,
                                            int nb, K* __restrict__ dst, bool final_pass, K* sm) {
+    constexpr int IPT = SortShape<K>::ITEMS;
     const int t = threadIdx.x;
-    K* Bs = sm + pad32(na) + 1;
+    K* Bs = sm + na + IPT;
     int e = t;
     for (; e + 3 * kBlock < na; e += 4 * kBlock) {
         const K x0 = A[e], x1 = A[e + kBlock], x2 = A[e + 2 * kBlock], x3 = A[e + 3 * kBlock];
-        sm[pad32(e)] = x0;
-        sm[pad32(e + kBlock)] = x1;
-        sm[pad32(e + 2 * kBlock)] = x2;
-        sm[pad32(e + 3 * kBlock)] = x3;
+        sm[e] = x0;
+        sm[e + kBlock] = x1;
+        sm[e + 2 * kBlock] = x2;
+        sm[e + 3 * kBlock] = x3;
     }
-    for (; e < na; e += kBlock) sm[pad32(e)] = A[e];
+    for (; e < na; e += kBlock) sm[e] = A[e];
     e = t;
     for (; e + 3 * kBlock < nb; e += 4 * kBlock) {
         const K x0 = B[e], x1 = B[e + kBlock], x2 = B[e + 2 * kBlock], x3 = B[e + 3 * kBlock];
-        Bs[pad32(e)] = x0;
-        Bs[pad32(e + kBlock)] = x1;
-        Bs[pad32(e + 2 * kBlock)] = x2;
-        Bs[pad32(e + 3 * kBlock)] = x3;
+        Bs[e] = x0;
+        Bs[e + kBlock] = x1;
+        Bs[e + 2 * kBlock] = x2;
+        Bs[e + 3 * kBlock] = x3;
     }
-    for (; e < nb; e += kBlock) Bs[pad32(e)] = B[e];
+    for (; e < nb; e += kBlock) Bs[e] = B[e];
+    if (t < IPT) sm[na + t] = ~K(0);
+    else if (t < 2 * IPT) Bs[nb + t - IPT] = ~K(0);
     __syncthreads();
     merge_spans<K, XF>(sm, na, Bs, nb, dst, final_pass);
 }
@@ -295,9 +307,10 @@ static_assert(2 * kTilesPerCta <= kBlock / 32, "one warp per split");
 
 template <typename K, int XF, bool FINAL>
 __global__ void __launch_bounds__(kBlock)
-k_merge(const K* __restrict__ src, K* __restrict__ dst, uint64_t n, uint64_t L, uint64_t tiles) {
+k_merge(const K* __restrict__ src, K* __restrict__ dst, uint64_t n, uint64_t L, uint64_t tiles,
+        volatile int32_t* err) {
     constexpr int OT = kBlock * SortShape<K>::ITEMS;
-    __shared__ __align__(16) K sm[staged_elems(OT)];
+    __shared__ __align__(16) K sm[staged_elems<K>(OT)];
     __shared__ uint64_t s_split[2 * kTilesPerCta];
     const uint64_t tile0 = (uint64_t)blockIdx.x * kTilesPerCta;
     const int ntiles = (int)(tiles - tile0 < (uint64_t)kTilesPerCta ? tiles - tile0 : kTilesPerCta);
@@ -320,6 +333,10 @@ k_merge(const K* __restrict__ src, K* __restrict__ dst, uint64_t n, uint64_t L, 
         const uint64_t a_s = s_split[2 * k], a_e = s_split[2 * k + 1];
         const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
         if (k) __syncthreads();  // the previous tile's shared-memory reads are done
+        if (!spans_ok(a_s, a_e, b_s, b_e, OT)) {  // CTA-uniform
+            if (threadIdx.x == 0) *err = kErrMergeSpan;
+            continue;
+        }
         merge_tile<K, XF>(src + p.ps + a_s, (int)(a_e - a_s), src + p.ps + p.la + b_s,
                           (int)(b_e - b_s), dst + o, FINAL, sm);
     }
@@ -354,10 +371,11 @@ bool sort_keys(Workspace& ws, void* d_data, uint64_t n) {
         {
             ProfScope prof(ws, "k_merge", 2 * n * sizeof(K));
             const unsigned grid = (unsigned)((tiles + kTilesPerCta - 1) / kTilesPerCta);
+            volatile int32_t* err = &ws.d_slot->spin_error;
             if (pass == passes)
-                k_merge<K, XF, true><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles);
+                k_merge<K, XF, true><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles, err);
             else
-                k_merge<K, XF, false><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles);
+                k_merge<K, XF, false><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles, err);
         }
         count_launch(1);
         cur = nxt;
@@ -433,9 +451,9 @@ k_seg_tile_sort(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start,
 template <typename K, int XF>
 __global__ void __launch_bounds__(kBlock)
 k_seg_merge(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start,
-            const uint32_t* __restrict__ item_seg, int pass) {
+            const uint32_t* __restrict__ item_seg, int pass, volatile int32_t* err) {
     constexpr int OT = kBlock * SortShape<K>::ITEMS;
-    __shared__ __align__(16) K sm[staged_elems(OT)];
+    __shared__ __align__(16) K sm[staged_elems<K>(OT)];
     __shared__ uint64_t s_split[2];
     const uint32_t item = blockIdx.x;
     if (item >= item_start[S]) return;
@@ -458,6 +476,10 @@ k_seg_merge(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start,
     __syncthreads();
     const uint64_t a_s = s_split[0], a_e = s_split[1];
     const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
+    if (!spans_ok(a_s, a_e, b_s, b_e, OT)) {  // CTA-uniform
+        if (threadIdx.x == 0) *err = kErrMergeSpan;
+        return;
+    }
     merge_tile<K, XF>(srcb + p.ps + a_s, (int)(a_e - a_s), srcb + p.ps + p.la + b_s,
                       (int)(b_e - b_s), g.loc(pass) + o, pass == g.P, sm);
 }
@@ -502,7 +524,8 @@ bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64
         k_seg_map<256><<<seg_map_grid(S), 256, 0, s>>>(item_start, S, item_seg);
         k_seg_tile_sort<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, item_seg);
         for (int pass = 1; pass <= pass_bound; ++pass)
-            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, item_seg, pass);
+            k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, item_seg, pass,
+                                                       &ws.d_slot->spin_error);
         return cuda_ok(cudaGetLastError(), "segmented sort launch");
     };
     if (!graph) return enqueue();
