@@ -824,11 +824,16 @@ def run_serving(px, lib, seconds: float) -> dict:
         lib.parallax_serve_get_stats(C.byref(st))
         lib.parallax_serve_stop()
         out["per_call_at_rate"] = one(0, rate)
+        # one call at a time: how a runtime that is not thread-safe (the reference's,
+        # src/kernel/kernel_launcher.hpp:172-176) has to be driven by 16 client threads
+        out["per_call_serialized_saturation"] = one(2, 0.0)
         out["serve_stats"] = {"requests": st.requests, "batches": st.batches,
                               "coalesced_requests": st.coalesced_requests,
                               "max_batch": st.max_batch, "memory_waits": st.memory_waits}
         out["throughput_ratio_saturation"] = round(
             out["served_saturation"]["req_s"] / out["per_call_saturation"]["req_s"], 3)
+        out["throughput_ratio_vs_serialized"] = round(
+            out["served_saturation"]["req_s"] / out["per_call_serialized_saturation"]["req_s"], 3)
     finally:
         lib.parallax_serve_stop()
         lg.px_loadgen_release()

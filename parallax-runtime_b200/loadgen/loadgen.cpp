@@ -42,7 +42,9 @@
 extern "C" {
 typedef struct px_loadgen_config {
     uint32_t threads;        /* client threads (16) */
-    uint32_t mode;           /* 0 per-call, 1 served */
+    uint32_t mode;           /* 0 per-call, 1 served, 2 per-call serialized by one lock
+                                (one call at a time, as a runtime that is not thread-safe
+                                must be driven) */
     double rate;             /* offered requests/s over all threads; <= 0: back-to-back */
     double seconds;          /* issuing window */
     uint64_t seed;
@@ -149,6 +151,8 @@ void free_buf(Item& it) {
 }
 
 // ---- per-call path: one synchronous ABI call ---------------------------------------------
+std::mutex g_call_mu;  // mode 2: one call at a time
+
 int run_call(Item& it) {
     const int t = it.t;
     const size_t s = kSize[t];
@@ -250,7 +254,7 @@ void warm_up(const px_loadgen_config& c) {
         it.t = 1;  // fp64: the largest buffers
         it.n = std::min<uint64_t>(1ull << c.log2_max, kPoolElems);
         while (!alloc_buf(it)) std::this_thread::yield();
-        if (c.mode == 0) {
+        if (c.mode != 1) {
             run_call(it);
         } else if (submit(it) == PARALLAX_OK) {
             parallax_serve_wait(it.ticket, nullptr);
@@ -273,7 +277,7 @@ void client(const px_loadgen_config& c, int tid, StartLine* line, ThreadOut* out
         }
     };
     advance();
-    if (c.mode == 0) {
+    if (c.mode == 0 || c.mode == 2) {
         sleep_until(t0);
         for (;;) {
             Item it = make_item(r, c);
@@ -281,7 +285,12 @@ void client(const px_loadgen_config& c, int tid, StartLine* line, ThreadOut* out
             if (it.arrival >= t_end) break;
             sleep_until(it.arrival);
             while (!alloc_buf(it)) std::this_thread::yield();
-            it.status = run_call(it);
+            if (c.mode == 2) {
+                std::lock_guard<std::mutex> g(g_call_mu);
+                it.status = run_call(it);
+            } else {
+                it.status = run_call(it);
+            }
             it.done = now_ns();
             free_buf(it);
             out->items.push_back(it);
