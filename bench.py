@@ -541,10 +541,8 @@ def main() -> None:
     step_ms = sum(statistics.fmean(op.times) for op in ops)
     bytes_step = sum(op.bytes_fn() for op in ops)
     if dist:
-        t = torch.tensor([step_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
-    value = world * bytes_step / (step_ms * 1e-3) / 1e9
+        step_ms = max_over_ranks(dist, torch, step_ms, "cuda")
+    value = job_gbs(world, bytes_step, step_ms)
     peak, peak_kind = hbm_peak()
 
     per_prim = {}
@@ -604,6 +602,18 @@ def main() -> None:
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def max_over_ranks(dist, torch, ms: float, device: str) -> float:
+    """The slowest rank's step time (every rank takes part; all get the result)."""
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gbs(world: int, bytes_per_rank_step: float, step_ms: float) -> float:
+    """Whole-job algorithmic GB/s: every rank (replica) moves its own step's bytes."""
+    return world * bytes_per_rank_step / (step_ms * 1e-3) / 1e9
 
 
 def traffic_from_profiles(kernel: str, alg_bytes: float):

@@ -207,13 +207,19 @@ __device__ __forceinline__ bool spans_ok(uint64_t a_s, uint64_t a_e, uint64_t b_
     return a_s <= a_e && b_s <= b_e && (a_e - a_s) + (b_e - b_s) <= (uint64_t)ot;
 }
 
-// Staged layout of a tile's two spans in shared memory: A at [0, na), IPT sentinel keys
-// (all ones, the largest transformed key), B at [na + IPT, na + IPT + nb), IPT sentinels.
-// A thread whose run in one span is exhausted keeps reading sentinels, which never win
-// against a real key (a real key equal to the sentinel has the same bits, so either choice
-// writes the same output), so the merge loop needs no bounds checks.
+// Staged layout of a tile's two spans in shared memory: each span keeps the position of
+// its first element within a 16-byte word (its phase), so it is staged with aligned
+// 16-byte vector loads and stores: A[i] at sm[pa + i] (pa = A's phase), IPT sentinel keys
+// (all ones, the largest transformed key) after it, B[j] at sm[bb + pb + j] (bb a
+// 16-byte-aligned start after A's sentinels), IPT sentinels after B. A thread whose run in
+// one span is exhausted keeps reading sentinels, which never win against a real key (a real
+// key equal to the sentinel has the same bits, so either choice writes the same output),
+// so the merge loop needs no bounds checks. The vectors at a span's two ends may carry up
+// to 16 - sizeof(K) bytes from outside the span; an aligned 16-byte word that holds one
+// byte of the span lies in the same memory page, so those reads cannot fault, and the
+// extra elements land in slots that the sentinels overwrite or nothing reads.
 template <typename K>
-constexpr int staged_elems(int ot) { return ot + 2 * SortShape<K>::ITEMS + 8; }
+constexpr int staged_elems(int ot) { return ot + 2 * SortShape<K>::ITEMS + 4 * (16 / (int)sizeof(K)); }
 
 // Merges the sorted spans As[0, na) and Bs[0, nb) (shared memory, sentinels after each,
 // na + nb <= OT, A wins ties) into dst[0, na + nb): every thread finds its start on the
@@ -267,35 +273,41 @@ __device__ __forceinline__ void merge_spans(const K* As, int na, const K* Bs, in
 }
 
 // Stages A[0, na) and B[0, nb) in sm (staged_elems(OT) elements, the layout above) with
-// coalesced plain loads, four independent loads per thread in flight, then merges them.
+// aligned 16-byte loads, all of a thread's vectors of both spans in flight at once, then
+// merges them.
 template <typename K, int XF>
 __device__ __forceinline__ void merge_tile(const K* __restrict__ A, int na, const K* __restrict__ B,
                                            int nb, K* __restrict__ dst, bool final_pass, K* sm) {
     constexpr int IPT = SortShape<K>::ITEMS;
+    constexpr int V = 16 / sizeof(K);
+    constexpr int OT = kBlock * IPT;
+    constexpr int MAXV = (OT + 2 * V) / V / kBlock + 1;  // vectors per thread, both spans
     const int t = threadIdx.x;
-    K* Bs = sm + na + IPT;
-    int e = t;
-    for (; e + 3 * kBlock < na; e += 4 * kBlock) {
-        const K x0 = A[e], x1 = A[e + kBlock], x2 = A[e + 2 * kBlock], x3 = A[e + 3 * kBlock];
-        sm[e] = x0;
-        sm[e + kBlock] = x1;
-        sm[e + 2 * kBlock] = x2;
-        sm[e + 3 * kBlock] = x3;
+    const int pa = (int)((reinterpret_cast<uintptr_t>(A) / sizeof(K)) % V);
+    const int pb = (int)((reinterpret_cast<uintptr_t>(B) / sizeof(K)) % V);
+    const int nva = na ? (pa + na + V - 1) / V : 0;
+    const int nvb = nb ? (pb + nb + V - 1) / V : 0;
+    const int bb = (pa + na + IPT + V - 1) / V * V;  // B's vector-aligned start
+    const uint4* Av = reinterpret_cast<const uint4*>(A - pa);
+    const uint4* Bv = reinterpret_cast<const uint4*>(B - pb);
+    uint4 r[MAXV];
+#pragma unroll
+    for (int k = 0; k < MAXV; ++k) {
+        const int v = t + k * kBlock;
+        if (v < nva) r[k] = Av[v];
+        else if (v < nva + nvb) r[k] = Bv[v - nva];
     }
-    for (; e < na; e += kBlock) sm[e] = A[e];
-    e = t;
-    for (; e + 3 * kBlock < nb; e += 4 * kBlock) {
-        const K x0 = B[e], x1 = B[e + kBlock], x2 = B[e + 2 * kBlock], x3 = B[e + 3 * kBlock];
-        Bs[e] = x0;
-        Bs[e + kBlock] = x1;
-        Bs[e + 2 * kBlock] = x2;
-        Bs[e + 3 * kBlock] = x3;
+#pragma unroll
+    for (int k = 0; k < MAXV; ++k) {
+        const int v = t + k * kBlock;
+        if (v < nva) reinterpret_cast<uint4*>(sm)[v] = r[k];
+        else if (v < nva + nvb) reinterpret_cast<uint4*>(sm + bb)[v - nva] = r[k];
     }
-    for (; e < nb; e += kBlock) Bs[e] = B[e];
-    if (t < IPT) sm[na + t] = ~K(0);
-    else if (t < 2 * IPT) Bs[nb + t - IPT] = ~K(0);
+    __syncthreads();  // the vectors' extra elements are in place before the sentinels
+    if (t < IPT) sm[pa + na + t] = ~K(0);
+    else if (t < 2 * IPT) sm[bb + pb + nb + t - IPT] = ~K(0);
     __syncthreads();
-    merge_spans<K, XF>(sm, na, Bs, nb, dst, final_pass);
+    merge_spans<K, XF>(sm + pa, na, sm + bb + pb, nb, dst, final_pass);
 }
 
 // One CTA per kTilesPerCta output tiles of OT keys. Each of the first 2 x kTilesPerCta

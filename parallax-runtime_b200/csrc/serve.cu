@@ -17,8 +17,9 @@
 //     element type, predicate, scan flavour) up to `solo_elements` long become ONE
 //     segmented launch over per-request descriptors (segmented.cu, sort.cu): a planner plus
 //     one persistent kernel, or the per-segment merge passes of the segmented sort. Longer
-//     requests, and kinds without a segmented form (reduce max/min, modulo predicates,
-//     unique, partition), run alone through the plain launchers.
+//     requests, kinds without a segmented form (reduce max/min, modulo predicates, unique,
+//     partition), and a request that finds no partner run alone through the plain
+//     launchers.
 // Requests that arrive while others are on the device are admitted into the next free
 // lane, so batches overlap on the device; a request's result does not depend on what it
 // was batched with (integer results are bit-exact, floating-point ones are within the
@@ -211,7 +212,7 @@ class Server {
         const Request& h = *l.reqs[0];
         const size_t S = l.reqs.size();
         cudaStream_t s = ws.stream();
-        if (!h.coalescible) {
+        if (!h.coalescible || S == 1) {  // one request: the plain launcher (fewer launches)
             l.h_res[0] = 0;
             switch (h.op) {
                 case ReqOp::REDUCE: return launch_reduce(ws, h.t, h.red, h.d_in, h.n, l.d_res);
@@ -264,7 +265,7 @@ class Server {
         for (size_t i = 0; i < l.reqs.size(); ++i) {
             Request* r = l.reqs[i];
             if (status == PARALLAX_OK && r->result) {
-                const uint64_t v = l.h_res[r->coalescible ? i : 0];
+                const uint64_t v = l.h_res[l.reqs.size() > 1 ? i : 0];
                 if (r->op == ReqOp::REDUCE) memcpy(r->result, &v, r->es);
                 else if (r->op == ReqOp::COMPACT) memcpy(r->result, &v, 8);
             }
@@ -311,7 +312,7 @@ class Server {
                 l.busy = true;
                 ++stats.batches;
                 if (l.reqs.size() > stats.max_batch) stats.max_batch = l.reqs.size();
-                if (l.reqs[0]->coalescible) stats.coalesced_requests += l.reqs.size();
+                if (l.reqs.size() > 1) stats.coalesced_requests += l.reqs.size();
                 else ++stats.solo_batches;
                 lk.unlock();
                 set_ok();

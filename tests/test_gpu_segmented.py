@@ -273,3 +273,46 @@ def test_zero_segments_is_a_no_op(lib, px, dev):
                                          off.data_ptr(), 0, r.data_ptr()) == px.OK
     assert lib.parallax_segmented_sort(px.builtin("sort:f32"), x.data_ptr(), 0,
                                        off.data_ptr(), 0) == px.OK
+
+
+_TUNE_SCRIPT = r'''
+import ctypes as C, importlib.util, sys
+import numpy as np, torch
+spec = importlib.util.spec_from_file_location("parallax_runtime_b200", sys.argv[1])
+px = importlib.util.module_from_spec(spec); spec.loader.exec_module(px)
+lib = px.load()
+off = np.array([0, 70000, 70001, 200000], np.uint64)
+x = torch.ones(200000, dtype=torch.float32, device="cuda")
+o = torch.from_numpy(off.view(np.uint8)).cuda()
+r = torch.zeros(3, dtype=torch.float32, device="cuda")
+lib.parallax_segmented_reduce(px.builtin("reduce:sum:f32"), x.data_ptr(), 200000, o.data_ptr(), 3,
+                              r.data_ptr())
+px.check("tuned reduce")
+assert r.cpu().tolist() == [70000.0, 1.0, 129999.0], r
+'''
+
+
+def test_tuner_cache_is_written_and_reused(tmp_path):
+    """The autotuner times the tile candidates once per (op, type, size bucket), stores the
+    choice in PARALLAX_TUNE_CACHE, and a later process reuses it without timing."""
+    import os
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+    cache = tmp_path / "tune.txt"
+    script = tmp_path / "run.py"
+    script.write_text(_TUNE_SCRIPT)
+    env = dict(os.environ, PARALLAX_TUNE_CACHE=str(cache), PARALLAX_DEBUG="1")
+    env.pop("PARALLAX_TUNE", None)
+    pkg = str(ROOT / "parallax-runtime_b200" / "__init__.py")
+    r1 = subprocess.run([sys.executable, str(script), pkg], env=env, capture_output=True,
+                        text=True, timeout=300)
+    assert r1.returncode == 0, r1.stderr[-2000:]
+    assert "tuned segmented op 0" in r1.stderr
+    entries = [ln.split() for ln in cache.read_text().splitlines() if ln.strip()]
+    assert entries and all(len(e) == 4 and e[3] in ("4", "8", "16") for e in entries)
+    r2 = subprocess.run([sys.executable, str(script), pkg], env=env, capture_output=True,
+                        text=True, timeout=300)
+    assert r2.returncode == 0, r2.stderr[-2000:]
+    assert "tuned segmented op" not in r2.stderr
