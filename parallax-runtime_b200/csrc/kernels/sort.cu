@@ -272,42 +272,71 @@ __device__ __forceinline__ void merge_spans(const K* As, int na, const K* Bs, in
     }
 }
 
+// Where a tile's two spans sit in the staged layout above.
+struct SpanPlace {
+    int pa, pb;    // phases (element offset within a 16-byte word)
+    int nva, nvb;  // 16-byte vectors per span
+    int bb;        // B's vector-aligned start
+};
+template <typename K>
+__device__ __forceinline__ SpanPlace span_place(const K* A, int na, const K* B, int nb) {
+    constexpr int IPT = SortShape<K>::ITEMS;
+    constexpr int V = 16 / sizeof(K);
+    SpanPlace q;
+    q.pa = (int)((reinterpret_cast<uintptr_t>(A) / sizeof(K)) % V);
+    q.pb = (int)((reinterpret_cast<uintptr_t>(B) / sizeof(K)) % V);
+    q.nva = na ? (q.pa + na + V - 1) / V : 0;
+    q.nvb = nb ? (q.pb + nb + V - 1) / V : 0;
+    q.bb = (q.pa + na + IPT + V - 1) / V * V;
+    return q;
+}
+template <typename K>
+constexpr int stage_vectors() {  // vectors per thread over both spans
+    return (kBlock * SortShape<K>::ITEMS + 2 * (16 / (int)sizeof(K))) / (16 / (int)sizeof(K)) /
+               kBlock + 1;
+}
+// Issues a thread's aligned 16-byte loads of both spans into registers.
+template <typename K>
+__device__ __forceinline__ void stage_load(const K* A, const K* B, const SpanPlace& q,
+                                           uint4 (&r)[stage_vectors<K>()]) {
+    const uint4* Av = reinterpret_cast<const uint4*>(A - q.pa);
+    const uint4* Bv = reinterpret_cast<const uint4*>(B - q.pb);
+#pragma unroll
+    for (int k = 0; k < stage_vectors<K>(); ++k) {
+        const int v = threadIdx.x + k * kBlock;
+        if (v < q.nva) r[k] = Av[v];
+        else if (v < q.nva + q.nvb) r[k] = Bv[v - q.nva];
+    }
+}
+// Stores the registers into the staged layout and adds the sentinels (two barriers).
+template <typename K>
+__device__ __forceinline__ void stage_store(K* sm, int na, int nb, const SpanPlace& q,
+                                            const uint4 (&r)[stage_vectors<K>()]) {
+    constexpr int IPT = SortShape<K>::ITEMS;
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < stage_vectors<K>(); ++k) {
+        const int v = t + k * kBlock;
+        if (v < q.nva) reinterpret_cast<uint4*>(sm)[v] = r[k];
+        else if (v < q.nva + q.nvb) reinterpret_cast<uint4*>(sm + q.bb)[v - q.nva] = r[k];
+    }
+    __syncthreads();  // the vectors' extra elements are in place before the sentinels
+    if (t < IPT) sm[q.pa + na + t] = ~K(0);
+    else if (t < 2 * IPT) sm[q.bb + q.pb + nb + t - IPT] = ~K(0);
+    __syncthreads();
+}
+
 // Stages A[0, na) and B[0, nb) in sm (staged_elems(OT) elements, the layout above) with
 // aligned 16-byte loads, all of a thread's vectors of both spans in flight at once, then
 // merges them.
 template <typename K, int XF>
 __device__ __forceinline__ void merge_tile(const K* __restrict__ A, int na, const K* __restrict__ B,
                                            int nb, K* __restrict__ dst, bool final_pass, K* sm) {
-    constexpr int IPT = SortShape<K>::ITEMS;
-    constexpr int V = 16 / sizeof(K);
-    constexpr int OT = kBlock * IPT;
-    constexpr int MAXV = (OT + 2 * V) / V / kBlock + 1;  // vectors per thread, both spans
-    const int t = threadIdx.x;
-    const int pa = (int)((reinterpret_cast<uintptr_t>(A) / sizeof(K)) % V);
-    const int pb = (int)((reinterpret_cast<uintptr_t>(B) / sizeof(K)) % V);
-    const int nva = na ? (pa + na + V - 1) / V : 0;
-    const int nvb = nb ? (pb + nb + V - 1) / V : 0;
-    const int bb = (pa + na + IPT + V - 1) / V * V;  // B's vector-aligned start
-    const uint4* Av = reinterpret_cast<const uint4*>(A - pa);
-    const uint4* Bv = reinterpret_cast<const uint4*>(B - pb);
-    uint4 r[MAXV];
-#pragma unroll
-    for (int k = 0; k < MAXV; ++k) {
-        const int v = t + k * kBlock;
-        if (v < nva) r[k] = Av[v];
-        else if (v < nva + nvb) r[k] = Bv[v - nva];
-    }
-#pragma unroll
-    for (int k = 0; k < MAXV; ++k) {
-        const int v = t + k * kBlock;
-        if (v < nva) reinterpret_cast<uint4*>(sm)[v] = r[k];
-        else if (v < nva + nvb) reinterpret_cast<uint4*>(sm + bb)[v - nva] = r[k];
-    }
-    __syncthreads();  // the vectors' extra elements are in place before the sentinels
-    if (t < IPT) sm[pa + na + t] = ~K(0);
-    else if (t < 2 * IPT) sm[bb + pb + nb + t - IPT] = ~K(0);
-    __syncthreads();
-    merge_spans<K, XF>(sm + pa, na, sm + bb + pb, nb, dst, final_pass);
+    const SpanPlace q = span_place(A, na, B, nb);
+    uint4 r[stage_vectors<K>()];
+    stage_load(A, B, q, r);
+    stage_store(sm, na, nb, q, r);
+    merge_spans<K, XF>(sm + q.pa, na, sm + q.bb + q.pb, nb, dst, final_pass);
 }
 
 // One CTA per kTilesPerCta output tiles of OT keys. Each of the first 2 x kTilesPerCta
@@ -337,20 +366,45 @@ k_merge(const K* __restrict__ src, K* __restrict__ dst, uint64_t n, uint64_t L, 
         if ((threadIdx.x & 31) == 0) s_split[warp] = v;
     }
     __syncthreads();
-    for (int k = 0; k < ntiles; ++k) {
+    struct Span {
+        const K* a;
+        const K* b;
+        int na, nb;
+        bool ok;
+    };
+    auto span = [&](int k) {
         const uint64_t o = (tile0 + k) * OT;
         const Pair p = pair_of(o, n, L);
         const uint64_t pair_end = p.ps + p.la + p.lb;
         const uint64_t d0 = o - p.ps, d1 = (o + OT < pair_end ? o + OT : pair_end) - p.ps;
         const uint64_t a_s = s_split[2 * k], a_e = s_split[2 * k + 1];
         const uint64_t b_s = d0 - a_s, b_e = d1 - a_e;
+        Span sp;
+        sp.ok = spans_ok(a_s, a_e, b_s, b_e, OT);  // else refused, never staged
+        sp.a = src + p.ps + a_s;
+        sp.b = src + p.ps + p.la + b_s;
+        sp.na = sp.ok ? (int)(a_e - a_s) : 0;
+        sp.nb = sp.ok ? (int)(b_e - b_s) : 0;
+        return sp;
+    };
+    // The next tile's vectors are loaded into registers while the current tile merges.
+    uint4 r[stage_vectors<K>()];
+    Span cur = span(0);
+    SpanPlace q = span_place(cur.a, cur.na, cur.b, cur.nb);
+    stage_load(cur.a, cur.b, q, r);
+    for (int k = 0; k < ntiles; ++k) {
         if (k) __syncthreads();  // the previous tile's shared-memory reads are done
-        if (!spans_ok(a_s, a_e, b_s, b_e, OT)) {  // CTA-uniform
-            if (threadIdx.x == 0) *err = kErrMergeSpan;
-            continue;
+        if (!cur.ok && threadIdx.x == 0) *err = kErrMergeSpan;
+        stage_store(sm, cur.na, cur.nb, q, r);
+        const K* As = sm + q.pa;
+        const K* Bs = sm + q.bb + q.pb;
+        const int na = cur.na, nb = cur.nb;
+        if (k + 1 < ntiles) {
+            cur = span(k + 1);
+            q = span_place(cur.a, cur.na, cur.b, cur.nb);
+            stage_load(cur.a, cur.b, q, r);
         }
-        merge_tile<K, XF>(src + p.ps + a_s, (int)(a_e - a_s), src + p.ps + p.la + b_s,
-                          (int)(b_e - b_s), dst + o, FINAL, sm);
+        merge_spans<K, XF>(As, na, Bs, nb, dst + (tile0 + k) * OT, FINAL);
     }
 }
 
