@@ -810,10 +810,10 @@ def run_serving(px, lib, seconds: float) -> dict:
     if lg.px_loadgen_prepare(13) != px.OK:
         raise RuntimeError("loadgen prepare failed")
 
-    def one(mode, rate):
+    def one(mode, rate, log2_max=26, inflight=8):
         cfg = LoadgenConfig(threads=16, mode=mode, rate=rate, seconds=seconds, seed=13,
-                            log2_min=10, log2_max=26, max_inflight=8 if rate <= 0 else 64,
-                            warmup=1)
+                            log2_min=10, log2_max=log2_max,
+                            max_inflight=inflight if rate <= 0 else 64, warmup=1)
         r = LoadgenResult()
         if lg.px_loadgen_run(C.byref(cfg), C.byref(r)) != px.OK:
             raise RuntimeError("loadgen run failed")
@@ -837,6 +837,15 @@ def run_serving(px, lib, seconds: float) -> dict:
         # one call at a time: how a runtime that is not thread-safe (the reference's,
         # src/kernel/kernel_launcher.hpp:172-176) has to be driven by 16 client threads
         out["per_call_serialized_saturation"] = one(2, 0.0)
+        # where coalescing pays: the same mix restricted to small requests (2^10..2^16),
+        # whose cost is launch and synchronisation rather than HBM traffic
+        out["small_requests"] = {"per_call_saturation": one(0, 0.0, 16)}
+        assert lib.parallax_serve_start(None) == px.OK
+        out["small_requests"]["served_saturation"] = one(1, 0.0, 16, inflight=32)
+        lib.parallax_serve_stop()
+        out["small_requests"]["throughput_ratio"] = round(
+            out["small_requests"]["served_saturation"]["req_s"] /
+            out["small_requests"]["per_call_saturation"]["req_s"], 3)
         out["serve_stats"] = {"requests": st.requests, "batches": st.batches,
                               "coalesced_requests": st.coalesced_requests,
                               "max_batch": st.max_batch, "memory_waits": st.memory_waits}

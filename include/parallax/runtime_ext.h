@@ -144,7 +144,7 @@ int parallax_scan_noalloc(parallax_kernel_t scan_kernel, const void* input, void
  * blocks or device memory. A request's result does not depend on what it was batched with
  * (integers bit-exact; floating point within the primitives' tolerance). */
 typedef struct parallax_serve_config {
-    uint32_t lanes;          /* batches in flight on the device (0: 4) */
+    uint32_t lanes;          /* batches in flight on the device (0: 8) */
     uint32_t max_batch;      /* requests per coalesced launch (0: 1024) */
     uint64_t solo_elements;  /* longer requests run alone (0: 2^22) */
     uint64_t inflight_bytes; /* admission budget: operand + temporary bytes of admitted,

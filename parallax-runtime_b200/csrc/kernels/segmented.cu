@@ -299,13 +299,16 @@ bool enqueue_typed(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     constexpr int TILE = kBlock * ITEMS;
     cudaStream_t s = ws.stream();
     volatile int32_t* err = &ws.d_slot->spin_error;
+    const uint64_t items_cap = c.S + c.count / TILE + 1;  // bound on the planner's items
     const SegEmpty empty = c.op == SEG_REDUCE ? SegEmpty::ZERO_RESULT
                          : c.op == SEG_COPY_IF ? SegEmpty::ZERO_COUNT : SegEmpty::NONE;
     k_seg_plan<kBlock><<<1, kBlock, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE, b.item_start,
                                             b.counters, empty,
                                             c.op == SEG_REDUCE ? b.tickets : nullptr, b.status,
-                                            b.status_cap, err);
-    k_seg_map<256><<<seg_map_grid(c.S), 256, 0, s>>>(b.item_start, c.S, b.item_seg);
+                                            b.status_cap, err,
+                                            items_cap <= kInlineItems ? b.item_seg : nullptr);
+    if (items_cap > kInlineItems)
+        k_seg_map<256><<<seg_map_grid(c.S), 256, 0, s>>>(b.item_start, c.S, b.item_seg);
     T init;
     memcpy(&init, &c.init_bits, sizeof(T));
     SegPred<T> pr;
@@ -313,16 +316,23 @@ bool enqueue_typed(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     pr.negate = c.pred.negate;
     pr.c = std::is_floating_point<T>::value ? (T)c.pred.f
          : std::is_signed<T>::value ? (T)c.pred.i : (T)c.pred.u;
-    int per_sm = 0;
-    void* kfn = nullptr;
-    switch (c.op) {
-        case SEG_REDUCE: kfn = (void*)k_segmented<T, ITEMS, SEG_REDUCE>; break;
-        case SEG_SCAN: kfn = (void*)k_segmented<T, ITEMS, SEG_SCAN>; break;
-        default: kfn = (void*)k_segmented<T, ITEMS, SEG_COPY_IF>; break;
+    // resident CTAs per SM of this instantiation (queried once), and no more CTAs than work
+    // items: a small batch launches a small grid
+    static int per_sm_of[3] = {0, 0, 0};
+    int& per_sm = per_sm_of[c.op];
+    if (per_sm == 0) {
+        void* kfn = nullptr;
+        switch (c.op) {
+            case SEG_REDUCE: kfn = (void*)k_segmented<T, ITEMS, SEG_REDUCE>; break;
+            case SEG_SCAN: kfn = (void*)k_segmented<T, ITEMS, SEG_SCAN>; break;
+            default: kfn = (void*)k_segmented<T, ITEMS, SEG_COPY_IF>; break;
+        }
+        int v = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kfn, kBlock, 0);
+        per_sm = v < 1 ? 1 : v;
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kBlock, 0);
-    if (per_sm < 1) per_sm = 1;
-    const unsigned grid = (unsigned)(per_sm * device_info().sm_count);
+    const uint64_t resident = (uint64_t)per_sm * device_info().sm_count;
+    const unsigned grid = (unsigned)(items_cap < resident ? items_cap : resident);
     switch (c.op) {
         case SEG_REDUCE:
             k_segmented<T, ITEMS, SEG_REDUCE><<<grid, kBlock, 0, s>>>(c.src, c.S, b, init, false, pr, err);

@@ -585,9 +585,11 @@ bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64
         cudaStream_t s = ws.stream();
         k_seg_plan<kBlock><<<1, kBlock, 0, s>>>(src, S, count, (uint32_t)TILE, item_start, counters,
                                                 SegEmpty::NONE, nullptr, st, ws.seg_status_cap,
-                                                &ws.d_slot->spin_error);
+                                                &ws.d_slot->spin_error,
+                                                items_cap <= kInlineItems ? item_seg : nullptr);
         const unsigned grid = (unsigned)items_cap;
-        k_seg_map<256><<<seg_map_grid(S), 256, 0, s>>>(item_start, S, item_seg);
+        if (items_cap > kInlineItems)
+            k_seg_map<256><<<seg_map_grid(S), 256, 0, s>>>(item_start, S, item_seg);
         k_seg_tile_sort<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, item_seg);
         for (int pass = 1; pass <= pass_bound; ++pass)
             k_seg_merge<K, XF><<<grid, kBlock, 0, s>>>(src, S, item_start, item_seg, pass,

@@ -69,7 +69,9 @@ __device__ __forceinline__ uint32_t find_segment(const uint32_t* item_start, uin
 
 // Inverse of the work list: item_seg[i] = the segment of work item i, so a kernel finds
 // its segment with one load instead of a binary search. One thread per segment writes
-// that segment's items (grid-stride over segments).
+// that segment's items (grid-stride over segments). Work lists of at most kInlineItems
+// items get it from the planner itself (`item_seg` argument) instead.
+constexpr uint64_t kInlineItems = 16384;
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_seg_map(const uint32_t* __restrict__ item_start, uint64_t S, uint32_t* __restrict__ item_seg) {
@@ -96,7 +98,7 @@ __global__ void __launch_bounds__(BLOCK)
 k_seg_plan(SegSrc src, uint64_t S, uint64_t count, uint32_t tile,
            uint32_t* __restrict__ item_start, uint32_t* __restrict__ counters, SegEmpty empty,
            uint32_t* __restrict__ seg_zero, StatusEntry* status, uint64_t status_cap,
-           volatile int32_t* err) {
+           volatile int32_t* err, uint32_t* __restrict__ item_seg) {
     __shared__ uint32_t s_warp[BLOCK / 32];
     __shared__ uint32_t s_carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -134,7 +136,12 @@ k_seg_plan(SegSrc src, uint64_t S, uint64_t count, uint32_t tile,
             if (w < warp) woff += v;
             total += v;
         }
-        if (s < S) item_start[s] = s_carry + woff + incl - items;
+        if (s < S) {
+            const uint32_t first = s_carry + woff + incl - items;
+            item_start[s] = first;
+            if (item_seg)  // small work lists: the inverse map too (saves a launch)
+                for (uint32_t i = 0; i < items; ++i) item_seg[first + i] = (uint32_t)s;
+        }
         __syncthreads();
         if (tid == 0) s_carry += total;
         __syncthreads();

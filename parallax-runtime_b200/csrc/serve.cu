@@ -65,11 +65,22 @@ struct Request {
     uint64_t footprint = 0;    // admitted bytes (operands + temporaries)
     void* tmp = nullptr;       // sort temporary: arena block (host-side address)
     bool coalescible = false;
-    // completion
+    // completion: the finisher sets done under m and notifies while holding it, so the
+    // waiter (which then deletes the request) never races the notification
     int status = PARALLAX_OK;
     uint64_t done_ns = 0;
-    bool done = false;         // guarded by the server mutex
+    bool done = false;
+    std::mutex m;
+    std::condition_variable cv;
 };
+
+void finish(Request* r, int status) {
+    r->status = status;
+    r->done_ns = now_ns();
+    std::lock_guard<std::mutex> g(r->m);
+    r->done = true;
+    r->cv.notify_one();
+}
 
 bool same_kind(const Request& a, const Request& b) {
     return a.op == b.op && a.t == b.t && a.red == b.red && a.mode == b.mode &&
@@ -96,7 +107,7 @@ class Server {
     std::vector<Lane> lanes;
     std::thread thr;
     std::mutex mu;
-    std::condition_variable cv_sched, cv_done;
+    std::condition_variable cv_sched;
     std::deque<Request*> queue;
     bool stopping = false;
     uint64_t inflight = 0;
@@ -104,7 +115,7 @@ class Server {
 
     bool init(const parallax_serve_config* c) {
         if (c) cfg = *c;
-        if (cfg.lanes == 0) cfg.lanes = 4;
+        if (cfg.lanes == 0) cfg.lanes = 8;
         if (cfg.max_batch == 0) cfg.max_batch = 1024;
         if (cfg.solo_elements == 0) cfg.solo_elements = 1ull << 22;
         if (cfg.inflight_bytes == 0) cfg.inflight_bytes = parallax_arena_capacity() / 2;
@@ -137,8 +148,8 @@ class Server {
     }
 
     int wait(Request* r, uint64_t* done_ns) {
-        std::unique_lock<std::mutex> lk(mu);
-        cv_done.wait(lk, [&] { return r->done; });
+        std::unique_lock<std::mutex> lk(r->m);
+        r->cv.wait(lk, [&] { return r->done; });
         if (done_ns) *done_ns = r->done_ns;
         return r->status;
     }
@@ -154,56 +165,57 @@ class Server {
 
   private:
     // ---- admission (mutex held) ----------------------------------------------------------------
-    bool admit(Request* r) {
+    enum class Admit { YES, WAIT, REJECT };
+    Admit admit(Request* r) {
         const bool idle = inflight == 0;
-        if (!idle && inflight + r->footprint > cfg.inflight_bytes) return false;
+        if (!idle && inflight + r->footprint > cfg.inflight_bytes) return Admit::WAIT;
         if (r->op == ReqOp::SORT && r->coalescible && r->n > 1) {
             void* p = parallax_arena_alloc(r->n * r->es, 256);
-            if (!p) {
-                if (!idle) return false;
-                finish_locked(r, PARALLAX_ERR_OUT_OF_MEMORY);  // cannot fit even alone
-                return true;
-            }
+            if (!p) return idle ? Admit::REJECT : Admit::WAIT;  // REJECT: cannot fit even alone
             parallax_arena_set_residency(p, PARALLAX_DEVICE_RESIDENT);
             r->tmp = p;
         }
         inflight += r->footprint;
         if (inflight > stats.peak_inflight_bytes) stats.peak_inflight_bytes = inflight;
-        return true;
+        return Admit::YES;
     }
 
     // Takes the next batch off the queue (mutex held); empty when the head must wait.
+    // Requests rejected at admission are taken off the queue and finished last (their
+    // waiters may free them at once).
     std::vector<Request*> form_batch() {
-        std::vector<Request*> b;
+        std::vector<Request*> b, rejected;
         while (!queue.empty()) {
             Request* head = queue.front();
-            if (!admit(head)) {
+            const Admit a = admit(head);
+            if (a == Admit::WAIT) {
                 ++stats.memory_waits;
-                return b;
+                break;
             }
             queue.pop_front();
-            if (head->done) continue;  // rejected at admission
+            if (a == Admit::REJECT) {
+                rejected.push_back(head);
+                continue;
+            }
             b.push_back(head);
             break;
         }
-        if (b.empty() || !b[0]->coalescible) return b;
-        for (auto it = queue.begin(); it != queue.end() && b.size() < cfg.max_batch;) {
-            Request* r = *it;
-            if (!r->coalescible || !same_kind(*r, *b[0])) {
-                ++it;
-                continue;
+        if (!b.empty() && b[0]->coalescible) {
+            for (auto it = queue.begin(); it != queue.end() && b.size() < cfg.max_batch;) {
+                Request* r = *it;
+                if (!r->coalescible || !same_kind(*r, *b[0])) {
+                    ++it;
+                    continue;
+                }
+                const Admit a = admit(r);
+                if (a == Admit::WAIT) break;  // keep arrival order for what does not fit
+                it = queue.erase(it);
+                if (a == Admit::REJECT) rejected.push_back(r);
+                else b.push_back(r);
             }
-            if (!admit(r)) break;  // keep arrival order for what does not fit
-            it = queue.erase(it);
-            if (!r->done) b.push_back(r);
         }
+        for (Request* r : rejected) finish(r, PARALLAX_ERR_OUT_OF_MEMORY);
         return b;
-    }
-
-    void finish_locked(Request* r, int status) {
-        r->status = status;
-        r->done_ns = now_ns();
-        r->done = true;
     }
 
     // ---- launch (no mutex) ---------------------------------------------------------------------
@@ -276,14 +288,11 @@ class Server {
         }
         {
             std::lock_guard<std::mutex> g(mu);
-            for (Request* r : l.reqs) {
-                inflight -= r->footprint;
-                finish_locked(r, status);
-            }
+            for (Request* r : l.reqs) inflight -= r->footprint;
         }
+        for (Request* r : l.reqs) finish(r, status);  // r may be deleted right after
         l.reqs.clear();
         l.busy = false;
-        cv_done.notify_all();
     }
 
     void loop() {
@@ -306,7 +315,6 @@ class Server {
             for (Lane& l : lanes) {
                 if (l.busy || queue.empty()) continue;
                 std::vector<Request*> b = form_batch();
-                cv_done.notify_all();  // requests rejected at admission are finished
                 if (b.empty()) break;
                 l.reqs = std::move(b);
                 l.busy = true;
@@ -477,7 +485,7 @@ PXB_EXPORT int parallax_serve_wait(uint64_t ticket, uint64_t* done_ns) {
         return PARALLAX_ERR_INVALID_ARGUMENT;
     }
     int st;
-    if (r->done && r->n == 0) {
+    if (r->n == 0) {  // finished at submission by this thread
         st = r->status;
         if (done_ns) *done_ns = r->done_ns;
     } else {
