@@ -339,22 +339,24 @@ __device__ __forceinline__ void merge_tile(const K* __restrict__ A, int na, cons
     merge_spans<K, XF>(sm + q.pa, na, sm + q.bb + q.pb, nb, dst, final_pass);
 }
 
-// One CTA per kTilesPerCta output tiles of OT keys. Each of the first 2 x kTilesPerCta
+// One CTA per `tpc` (1..kTilesPerCta) output tiles of OT keys. Each of the first 2 x tpc
 // warps finds one tile start or end on the merge path of the tile's run pair (a 32-ary
-// search over HBM, all searches in parallel, so the latency is paid once per four tiles);
-// the CTA then stages and merges its tiles in turn.
+// search over HBM, all searches in parallel, so the latency is paid once per CTA); the CTA
+// then stages and merges its tiles in turn. Sorts of 2048 tiles or more use four tiles per
+// CTA; smaller ones use one, for more CTAs and shorter ones.
 constexpr int kTilesPerCta = 4;
 static_assert(2 * kTilesPerCta <= kBlock / 32, "one warp per split");
 
-template <typename K, int XF, bool FINAL>
+template <typename K, int XF, bool FINAL, int TPC>
 __global__ void __launch_bounds__(kBlock)
 k_merge(const K* __restrict__ src, K* __restrict__ dst, uint64_t n, uint64_t L, uint64_t tiles,
         volatile int32_t* err) {
+    constexpr int tpc = TPC;
     constexpr int OT = kBlock * SortShape<K>::ITEMS;
     __shared__ __align__(16) K sm[staged_elems<K>(OT)];
-    __shared__ uint64_t s_split[2 * kTilesPerCta];
-    const uint64_t tile0 = (uint64_t)blockIdx.x * kTilesPerCta;
-    const int ntiles = (int)(tiles - tile0 < (uint64_t)kTilesPerCta ? tiles - tile0 : kTilesPerCta);
+    __shared__ uint64_t s_split[2 * TPC];
+    const uint64_t tile0 = (uint64_t)blockIdx.x * tpc;
+    const int ntiles = (int)(tiles - tile0 < (uint64_t)tpc ? tiles - tile0 : tpc);
     const int warp = threadIdx.x >> 5;
     if (warp < 2 * ntiles) {
         const uint64_t o = (tile0 + warp / 2) * OT;
@@ -436,12 +438,20 @@ bool sort_keys(Workspace& ws, void* d_data, uint64_t n) {
         K* nxt = cur == data ? tmp : data;
         {
             ProfScope prof(ws, "k_merge", 2 * n * sizeof(K));
-            const unsigned grid = (unsigned)((tiles + kTilesPerCta - 1) / kTilesPerCta);
+            // four tiles per CTA from 2048 tiles (512 CTAs) up, one below
             volatile int32_t* err = &ws.d_slot->spin_error;
-            if (pass == passes)
-                k_merge<K, XF, true><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles, err);
-            else
-                k_merge<K, XF, false><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles, err);
+            if (tiles >= 2048) {
+                const unsigned grid = (unsigned)((tiles + kTilesPerCta - 1) / kTilesPerCta);
+                if (pass == passes)
+                    k_merge<K, XF, true, kTilesPerCta><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles, err);
+                else
+                    k_merge<K, XF, false, kTilesPerCta><<<grid, kBlock, 0, s>>>(cur, nxt, n, L, tiles, err);
+            } else {
+                if (pass == passes)
+                    k_merge<K, XF, true, 1><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, tiles, err);
+                else
+                    k_merge<K, XF, false, 1><<<(unsigned)tiles, kBlock, 0, s>>>(cur, nxt, n, L, tiles, err);
+            }
         }
         count_launch(1);
         cur = nxt;
