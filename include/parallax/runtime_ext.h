@@ -124,7 +124,7 @@ int parallax_segmented_sort(parallax_kernel_t kernel, void* data, size_t count,
  * parallax_status.
  * The runtime allocates nothing for it: the look-back status lives in one static device
  * array of 576.25 KiB that every GPU loading this library holds until the process exits.
- * That caps count at 24576 tiles: 301,989,888 elements of a 4-byte type, 150,994,944 of
+ * That caps count at 24576 tiles: 704,643,072 elements of a 4-byte type, 352,321,536 of
  * an 8-byte type; larger counts return PARALLAX_ERR_INVALID_ARGUMENT and touch nothing.
  * The first call on a device looks up that array's device address (once per device, with
  * the device current); make that first call before any stream capture. All calls share

@@ -7,9 +7,9 @@
 // fp32 counts inexact beyond 2^24; here counts are 32-bit within a tile and 64-bit
 // across tiles.
 //
-// Here: one CTA per 48 KiB tile, in blockIdx order, staged as four bulk-copied sub-tiles
-// (tiles.cuh). Phase 1 evaluates the predicate (or the adjacent-difference test for
-// unique) on 12 / 6 consecutive elements per thread as each sub-tile lands, keeps the
+// Here: one 512-thread CTA per 112 KiB tile (two per SM), in blockIdx order, staged as two
+// bulk-copied sub-tiles (tiles.cuh). Phase 1 evaluates the predicate (or the adjacent-difference test for
+// unique) on 28 / 14 consecutive elements per thread as each sub-tile lands, keeps the
 // flags as bit masks, and ranks the kept elements with one shuffle scan per sub-tile and
 // one 32-lane scan over the (sub-tile, warp) counts; warp 0 gets the tile's output offset
 // by decoupled look-back on kept counts. Phase 2 packs the kept elements at the front of
@@ -31,9 +31,9 @@
 namespace pxb {
 namespace {
 
-constexpr int kBlock = 256;
-constexpr int kVpt = 3;
-constexpr int kSub = 4;
+constexpr int kBlock = 512;  // tile shape as in scan.cu (measured: 112 KiB tiles, 2 CTAs/SM)
+constexpr int kVpt = 7;
+constexpr int kSub = 2;
 
 template <typename T>
 struct Shape {
@@ -257,7 +257,7 @@ __device__ __forceinline__ void compact_tile(T* buf, uint64_t* bars, uint32_t pa
 
 // One CTA per tile, in blockIdx order (unaligned input).
 template <typename T, int MODE, bool BULK>
-__global__ void __launch_bounds__(kBlock, 4)
+__global__ void __launch_bounds__(kBlock, 2)
 k_compact(const T* in, T* out, uint64_t n, PredDev<T> pred, TileStatus<uint64_t> ts,
           const unsigned long long* __restrict__ num_true,
           unsigned long long* __restrict__ count_out) {

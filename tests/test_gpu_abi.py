@@ -260,6 +260,7 @@ def test_async_mode_with_device_result(lib, px, ox, dev):
     x = ox.gen("i64_full", 30, 1 << 20)
     d = dev.put(x)
     r = torch.zeros(1, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()  # the runtime works on its own stream
     assert lib.parallax_set_async(1) == 0
     try:
         lib.parallax_reduce(px.builtin("reduce:sum:i64"), d.data_ptr(), x.size, 8, r.data_ptr())

@@ -21,6 +21,7 @@ def ones(dev):
     if torch.cuda.get_device_properties(0).total_memory < 60 << 30:
         pytest.skip("needs about 40 GB of device memory")
     x = torch.ones(N, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()  # the runtime works on its own stream
     yield x
     del x
     torch.cuda.empty_cache()
@@ -42,6 +43,7 @@ def test_reduce_over_2e32(lib, px, ones):
 def test_scans_over_2e32(lib, px, dev, ones):
     torch = dev.torch
     out = torch.empty(N, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
     h = px.builtin("scan:i32")
     init = np.array([7], np.int32)
     lib.parallax_exclusive_scan(h, h, h, ones.data_ptr(), out.data_ptr(), N, 4, init.ctypes.data)
@@ -61,6 +63,7 @@ def test_scans_over_2e32(lib, px, dev, ones):
 def test_copy_if_over_2e32(lib, px, dev, ones):
     torch = dev.torch
     out = torch.zeros(N, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
     h = px.builtin("copy_if:i32:gt:0")
     k = lib.parallax_copy_if(h, h, h, h, ones.data_ptr(), out.data_ptr(), N, 4, 0)
     px.check("copy_if")

@@ -285,6 +285,7 @@ off = np.array([0, 70000, 70001, 200000], np.uint64)
 x = torch.ones(200000, dtype=torch.float32, device="cuda")
 o = torch.from_numpy(off.view(np.uint8)).cuda()
 r = torch.zeros(3, dtype=torch.float32, device="cuda")
+torch.cuda.synchronize()
 lib.parallax_segmented_reduce(px.builtin("reduce:sum:f32"), x.data_ptr(), 200000, o.data_ptr(), 3,
                               r.data_ptr())
 px.check("tuned reduce")

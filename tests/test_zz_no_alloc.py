@@ -22,7 +22,7 @@ from cases import F32_TOL, F64_TOL
 pytestmark = pytest.mark.gpu
 
 MAX_TILES = 24576
-TILE = {4: 12288, 8: 6144}  # elements per look-back tile of the scan kernel (48 KiB)
+TILE = {4: 28672, 8: 14336}  # elements per look-back tile of the scan kernel (112 KiB)
 
 
 def gen(ox, t, n, seed):
@@ -101,10 +101,13 @@ def test_noalloc_rejects_counts_beyond_its_static_capacity(lib, px, dev):
 
 
 def test_noalloc_largest_count(lib, px, ox, dev):
+    torch = dev.torch
     n = MAX_TILES * TILE[8]
-    x = np.ones(n, np.int64)
-    d = dev.put(x)
+    d = torch.ones(n, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
     h = px.builtin("scan:i64")
     assert lib.parallax_scan_noalloc(h, d.data_ptr(), d.data_ptr(), n, 8, None, None) == px.OK
-    got = dev.get(d, np.int64, n)
-    assert got[0] == 1 and got[-1] == n and np.array_equal(got[::4099], np.arange(1, n + 1)[::4099])
+    idx = np.unique(np.concatenate([[0, 1, n - 2, n - 1], np.arange(0, n, 4099)]))
+    got = d[torch.from_numpy(idx).cuda()].cpu().numpy()
+    assert np.array_equal(got, idx + 1)
+    del d
