@@ -16,6 +16,10 @@ constexpr int32_t kErrSegmentOffsets = 0x5e90;
 // were inconsistent (only possible if a run was not sorted); the tile is skipped instead of
 // staging outside its shared-memory buffer.
 constexpr int32_t kErrMergeSpan = 0x5e91;
+// Mapped error-word code of the radix passes: a CTA claimed a tile beyond the array or
+// computed an output position outside it (only possible if a look-back word was corrupt);
+// the access is skipped.
+constexpr int32_t kErrRadixRange = 0x5e92;
 
 // x % m == r for 32-bit integers with C semantics (the remainder takes the sign of x),
 // dividing |x| by |m| as an invariant divisor: one multiply-high and two shifts

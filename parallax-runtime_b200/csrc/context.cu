@@ -189,6 +189,35 @@ void* Workspace::seg_status(uint64_t entries) {
     return d_seg_status;
 }
 
+void* Workspace::radix(size_t bytes) {
+    if (bytes <= radix_cap) return d_radix;
+    cudaStream_t s = stream();
+    if (d_radix) {
+        if (!cuda_ok(cudaStreamSynchronize(s), "radix buffer sync")) return nullptr;
+        cudaFree(d_radix);
+        d_radix = nullptr;
+        radix_cap = 0;
+    }
+    size_t cap = 1 << 20;
+    while (cap < bytes) cap <<= 1;
+    if (!cuda_ok(cudaMalloc(&d_radix, cap), "cudaMalloc(radix buffer)")) return nullptr;
+    if (!cuda_ok(cudaMemsetAsync(d_radix, 0, cap, s), "cudaMemset(radix buffer)")) return nullptr;
+    radix_cap = cap;
+    radix_epoch = 1;
+    ++generation;
+    return d_radix;
+}
+
+uint32_t Workspace::next_radix_epochs(uint32_t count) {
+    if (radix_epoch + count >= (1u << 22)) {
+        cudaMemsetAsync(d_radix, 0, radix_cap, stream());
+        radix_epoch = 1;
+    }
+    const uint32_t e = radix_epoch;
+    radix_epoch += count;
+    return e;
+}
+
 bool graph_launch(Workspace& ws, const std::string& key, const std::function<bool()>& enqueue) {
     static const bool enabled =
         !(getenv("PARALLAX_GRAPHS") && atoi(getenv("PARALLAX_GRAPHS")) == 0);
@@ -361,6 +390,10 @@ int sync_stream(Workspace& ws) {
         ws.h_slot->spin_error = 0;
         if (code == kErrMergeSpan) {
             set_error(PARALLAX_ERR_CUDA, "sort: a merge pass met an unsorted run (tile skipped)");
+            return PARALLAX_ERR_CUDA;
+        }
+        if (code == kErrRadixRange) {
+            set_error(PARALLAX_ERR_CUDA, "sort: a radix pass met an out-of-range position (skipped)");
             return PARALLAX_ERR_CUDA;
         }
         if (code == kErrSegmentOffsets) {

@@ -1,0 +1,419 @@
+// Ascending sort of large arrays: one-sweep LSD radix sort with 8-bit digits.
+//
+// Reference: a global bitonic network, one dispatch + fence wait per (k, j) stage
+// (src/kernel/kernel_launcher.cpp:1568-1606, shaders/bitonic.comp:15-29).
+//
+// Keys are ordered as unsigned integers after the order-preserving transform of
+// sortkey.cuh, exactly as the merge sort in sort.cu orders them. A sort under a total order
+// of the key bits has one result, so both paths return the same bytes.
+//
+// Method: D. Adinets and D. Merrill, "Onesweep: A Faster Least Significant Digit Radix Sort
+// for GPUs" (2022). One upfront kernel counts the histogram of every digit position in a
+// single read of the keys. Then each digit pass, lowest digit first, reads and writes the
+// keys once:
+//   1. a CTA claims the next tile (atomic counter, so every tile it waits on belongs to a
+//      CTA that is already running or done) and loads its keys, warp-striped;
+//   2. ranks them stably by the current digit, warp by warp: each warp walks its keys in
+//      index order and, per 32 keys, groups lanes with equal digits (shared lane masks), so
+//      a key's rank is the warp's running count of its digit plus its lower peers;
+//   3. publishes the tile's 256 digit counts at once (state AGG), then finds each digit's
+//      global offset by decoupled look-back over the per-(tile, digit) words of earlier
+//      tiles (one thread per digit) and publishes the inclusive count (state INC); tile 0
+//      starts every chain from the exclusive scan of the upfront histogram;
+//   4. places the keys in digit order in shared memory and writes each digit's run to
+//      its global offset, so a warp's stores cover consecutive addresses.
+// Look-back words are 64-bit: [63:42] pass epoch, [41:40] state, [39:0] count. Words of
+// earlier passes carry older epochs and read as "not ready", so nothing is cleared between
+// passes. Waits are bounded like the other look-backs (lookback.cuh: kSpinLimit).
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../runtime.hpp"
+#include "../sortkey.cuh"
+#include "../tiles.cuh"
+
+namespace pxb {
+namespace {
+
+constexpr int kBins = 256;
+constexpr int kValBits = 40;
+constexpr uint64_t kValMask = (uint64_t(1) << kValBits) - 1;
+constexpr uint64_t kStAgg = uint64_t(1) << kValBits;
+constexpr uint64_t kStInc = uint64_t(2) << kValBits;
+constexpr int kEpochShift = 42;
+
+template <typename K> struct RadixShape;
+template <> struct RadixShape<uint32_t> { static constexpr int BLOCK = 512, ITEMS = 16; };
+template <> struct RadixShape<uint64_t> { static constexpr int BLOCK = 512, ITEMS = 8; };
+
+// Each warp ranks its keys as kSubs independent streams (the first and second half of its
+// keys), each with its own count and mask tables, so the two dependency chains overlap.
+constexpr int kSubs = 2;
+
+template <typename K>
+constexpr size_t radix_smem() {
+    return (size_t)RadixShape<K>::BLOCK * RadixShape<K>::ITEMS * sizeof(K) +
+           (size_t)(RadixShape<K>::BLOCK / 32) * kSubs * kBins * sizeof(uint32_t);
+}
+
+template <typename K>
+__device__ __forceinline__ uint32_t digit_of(K k, int shift) {
+    return (uint32_t)(k >> shift) & 0xffu;
+}
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---- upfront histogram ----------------------------------------------------------------------
+// Counts, for every digit position p, how many keys have each digit value, in one read of
+// the keys. Shared-memory atomics are the limit here, and what they cost is bank conflicts:
+// each lane counts into its own copy of the histograms, laid out [p][digit][copy] with
+// copy = lane % COPIES, so with 32 copies lane l always hits bank l (conflict-free) and
+// with 16 copies at most two lanes share a bank. The host sizes the grid so that every
+// per-CTA count stays below 2^32.
+template <typename K> struct HistShape;
+template <> struct HistShape<uint32_t> { static constexpr int COPIES = 32, U = 16; };
+template <> struct HistShape<uint64_t> { static constexpr int COPIES = 16, U = 8; };
+constexpr int kHistBlock = 1024;
+
+template <typename K>
+constexpr size_t hist_smem() {
+    return (size_t)sizeof(K) * kBins * HistShape<K>::COPIES * sizeof(uint32_t);
+}
+
+template <typename K, int XF>
+__global__ void __launch_bounds__(kHistBlock)
+    k_radix_hist(const K* __restrict__ in, uint64_t n, unsigned long long* __restrict__ hist) {
+    constexpr int P = sizeof(K);
+    constexpr int COPIES = HistShape<K>::COPIES, U = HistShape<K>::U;
+    extern __shared__ __align__(16) uint32_t sh[];  // [P][kBins][COPIES]
+    for (int i = threadIdx.x; i < P * kBins * COPIES; i += kHistBlock) sh[i] = 0u;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    uint32_t* const mine = sh + (lane % COPIES);
+    const uint64_t stride = (uint64_t)gridDim.x * kHistBlock;
+    uint64_t i = (uint64_t)blockIdx.x * kHistBlock + threadIdx.x;
+    for (; i + (U - 1) * stride < n; i += U * stride) {
+        K k[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) k[u] = to_key<K, XF>(__ldcs(in + i + u * stride));
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                atomicAdd(mine + (p * kBins + digit_of(k[u], 8 * p)) * COPIES, 1u);
+    }
+    for (; i < n; i += stride) {
+        const K k = to_key<K, XF>(in[i]);
+#pragma unroll
+        for (int p = 0; p < P; ++p) atomicAdd(mine + (p * kBins + digit_of(k, 8 * p)) * COPIES, 1u);
+    }
+    __syncthreads();
+    // one (position, digit) row per thread; copies read in a lane-rotated order so a warp's
+    // 32 rows hit 32 different banks
+    for (int j = threadIdx.x; j < P * kBins; j += kHistBlock) {
+        uint32_t v = 0;
+#pragma unroll 8
+        for (int c = 0; c < COPIES; ++c) v += sh[j * COPIES + ((c + lane) % COPIES)];
+        if (v) atomicAdd(&hist[j], (unsigned long long)v);
+    }
+}
+
+// Exclusive scan over the 256 digits held by threads 0..255 (one value each); every thread
+// of the CTA calls it (threads 256.. pass zero). `part` is shared scratch of 8 elements.
+template <typename T, int BLOCK>
+__device__ __forceinline__ T digit_exclusive_scan(T v, T* part) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const T inc = warp_inclusive_scan(v, OpSum());
+    if (warp < kBins / 32 && lane == 31) part[warp] = inc;
+    __syncthreads();
+    T before = T(0);
+    if (warp < kBins / 32)
+        for (int w = 0; w < warp; ++w) before += part[w];
+    __syncthreads();  // part may be reused by the caller's next scan
+    return before + inc - v;
+}
+
+// ---- one digit pass --------------------------------------------------------------------------
+// XF_IN transforms keys as they are read (the first pass reads the caller's values),
+// XF_OUT restores them as they are written (the last pass writes the caller's values).
+template <typename K, int XF_IN, int XF_OUT>
+__global__ void __launch_bounds__(RadixShape<K>::BLOCK, 2)
+    k_radix_pass(const K* __restrict__ in, K* __restrict__ out, uint64_t n, int shift,
+                 const unsigned long long* __restrict__ hist, uint64_t* status, uint32_t epoch,
+                 uint64_t tiles, uint32_t* counters, volatile int32_t* err) {
+    constexpr int BLOCK = RadixShape<K>::BLOCK, ITEMS = RadixShape<K>::ITEMS;
+    constexpr int TILE = BLOCK * ITEMS, WARPS = BLOCK / 32;
+    constexpr int TABLES = WARPS * kSubs, HALF = ITEMS / kSubs;
+    static_assert(BLOCK >= kBins, "one thread per digit");
+    static_assert(ITEMS % kSubs == 0, "whole streams");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K* const s_keys = reinterpret_cast<K*>(smem_raw);
+    uint32_t* const s_wh = reinterpret_cast<uint32_t*>(smem_raw + (size_t)TILE * sizeof(K));
+    __shared__ uint64_t s_goff[kBins];
+    __shared__ uint64_t s_part64[kBins / 32];
+    __shared__ uint32_t s_part32[kBins / 32];
+    __shared__ uint32_t s_tile;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(&counters[0], 1u);
+    // count table of stream s of this warp: wh + s * kBins; its lane-mask table: mm + s * kBins
+    uint32_t* const wh = s_wh + warp * kSubs * kBins;
+    // the ranking's lane-mask tables borrow the key buffer, which is free until step 4a
+    static_assert((size_t)TILE * sizeof(K) >= (size_t)TABLES * kBins * 4, "mask tables fit");
+    uint32_t* const mm = reinterpret_cast<uint32_t*>(s_keys) + warp * kSubs * kBins;
+#pragma unroll
+    for (int i = lane; i < kSubs * kBins; i += 32) {
+        wh[i] = 0u;
+        mm[i] = 0u;
+    }
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= tiles) {  // claim counter out of step: touch nothing
+        if (tid == 0) {
+            *err = kErrRadixRange;
+            persistent_exit(counters);
+        }
+        return;
+    }
+    const uint64_t base = tile * TILE;
+    const uint64_t rem = n - base;
+    const uint32_t valid = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+
+    // 1. keys of warp w: tile positions [w * 32 * ITEMS, (w + 1) * 32 * ITEMS), item i of
+    // lane l at w * 32 * ITEMS + 32 i + l, so items walked in order visit keys in index order
+    K k[ITEMS];
+    const uint32_t w0 = (uint32_t)warp * 32 * ITEMS + lane;
+    if (valid == (uint32_t)TILE) {
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) k[i] = to_key<K, XF_IN>(__ldcs(in + base + w0 + 32 * i));
+    } else {
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            const uint32_t li = w0 + 32 * i;  // padding: the largest key, digit 255 at the end
+            k[i] = li < valid ? to_key<K, XF_IN>(in[base + li]) : ~K(0);
+        }
+    }
+
+    // 2. stable warp-level ranking by the current digit. Lanes holding the same digit find
+    // each other through a per-stream table of 256 lane masks (shared-memory atomic OR of
+    // the lane's bit, read back, cleared by the group's highest lane); a key's rank is the
+    // stream's running count of its digit plus its lower peers, and the highest peer
+    // advances the count. This keeps the ranking off the SM's narrow branch unit (where match-any
+    // issues) and off the ALU (eight ballots per key cost more than the whole pass).
+    static_assert(ITEMS % 2 == 0 && 32 * HALF <= 0xffff, "two 16-bit ranks per register");
+    uint32_t rk[ITEMS / 2];  // rank within the item's stream, two per register
+    const uint32_t lt = lanemask_lt();
+    const uint32_t le = lt | (1u << lane);
+#pragma unroll
+    for (int j = 0; j < HALF; ++j) {  // item j of every stream
+        uint32_t d[kSubs], peers[kSubs], c[kSubs];
+#pragma unroll
+        for (int t = 0; t < kSubs; ++t) {
+            d[t] = digit_of(k[t * HALF + j], shift) + t * kBins;
+            atomicOr(&mm[d[t]], 1u << lane);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < kSubs; ++t) {
+            peers[t] = mm[d[t]];
+            c[t] = wh[d[t]] + __popc(peers[t] & lt);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < kSubs; ++t) {
+            if ((peers[t] & ~le) == 0) {  // the highest peer
+                wh[d[t]] = c[t] + 1;
+                mm[d[t]] = 0u;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < kSubs; ++t) {
+            const int i = t * HALF + j;
+            if (i % 2 == 0) rk[i / 2] = c[t];
+            else rk[i / 2] |= c[t] << 16;
+        }
+    }
+    __syncthreads();
+
+    // 3a. per digit: counts of the streams -> exclusive over streams (in key order); tile
+    // count; publish AGG
+    uint32_t cnt = 0;
+    if (tid < kBins) {
+#pragma unroll 8
+        for (int w = 0; w < TABLES; ++w) {
+            const uint32_t c = s_wh[w * kBins + tid];
+            s_wh[w * kBins + tid] = cnt;
+            cnt += c;
+        }
+        if (tile != 0)
+            st_relaxed_u64(&status[tile * kBins + tid],
+                           ((uint64_t)epoch << kEpochShift) | kStAgg | cnt);
+    }
+    const uint32_t loc = digit_exclusive_scan<uint32_t, BLOCK>(tid < kBins ? cnt : 0u, s_part32);
+    uint64_t start = 0;  // tile 0: the digit's first output position
+    if (tile == 0)
+        start = digit_exclusive_scan<uint64_t, BLOCK>(tid < kBins ? (uint64_t)hist[tid] : 0ull,
+                                                      s_part64);
+    if (tid < kBins) {
+#pragma unroll 8
+        for (int w = 0; w < TABLES; ++w) s_wh[w * kBins + tid] += loc;
+    }
+    __syncthreads();
+
+    // 4a. keys in digit order in shared memory
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const uint32_t r = (i % 2 == 0) ? (rk[i / 2] & 0xffffu) : (rk[i / 2] >> 16);
+        s_keys[wh[(i / HALF) * kBins + digit_of(k[i], shift)] + r] = k[i];
+    }
+
+    // 3b. look-back, one thread per digit
+    if (tid < kBins) {
+        uint64_t excl = start;
+        if (tile != 0) {
+            for (int64_t j = (int64_t)tile - 1; j >= 0; --j) {
+                uint64_t w = 0;
+                uint32_t spins = 0;
+                bool gave_up = false;
+                for (;;) {
+                    w = ld_relaxed_u64(&status[(uint64_t)j * kBins + tid]);
+                    if ((uint32_t)(w >> kEpochShift) == epoch && (w & (kStAgg | kStInc))) break;
+                    if (++spins > kSpinLimit) {
+                        *err = 1;
+                        gave_up = true;
+                        break;
+                    }
+                    if (spins > 8) nanosleep_ns(32);
+                }
+                if (gave_up) break;
+                excl += w & kValMask;
+                if (w & kStInc) break;
+            }
+        }
+        st_relaxed_u64(&status[tile * kBins + tid],
+                       ((uint64_t)epoch << kEpochShift) | kStInc | ((excl + cnt) & kValMask));
+        s_goff[tid] = excl - loc;  // output position of tile-sorted index x: s_goff[d] + x
+    }
+    __syncthreads();
+
+    // 4b. each digit's run to its global offset
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t x = (uint32_t)j * BLOCK + tid;
+        if (x < valid) {
+            const K key = s_keys[x];
+            const uint64_t pos = s_goff[digit_of(key, shift)] + x;
+            if (pos < n) out[pos] = from_key<K, XF_OUT>(key);
+            else *err = kErrRadixRange;
+        }
+    }
+    if (tid == 0) persistent_exit(counters);
+}
+
+template <typename K, int XF_IN, int XF_OUT>
+bool launch_pass(const K* in, K* out, uint64_t n, int shift, const unsigned long long* hist,
+                 uint64_t* status, uint32_t epoch, uint32_t* counters, volatile int32_t* err,
+                 uint64_t tiles, cudaStream_t s) {
+    constexpr size_t smem = radix_smem<K>();
+    if (!smem_opt_in<k_radix_pass<K, XF_IN, XF_OUT>>(smem))
+        return cuda_ok(cudaGetLastError(), "k_radix_pass shared-memory opt-in");
+    k_radix_pass<K, XF_IN, XF_OUT><<<(unsigned)tiles, RadixShape<K>::BLOCK, smem, s>>>(
+        in, out, n, shift, hist, status, epoch, tiles, counters, err);
+    return true;
+}
+
+template <typename K, int XF>
+bool radix_sort_keys(Workspace& ws, void* d_data, uint64_t n) {
+    constexpr int P = sizeof(K);
+    constexpr int TILE = RadixShape<K>::BLOCK * RadixShape<K>::ITEMS;
+    const uint64_t tiles = (n + TILE - 1) / TILE;
+    if (tiles > 0x7fffffffull || n > kValMask) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "sort: too many elements");
+        return false;
+    }
+    K* data = static_cast<K*>(d_data);
+    K* tmp = static_cast<K*>(ws.temp(n * sizeof(K)));
+    if (!tmp) return false;
+    // radix buffer: [0, 256) tile claim / exit counters, then P histograms, then the
+    // per-(tile, digit) look-back words
+    constexpr size_t hist_off = 256, status_off = hist_off + (size_t)P * kBins * 8;
+    char* rb = static_cast<char*>(ws.radix(status_off + tiles * kBins * 8));
+    if (!rb) return false;
+    const uint32_t ep0 = ws.next_radix_epochs(P);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(rb);
+    auto* hist = reinterpret_cast<unsigned long long*>(rb + hist_off);
+    auto* status = reinterpret_cast<uint64_t*>(rb + status_off);
+    volatile int32_t* err = &ws.d_slot->spin_error;
+    cudaStream_t s = ws.stream();
+    if (!cuda_ok(cudaMemsetAsync(hist, 0, (size_t)P * kBins * 8, s), "radix histogram clear"))
+        return false;
+    {
+        // grid: one CTA per SM (the copies fill most of its shared memory), more when needed
+        // to keep per-CTA counts below 2^31
+        uint64_t grid = (uint64_t)device_info().sm_count;
+        const uint64_t need = (n + kHistBlock - 1) / kHistBlock;
+        if (grid > need) grid = need;
+        const uint64_t min_grid = (n >> 31) + 1;
+        if (grid < min_grid) grid = min_grid;
+        constexpr size_t hsmem = hist_smem<K>();
+        if (!smem_opt_in<k_radix_hist<K, XF>>(hsmem))
+            return cuda_ok(cudaGetLastError(), "k_radix_hist shared-memory opt-in");
+        ProfScope prof(ws, "k_radix_hist", n * sizeof(K));
+        k_radix_hist<K, XF><<<(unsigned)grid, kHistBlock, hsmem, s>>>(data, n, hist);
+    }
+    count_launch();
+    static_assert(P % 2 == 0, "an even number of passes ends in the caller's array");
+    for (int p = 0; p < P; ++p) {
+        const K* src = (p % 2 == 0) ? data : tmp;
+        K* dst = (p % 2 == 0) ? tmp : data;
+        const unsigned long long* hp = hist + (size_t)p * kBins;
+        bool ok;
+        {
+            ProfScope prof(ws, "k_radix_pass", 2 * n * sizeof(K));
+            if (p == 0)
+                ok = launch_pass<K, XF, 0>(src, dst, n, 8 * p, hp, status, ep0 + p, counters, err,
+                                           tiles, s);
+            else if (p == P - 1)
+                ok = launch_pass<K, 0, XF>(src, dst, n, 8 * p, hp, status, ep0 + p, counters, err,
+                                           tiles, s);
+            else
+                ok = launch_pass<K, 0, 0>(src, dst, n, 8 * p, hp, status, ep0 + p, counters, err,
+                                          tiles, s);
+        }
+        if (!ok) return false;
+        count_launch();
+    }
+    return cuda_ok(cudaGetLastError(), "radix sort launch");
+}
+
+}  // namespace
+
+bool launch_radix_sort(Workspace& ws, DType t, void* d_data, size_t n) {
+    switch (t) {
+        case DType::U32: return radix_sort_keys<uint32_t, 0>(ws, d_data, n);
+        case DType::I32: return radix_sort_keys<uint32_t, 1>(ws, d_data, n);
+        case DType::F32: return radix_sort_keys<uint32_t, 2>(ws, d_data, n);
+        case DType::U64: return radix_sort_keys<uint64_t, 0>(ws, d_data, n);
+        case DType::I64: return radix_sort_keys<uint64_t, 1>(ws, d_data, n);
+        case DType::F64: return radix_sort_keys<uint64_t, 2>(ws, d_data, n);
+        default: break;
+    }
+    set_error(PARALLAX_ERR_INVALID_ARGUMENT, "sort: unsupported element type");
+    return false;
+}
+
+}  // namespace pxb

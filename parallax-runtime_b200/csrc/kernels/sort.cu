@@ -20,10 +20,12 @@
 // sort are (key << 32 | value) and sort as plain 64-bit keys, i.e. stably by key.
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "../runtime.hpp"
 #include "../segplan.cuh"
+#include "../sortkey.cuh"
 
 namespace pxb {
 namespace {
@@ -33,22 +35,6 @@ constexpr int kBlock = 256;
 template <typename K> struct SortShape;
 template <> struct SortShape<uint32_t> { static constexpr int ITEMS = 16; };
 template <> struct SortShape<uint64_t> { static constexpr int ITEMS = 8; };
-
-// XF: 0 unsigned (identity), 1 signed integer, 2 IEEE float
-template <typename K, int XF>
-__device__ __forceinline__ K to_key(K b) {
-    constexpr K sign = K(1) << (sizeof(K) * 8 - 1);
-    if constexpr (XF == 1) return b ^ sign;
-    if constexpr (XF == 2) return (b & sign) ? ~b : (b | sign);
-    return b;
-}
-template <typename K, int XF>
-__device__ __forceinline__ K from_key(K k) {
-    constexpr K sign = K(1) << (sizeof(K) * 8 - 1);
-    if constexpr (XF == 1) return k ^ sign;
-    if constexpr (XF == 2) return (k & sign) ? (k ^ sign) : ~k;
-    return k;
-}
 
 template <typename K>
 __device__ __forceinline__ K kmin(K a, K b) { return b < a ? b : a; }
@@ -631,8 +617,21 @@ bool seg_sort_dispatch(Workspace& ws, DType t, const SegSrc& src, uint64_t count
 
 }  // namespace
 
+// Sizes from which the radix sort (a histogram launch plus one pass per key byte) beats the
+// merge sort (a tile-sort launch plus log2(tiles) merge passes). PARALLAX_SORT=merge or
+// =radix forces one path (read on every call).
+constexpr size_t kRadixMin4 = size_t(1) << 16;
+constexpr size_t kRadixMin8 = size_t(1) << 19;
+
 bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
     if (n <= 1) return true;
+    const size_t es = dtype_size(t);
+    bool radix = n >= (es == 4 ? kRadixMin4 : kRadixMin8);
+    if (const char* e = getenv("PARALLAX_SORT")) {
+        if (!strcmp(e, "merge")) radix = false;
+        else if (!strcmp(e, "radix")) radix = true;
+    }
+    if (radix && (es == 4 || es == 8)) return launch_radix_sort(ws, t, d_data, n);
     switch (t) {
         case DType::U32: return sort_keys<uint32_t, 0>(ws, d_data, n);
         case DType::I32: return sort_keys<uint32_t, 1>(ws, d_data, n);

@@ -101,6 +101,9 @@ struct Workspace {
     size_t seg_cap = 0;
     void* d_seg_status = nullptr;         // segmented launches: look-back status entries only
     size_t seg_status_cap = 0;            // in entries
+    void* d_radix = nullptr;              // radix sort: tile claim counters, digit histograms,
+    size_t radix_cap = 0;                 // per-(tile, digit) look-back words
+    uint32_t radix_epoch = 1;             // next epoch of those words, see next_radix_epochs()
     // Bumped whenever a workspace buffer is reallocated: cached graphs captured with older
     // buffer addresses are re-captured.
     uint64_t generation = 0;
@@ -118,6 +121,12 @@ struct Workspace {
     // segment buffer. A buffer of their own (zeroed on (re)allocation) so no other data
     // ever lies where a status word is read.
     void* seg_status(uint64_t entries);
+    // Radix sort buffer (zeroed on (re)allocation): only radix-sort words ever live there.
+    void* radix(size_t bytes);
+    // `count` consecutive 22-bit epochs (one per radix pass) for the radix sort's look-back
+    // words; returns the first. Called before a sort enqueues anything: on wrap-around it
+    // enqueues a clear of the buffer, so no stale word can alias a reused epoch.
+    uint32_t next_radix_epochs(uint32_t count);
     void* stage(int slot, size_t bytes);
     // Look-back status words carry the launch epoch, so stale words from earlier
     // launches read as "not ready" without clearing the array between launches.
@@ -233,6 +242,8 @@ bool launch_compact(Workspace& ws, DType t, CompactMode mode, const Pred& p, con
 bool launch_count_if(Workspace& ws, DType t, const Pred& p, const void* d_in, size_t n,
                      uint64_t* d_count);
 bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n);
+// One-sweep LSD radix sort (kernels/radix.cu); launch_sort picks it for large arrays.
+bool launch_radix_sort(Workspace& ws, DType t, void* d_data, size_t n);
 bool launch_map(Workspace& ws, MapOp op, const void* d_in, void* d_out, size_t n,
                 const void* captures, size_t capture_size);
 bool launch_find(Workspace& ws, DType t, const Pred& p, const void* d_in, size_t n,
