@@ -20,7 +20,11 @@ Lines printed (one JSON line on stdout from rank 0):
           downloads its results inside the timed region;
   roofline of the dominant kernel from live per-launch CUDA events;
   cpu_baseline: the reference's own CPU path (its stdpar.hpp host fallbacks, compiled in
-          oracle/_ref) on a bounded sample of the same workload.
+          oracle/_ref) on a bounded sample of the same workload;
+  workloads: segmented primitives (4096 lognormal segments), map with in-kernel
+          relocation, both device sort paths on 2^26 uint32 keys (bitonic tile sort +
+          merge passes against the one-sweep radix sort the step uses at that size), and
+          the serving mix.
 `--impl reference` runs only that CPU path as the benchmark arm.
 Multi-GPU (torchrun): every rank runs the full workload on its own GPU (replicas, weak
 scaling); time is the max over ranks.
@@ -571,6 +575,8 @@ def main() -> None:
         lib.parallax_set_async(1)
         workloads["segmented"] = run_segmented(px, lib, torch, stream, args.steps, args.warmup, peak)
         workloads["map"] = run_map(px, lib, torch, stream, args.steps, args.warmup, peak)
+        workloads["sort_paths"] = run_sort_paths(px, lib, torch, stream, args.steps, args.warmup,
+                                                 peak)
     lib.parallax_set_async(0)
     lib.parallax_set_stream(None)
     if selected is None and not args.no_workloads and rank == 0:
@@ -782,6 +788,40 @@ def run_map(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dic
             "reduce": {"ms": round(ms_red, 4), "GB_s": round(b_red / ms_red / 1e6, 1)},
             "GB_s": round((b_map + b_red) / (ms_map + ms_red) / 1e6, 1),
             "frac_of_peak": round((b_map + b_red) / (ms_map + ms_red) / 1e6 / peak, 3)}
+
+
+def run_sort_paths(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dict:
+    """Both device sort paths on the same 2^26 uint32 keys (splitmix64 seed 21): the bitonic
+    tile sort + merge passes (PARALLAX_SORT=merge) and the one-sweep radix sort that
+    parallax_sort picks at this size; the two results must be the same bytes."""
+    n = 1 << 26
+    keys = torch.from_numpy(gen("u32_full", 21, n).view(np.int32)).cuda()
+    x = torch.empty_like(keys)
+    h = px.builtin("sort:u32")
+    out, res = {}, {}
+    old = os.environ.get("PARALLAX_SORT")
+    try:
+        for path in ("merge", "radix"):
+            os.environ["PARALLAX_SORT"] = path
+            ms = timed_calls(torch, stream, lambda: lib.parallax_sort(h, x.data_ptr(), n, 4),
+                             steps, warmup, restore=lambda: x.copy_(keys))
+            px.check(f"sort ({path})")
+            stream.synchronize()
+            res[path] = x.clone()
+            gbs = 2 * n * 4 / ms / 1e6
+            out[path] = {"ms": round(ms, 4), "GB_s": round(gbs, 1),
+                         "frac_of_peak": round(gbs / peak, 3),
+                         "Gkeys_s": round(n / ms / 1e6, 2)}
+    finally:
+        if old is None:
+            os.environ.pop("PARALLAX_SORT", None)
+        else:
+            os.environ["PARALLAX_SORT"] = old
+    if not torch.equal(res["merge"], res["radix"]):
+        raise RuntimeError("sort paths: merge and radix results differ")
+    out["workload"] = "2^26 uint32 keys, full range, splitmix64 seed 21 (2n*4 byte basis)"
+    out["radix_speedup"] = round(out["merge"]["ms"] / out["radix"]["ms"], 2)
+    return out
 
 
 class LoadgenConfig(C.Structure):
