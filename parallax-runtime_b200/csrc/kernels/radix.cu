@@ -42,6 +42,7 @@ constexpr uint64_t kValMask = (uint64_t(1) << kValBits) - 1;
 constexpr uint64_t kStAgg = uint64_t(1) << kValBits;
 constexpr uint64_t kStInc = uint64_t(2) << kValBits;
 constexpr int kEpochShift = 42;
+constexpr int kLookWindow = 4;  // predecessor words a look-back step loads at once
 
 template <typename K> struct RadixShape;
 template <> struct RadixShape<uint32_t> { static constexpr int BLOCK = 512, ITEMS = 16; };
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, 2)
     K* const s_keys = reinterpret_cast<K*>(smem_raw);
     uint32_t* const s_wh = reinterpret_cast<uint32_t*>(smem_raw + (size_t)TILE * sizeof(K));
     __shared__ uint64_t s_goff[kBins];
+    __shared__ uint32_t s_loc[kBins];
     __shared__ uint64_t s_part64[kBins / 32];
     __shared__ uint32_t s_part32[kBins / 32];
     __shared__ uint32_t s_tile;
@@ -268,40 +270,47 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, 2)
     if (tile == 0)
         start = digit_exclusive_scan<uint64_t, BLOCK>(tid < kBins ? (uint64_t)hist[tid] : 0ull,
                                                       s_part64);
-    if (tid < kBins) {
-#pragma unroll 8
-        for (int w = 0; w < TABLES; ++w) s_wh[w * kBins + tid] += loc;
-    }
+    if (tid < kBins) s_loc[tid] = loc;
     __syncthreads();
 
     // 4a. keys in digit order in shared memory
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         const uint32_t r = (i % 2 == 0) ? (rk[i / 2] & 0xffffu) : (rk[i / 2] >> 16);
-        s_keys[wh[(i / HALF) * kBins + digit_of(k[i], shift)] + r] = k[i];
+        const uint32_t d = digit_of(k[i], shift);
+        s_keys[s_loc[d] + wh[(i / HALF) * kBins + d] + r] = k[i];
     }
 
-    // 3b. look-back, one thread per digit
+    // 3b. look-back, one thread per digit. The words of the kLookWindow nearest unvisited
+    // predecessors are loaded together, so one round trip to L2 covers several tiles; they
+    // are then consumed in order until an inclusive count ends the walk.
     if (tid < kBins) {
         uint64_t excl = start;
         if (tile != 0) {
-            for (int64_t j = (int64_t)tile - 1; j >= 0; --j) {
-                uint64_t w = 0;
-                uint32_t spins = 0;
-                bool gave_up = false;
-                for (;;) {
-                    w = ld_relaxed_u64(&status[(uint64_t)j * kBins + tid]);
-                    if ((uint32_t)(w >> kEpochShift) == epoch && (w & (kStAgg | kStInc))) break;
-                    if (++spins > kSpinLimit) {
-                        *err = 1;
-                        gave_up = true;
-                        break;
+            bool done = false;
+            for (int64_t j = (int64_t)tile - 1; !done && j >= 0; j -= kLookWindow) {
+                uint64_t w[kLookWindow];
+#pragma unroll
+                for (int q = 0; q < kLookWindow; ++q)
+                    w[q] = j - q >= 0 ? ld_relaxed_u64(&status[(uint64_t)(j - q) * kBins + tid]) : 0;
+#pragma unroll
+                for (int q = 0; q < kLookWindow; ++q) {
+                    if (done || j - q < 0) break;
+                    uint64_t v = w[q];
+                    uint32_t spins = 0;
+                    while (!((uint32_t)(v >> kEpochShift) == epoch && (v & (kStAgg | kStInc)))) {
+                        if (++spins > kSpinLimit) {
+                            *err = 1;
+                            done = true;
+                            break;
+                        }
+                        if (spins > 8) nanosleep_ns(32);
+                        v = ld_relaxed_u64(&status[(uint64_t)(j - q) * kBins + tid]);
                     }
-                    if (spins > 8) nanosleep_ns(32);
+                    if (done) break;
+                    excl += v & kValMask;
+                    if (v & kStInc) done = true;
                 }
-                if (gave_up) break;
-                excl += w & kValMask;
-                if (w & kStInc) break;
             }
         }
         st_relaxed_u64(&status[tile * kBins + tid],
