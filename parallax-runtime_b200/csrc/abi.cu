@@ -109,6 +109,28 @@ Workspace* begin(Handle* h, const char* fn, size_t elem_size, std::initializer_l
 
 int finish(Workspace& ws) { return ws.async ? PARALLAX_OK : sync_stream(ws); }
 
+// Operands from this size up whose host copies a synchronous scan overlaps with its tiles.
+constexpr size_t kCopyOverlapMin = size_t(64) << 20;
+
+// A pointer into a live arena block in coherent mode (the call copies it both ways).
+bool coherent_arena(const void* p) {
+    ArenaBlock b;
+    return p && arena_contains(p) && arena_find(p, &b) && b.residency != PARALLAX_DEVICE_RESIDENT;
+}
+// Device memory a call uses in place: a device-resident arena block or a CUDA pointer.
+bool in_place_device(const void* p) {
+    if (!p) return false;
+    if (arena_contains(p)) {
+        ArenaBlock b;
+        return arena_find(p, &b) && b.residency == PARALLAX_DEVICE_RESIDENT;
+    }
+    cudaPointerAttributes attr;
+    const bool dev = cudaPointerGetAttributes(&attr, p) == cudaSuccess &&
+                     (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    return dev;
+}
+
 // Grid for USER kernels (grid-stride contract in kernel_abi.h).
 dim3 user_grid(size_t count) {
     size_t blocks = (count + 255) / 256;
@@ -306,10 +328,16 @@ PXB_EXPORT void parallax_scan(parallax_kernel_t scan_kernel, parallax_kernel_t a
     }
     if (count <= 1) return;  // identity (kernel_launcher.cpp:1291)
     size_t bytes = count * dtype_size(h->dtype);
+    const bool overlap = !ws->async && bytes >= kCopyOverlapMin && coherent_arena(data);
     Operand op;
-    if (!resolve_operand(*ws, data, bytes, true, 0, &op)) return;
-    if (!launch_scan(*ws, h->dtype, false, op.dev, op.dev, count, nullptr)) return;
-    if (!writeback_operand(*ws, op, bytes)) return;
+    if (!resolve_operand(*ws, data, bytes, !overlap, 0, &op)) return;
+    if (overlap) {
+        if (!launch_scan_copies(*ws, h->dtype, false, data, op.dev, data, op.dev, count, nullptr))
+            return;
+    } else {
+        if (!launch_scan(*ws, h->dtype, false, op.dev, op.dev, count, nullptr)) return;
+        if (!writeback_operand(*ws, op, bytes)) return;
+    }
     finish(*ws);
 }
 
@@ -328,11 +356,20 @@ PXB_EXPORT void parallax_exclusive_scan(parallax_kernel_t scan_kernel,
     if (count == 0) return;
     size_t bytes = count * dtype_size(h->dtype);
     uint64_t zero = 0;
+    const bool in_c = coherent_arena(input), out_c = coherent_arena(output);
+    const bool overlap = !ws->async && bytes >= kCopyOverlapMin && (in_c || out_c) &&
+                         (in_c || in_place_device(input)) && (out_c || in_place_device(output));
     Operand oi, oo;
-    if (!resolve_operand(*ws, input, bytes, true, 0, &oi)) return;
+    if (!resolve_operand(*ws, input, bytes, !overlap, 0, &oi)) return;
     if (!resolve_operand(*ws, output, bytes, false, 1, &oo)) return;
-    if (!launch_scan(*ws, h->dtype, true, oi.dev, oo.dev, count, init ? init : &zero)) return;
-    if (!writeback_operand(*ws, oo, bytes)) return;
+    if (overlap) {
+        if (!launch_scan_copies(*ws, h->dtype, true, in_c ? input : nullptr, oi.dev,
+                                out_c ? output : nullptr, oo.dev, count, init ? init : &zero))
+            return;
+    } else {
+        if (!launch_scan(*ws, h->dtype, true, oi.dev, oo.dev, count, init ? init : &zero)) return;
+        if (!writeback_operand(*ws, oo, bytes)) return;
+    }
     finish(*ws);
 }
 

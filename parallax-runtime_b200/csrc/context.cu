@@ -208,6 +208,20 @@ void* Workspace::radix(size_t bytes) {
     return d_radix;
 }
 
+bool Workspace::copy_streams() {
+    if (copy_up && copy_down && ev_copy[3]) return true;
+    if (!copy_up && !cuda_ok(cudaStreamCreateWithFlags(&copy_up, cudaStreamNonBlocking),
+                             "cudaStreamCreate(upload)"))
+        return false;
+    if (!copy_down && !cuda_ok(cudaStreamCreateWithFlags(&copy_down, cudaStreamNonBlocking),
+                               "cudaStreamCreate(download)"))
+        return false;
+    for (cudaEvent_t& e : ev_copy)
+        if (!e && !cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate"))
+            return false;
+    return true;
+}
+
 uint32_t Workspace::next_radix_epochs(uint32_t count) {
     if (radix_epoch + count >= (1u << 22)) {
         cudaMemsetAsync(d_radix, 0, radix_cap, stream());

@@ -19,8 +19,8 @@
 //   5. rescans each row, writes results into the staged tile and stores it with one bulk
 //      copy.
 // HBM traffic is the algorithmic minimum: n*s read + n*s written.
-// Accumulation: fp32 data is scanned per thread in fp32 (12 terms) and carried across
-// threads, warps and tiles in fp64; integers wrap around in their unsigned type.
+// Accumulation: fp32 data is scanned per thread in fp32 (28 terms per sub-tile) and carried
+// across threads, warps and tiles in fp64; integers wrap around in their unsigned type.
 #include <stdint.h>
 #include <string.h>
 
@@ -150,10 +150,13 @@ __device__ __forceinline__ void scan_tile(T* buf, uint64_t* bars, uint32_t parit
 
 // One CTA per 112 KiB tile, in blockIdx order: unaligned operands (BULK = false) and the
 // allocation-free entry point.
+// `tile0` is the first tile of this launch: a scan launched in chunks (so its copies can
+// overlap its tiles) passes each chunk's first tile, and every chunk shares one look-back
+// epoch, so the first tile of a chunk looks back into the chunks before it.
 template <typename T, bool EXCL, bool BULK>
 __global__ void __launch_bounds__(kBlock, 2)
 k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan)
-       typename ScanTypes<T>::A init, TileStatus<typename ScanTypes<T>::A> ts) {
+       typename ScanTypes<T>::A init, TileStatus<typename ScanTypes<T>::A> ts, uint64_t tile0) {
     using A = typename ScanTypes<T>::A;
     constexpr int SUB = ScanShape<T>::SUB;
     constexpr int TILE = ScanShape<T>::TILE;
@@ -164,7 +167,7 @@ k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan
     __shared__ A s_red[kBlock / 32 + 1];
     __shared__ int s_first[kBlock / 32];
     const int tid = threadIdx.x;
-    const uint64_t tile = blockIdx.x;
+    const uint64_t tile = tile0 + blockIdx.x;
     const uint64_t base = tile * (uint64_t)TILE;
     const uint64_t rem = n - base;
     const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
@@ -259,13 +262,15 @@ k_scan_persistent(const T* in, T* out, uint64_t n, uint64_t num_tiles,
     }
 }
 
+// Launches tiles [tile0, tile0 + count).
 template <typename T, bool EXCL, bool BULK>
 bool launch_tiles_single(const T* in, T* out, uint64_t n, typename ScanTypes<T>::A init,
-                         TileStatus<typename ScanTypes<T>::A> ts, uint64_t tiles,
-                         cudaStream_t s) {
+                         TileStatus<typename ScanTypes<T>::A> ts, uint64_t count,
+                         cudaStream_t s, uint64_t tile0 = 0) {
     if (!smem_opt_in<k_scan<T, EXCL, BULK>>(ScanShape<T>::SMEM))
         return cuda_ok(cudaGetLastError(), "k_scan shared-memory opt-in");
-    k_scan<T, EXCL, BULK><<<(unsigned)tiles, kBlock, ScanShape<T>::SMEM, s>>>(in, out, n, init, ts);
+    k_scan<T, EXCL, BULK><<<(unsigned)count, kBlock, ScanShape<T>::SMEM, s>>>(in, out, n, init,
+                                                                            ts, tile0);
     return true;
 }
 
@@ -326,7 +331,103 @@ bool scan_typed(Workspace& ws, bool exclusive, const void* d_in, void* d_out, ui
     return cuda_ok(cudaGetLastError(), "k_scan launch");
 }
 
+// Scan of host arena operands with the copies interleaved with the tiles. The tiles are
+// launched in chunks of kCopyChunkTiles on the workspace stream; chunk c's upload runs on
+// the workspace's upload stream and chunk c's download on its download stream, ordered by
+// events, so while the tiles of chunk c run, chunk c+1 is on its way up and chunk c-1 on its
+// way down (the two copy directions run on separate copy engines). All chunks share one
+// look-back epoch: the result is the same scan as one launch over every tile.
+constexpr uint64_t kCopyChunkTiles = 296;  // two waves of two CTAs per SM: ~33 MB of fp32
+
+template <typename T>
+bool scan_copies_typed(Workspace& ws, bool exclusive, const void* h_in, const void* d_in,
+                       void* h_out, void* d_out, uint64_t n, const void* init_host) {
+    using A = typename ScanTypes<T>::A;
+    constexpr int TILE = ScanShape<T>::TILE;
+    const uint64_t tiles = (n + TILE - 1) / TILE;
+    const bool bulk = (reinterpret_cast<uintptr_t>(d_in) % 16 == 0) &&
+                      (reinterpret_cast<uintptr_t>(d_out) % 16 == 0);
+    if (tiles > 0x7fffffffull || !bulk || !ws.copy_streams()) {
+        cudaGetLastError();
+        // one launch, copies before and after it
+        cudaStream_t s = ws.stream();
+        if (h_in && !arena_copy_async(const_cast<void*>(d_in), h_in, n * sizeof(T), true, s))
+            return false;
+        if (!scan_typed<T>(ws, exclusive, d_in, d_out, n, init_host)) return false;
+        return !h_out || arena_copy_async(h_out, d_out, n * sizeof(T), false, s);
+    }
+    char* scratch = ws.scratch(tiles);
+    if (!scratch) return false;
+    auto ts = tile_status_at<A>(scratch, ws.next_epoch(), &ws.d_slot->spin_error);
+    A init = A(0);
+    if (exclusive && init_host) {
+        T v;
+        memcpy(&v, init_host, sizeof(T));
+        init = (A)v;
+    }
+    const T* in = static_cast<const T*>(d_in);
+    T* out = static_cast<T*>(d_out);
+    cudaStream_t s = ws.stream();
+    // the copy streams start after everything already queued on the workspace stream
+    if (!cuda_ok(cudaEventRecord(ws.ev_copy[0], s), "copy event") ||
+        !cuda_ok(cudaStreamWaitEvent(ws.copy_up, ws.ev_copy[0], 0), "copy wait") ||
+        !cuda_ok(cudaStreamWaitEvent(ws.copy_down, ws.ev_copy[0], 0), "copy wait"))
+        return false;
+    uint64_t chunks = 0;
+    for (uint64_t t0 = 0; t0 < tiles; t0 += kCopyChunkTiles, ++chunks) {
+        const uint64_t t1 = t0 + kCopyChunkTiles < tiles ? t0 + kCopyChunkTiles : tiles;
+        const uint64_t e0 = t0 * TILE, e1 = t1 * TILE < n ? t1 * TILE : n;
+        const size_t off = e0 * sizeof(T), bytes = (e1 - e0) * sizeof(T);
+        if (h_in) {
+            if (!arena_copy_async(const_cast<T*>(in) + e0, static_cast<const char*>(h_in) + off,
+                                  bytes, true, ws.copy_up) ||
+                !cuda_ok(cudaEventRecord(ws.ev_copy[1], ws.copy_up), "copy event") ||
+                !cuda_ok(cudaStreamWaitEvent(s, ws.ev_copy[1], 0), "copy wait"))
+                return false;
+        }
+        const bool ok =
+            exclusive ? launch_tiles_single<T, true, true>(in, out, n, init, ts, t1 - t0, s, t0)
+                      : launch_tiles_single<T, false, true>(in, out, n, init, ts, t1 - t0, s, t0);
+        if (!ok) return false;
+        if (h_out) {
+            if (!cuda_ok(cudaEventRecord(ws.ev_copy[2], s), "copy event") ||
+                !cuda_ok(cudaStreamWaitEvent(ws.copy_down, ws.ev_copy[2], 0), "copy wait") ||
+                !arena_copy_async(static_cast<char*>(h_out) + off, out + e0, bytes, false,
+                                  ws.copy_down))
+                return false;
+        }
+    }
+    count_launch((unsigned)chunks);
+    // the workspace stream (what a synchronous call waits on) ends after the last download
+    if (!cuda_ok(cudaEventRecord(ws.ev_copy[3], ws.copy_down), "copy event") ||
+        !cuda_ok(cudaStreamWaitEvent(s, ws.ev_copy[3], 0), "copy wait"))
+        return false;
+    return cuda_ok(cudaGetLastError(), "k_scan launch");
+}
+
 }  // namespace
+
+bool launch_scan_copies(Workspace& ws, DType t, bool exclusive, const void* h_in,
+                        const void* d_in, void* h_out, void* d_out, size_t n,
+                        const void* init_host) {
+    switch (t) {
+        case DType::F32:
+            return scan_copies_typed<float>(ws, exclusive, h_in, d_in, h_out, d_out, n, init_host);
+        case DType::F64:
+            return scan_copies_typed<double>(ws, exclusive, h_in, d_in, h_out, d_out, n, init_host);
+        case DType::I32:
+            return scan_copies_typed<int32_t>(ws, exclusive, h_in, d_in, h_out, d_out, n, init_host);
+        case DType::I64:
+            return scan_copies_typed<int64_t>(ws, exclusive, h_in, d_in, h_out, d_out, n, init_host);
+        case DType::U32:
+            return scan_copies_typed<uint32_t>(ws, exclusive, h_in, d_in, h_out, d_out, n, init_host);
+        case DType::U64:
+            return scan_copies_typed<uint64_t>(ws, exclusive, h_in, d_in, h_out, d_out, n, init_host);
+        default: break;
+    }
+    set_error(PARALLAX_ERR_INVALID_ARGUMENT, "scan: unsupported element type");
+    return false;
+}
 
 bool launch_scan(Workspace& ws, DType t, bool exclusive, const void* d_in, void* d_out, size_t n,
                  const void* init_host) {

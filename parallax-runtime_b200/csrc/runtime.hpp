@@ -104,6 +104,11 @@ struct Workspace {
     void* d_radix = nullptr;              // radix sort: tile claim counters, digit histograms,
     size_t radix_cap = 0;                 // per-(tile, digit) look-back words
     uint32_t radix_epoch = 1;             // next epoch of those words, see next_radix_epochs()
+    // Copy streams of calls whose host operand copies overlap their kernels (uploads and
+    // downloads on separate copy engines) and the events that order them; see copy_streams().
+    cudaStream_t copy_up = nullptr;
+    cudaStream_t copy_down = nullptr;
+    cudaEvent_t ev_copy[4] = {nullptr, nullptr, nullptr, nullptr};
     // Bumped whenever a workspace buffer is reallocated: cached graphs captured with older
     // buffer addresses are re-captured.
     uint64_t generation = 0;
@@ -128,6 +133,8 @@ struct Workspace {
     // enqueues a clear of the buffer, so no stale word can alias a reused epoch.
     uint32_t next_radix_epochs(uint32_t count);
     void* stage(int slot, size_t bytes);
+    // Creates the copy streams and events on first use; false when that fails.
+    bool copy_streams();
     // Look-back status words carry the launch epoch, so stale words from earlier
     // launches read as "not ready" without clearing the array between launches.
     uint32_t next_epoch();
@@ -233,6 +240,12 @@ Handle* builtin_handle(const char* spec);
 // Reduce: writes one element (type of dtype; sum of f32 is rounded from fp64) to d_out.
 bool launch_reduce(Workspace& ws, DType t, RedOp op, const void* d_in, size_t n, void* d_out);
 // Inclusive (init == nullptr) or exclusive scan; in-place allowed.
+// Scan of host arena operands (page-locked mirror addresses h_in / h_out, either may be null
+// for a device-resident side) whose host-device copies overlap the scan: the tiles run in
+// chunks, each chunk's upload and download on the workspace's copy streams.
+bool launch_scan_copies(Workspace& ws, DType t, bool exclusive, const void* h_in,
+                        const void* d_in, void* h_out, void* d_out, size_t n,
+                        const void* init_host);
 bool launch_scan(Workspace& ws, DType t, bool exclusive, const void* d_in, void* d_out,
                  size_t n, const void* init_host);
 enum class CompactMode : int { SELECT = 0, UNIQUE = 1, PARTITION = 2 };
