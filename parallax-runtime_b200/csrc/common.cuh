@@ -28,6 +28,9 @@ constexpr int32_t kErrRadixRange = 0x5e92;
 // modulus that is zero in the element type; nothing matches it.
 struct FastMod32 {
     uint32_t am = 0, magic = 0, sh1 = 0, sh2 = 0;
+    // zero-remainder test (Granlund and Montgomery 1994, section 9): d = odd * 2^tz divides n
+    // iff rotr(n * odd^-1 mod 2^32, tz) <= floor((2^32 - 1) / d)
+    uint32_t inv = 0, tz = 0, lim = 0;
     static FastMod32 make(int64_t m) {  // m already converted to the element type
         FastMod32 f;
         const uint64_t d = (uint64_t)(m < 0 ? -m : m);
@@ -40,12 +43,36 @@ struct FastMod32 {
         f.magic = (uint32_t)(num / d + 1);
         f.sh1 = l < 1 ? l : 1;
         f.sh2 = l > 1 ? l - 1 : 0;
+        uint32_t odd = (uint32_t)d;
+        while (!(odd & 1u)) {
+            odd >>= 1;
+            ++f.tz;
+        }
+        uint32_t inv = odd;  // Newton iteration doubles the correct low bits: 3 -> 48
+        for (int i = 0; i < 4; ++i) inv *= 2u - odd * inv;
+        f.inv = inv;
+        f.lim = 0xffffffffu / (uint32_t)d;
         return f;
+    }
+    // d divides n (am != 0)
+    __device__ __forceinline__ bool divides(uint32_t n) const {
+        const uint32_t q = n * inv;
+        return __funnelshift_r(q, q, tz) <= lim;
     }
     __device__ __forceinline__ uint32_t rem(uint32_t n) const {
         const uint32_t t = __umulhi(magic, n);
         const uint32_t q = (t + ((n - t) >> sh1)) >> sh2;
         return n - q * am;
+    }
+    // x % m == 0 (C semantics: the sign of x does not matter)
+    template <typename T>
+    __device__ __forceinline__ bool eq0(T x) const {
+        static_assert(sizeof(T) == 4, "32-bit integers");
+        if constexpr (T(-1) < T(0)) {  // |INT_MIN| = 2^31 as unsigned
+            return am != 0 && divides(x < T(0) ? 0u - (uint32_t)x : (uint32_t)x);
+        } else {
+            return am != 0 && divides((uint32_t)x);
+        }
     }
     template <typename T>
     __device__ __forceinline__ bool eq(T x, T r) const {

@@ -85,7 +85,17 @@ struct PredDev {
             PXB_ROW(EQ, x[j] == c)
             PXB_ROW(NE, x[j] != c)
             PXB_ROW(NONZERO, x[j] != T(0))
-            PXB_ROW(MOD, mod_eq(x[j]))
+            case PredKind::MOD:
+                if constexpr (std::is_integral<T>::value && sizeof(T) == 4) {
+                    if (r == T(0)) {  // divisibility: a multiply and a compare per element
+#pragma unroll
+                        for (int j = 0; j < ITEMS; ++j) f |= (uint32_t)(fm.eq0(x[j]) != negate) << j;
+                        break;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < ITEMS; ++j) f |= (uint32_t)(mod_eq(x[j]) != negate) << j;
+                break;
 #undef PXB_ROW
             default: break;
         }

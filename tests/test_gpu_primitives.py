@@ -145,13 +145,21 @@ PREDS = [  # (spec tail, oracle kind, c, m, r)
 @pytest.mark.parametrize("m", [1, 2, 3, 5, 7, 10, 641, 65537, 6700417, 2**31 - 1, -1, -3, -7,
                                -(2**31) + 1, 2**31, 2**32 - 1, -(2**32) + 5])
 def test_modulo_predicate_divisors(lib, px, ox, dev, t, m):
-    """x % m == r through the multiply-high remainder (compaction and the count pass of
-    partition): every divisor class, both signs, the extreme values of the type."""
+    """x % m == r through the multiply-high remainder and, for r == 0, the multiply-by-inverse
+    divisibility test (compaction and the count pass of partition): every divisor class,
+    both signs, the extreme values of the type, exact multiples of m."""
     x = make(ox, t, 100003, seed=23)
     info = np.iinfo(x.dtype)
     x[:6] = np.array([0, 1, info.max, info.min, info.max - 1, info.min + 1]).astype(x.dtype)
     if t == "i32":
         x[6:8] = np.array([-1, -2], dtype=np.int32)
+    # exact multiples of m (both signs where the type has them) and their neighbours, so the
+    # zero-remainder test sees true cases for every divisor
+    k = np.arange(-40, 41, dtype=np.int64)
+    mult = (k * m).astype(np.int64)
+    mult = mult[(mult >= int(info.min)) & (mult <= int(info.max))]
+    near = np.concatenate([mult, mult[mult < int(info.max)] + 1, mult[mult > int(info.min)] - 1])
+    x[8:8 + near.size] = near.astype(x.dtype)
     for r in (0, 1, 2, -1):
         spec = f"copy_if:{t}:mod:{m}:{r}"
         got, k = compact_dev(lib, px, dev, spec, x)
