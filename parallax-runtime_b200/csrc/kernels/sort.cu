@@ -623,10 +623,12 @@ bool seg_sort_dispatch(Workspace& ws, DType t, const SegSrc& src, uint64_t count
 constexpr size_t kRadixMin4 = size_t(1) << 16;
 constexpr size_t kRadixMin8 = size_t(1) << 19;
 
+size_t sort_radix_min(DType t) { return dtype_size(t) == 4 ? kRadixMin4 : kRadixMin8; }
+
 bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
     if (n <= 1) return true;
     const size_t es = dtype_size(t);
-    bool radix = n >= (es == 4 ? kRadixMin4 : kRadixMin8);
+    bool radix = n >= sort_radix_min(t);
     if (const char* e = getenv("PARALLAX_SORT")) {
         if (!strcmp(e, "merge")) radix = false;
         else if (!strcmp(e, "radix")) radix = true;

@@ -255,6 +255,8 @@ bool launch_compact(Workspace& ws, DType t, CompactMode mode, const Pred& p, con
 bool launch_count_if(Workspace& ws, DType t, const Pred& p, const void* d_in, size_t n,
                      uint64_t* d_count);
 bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n);
+// Smallest array launch_sort gives to the radix sort (by default; PARALLAX_SORT overrides).
+size_t sort_radix_min(DType t);
 // One-sweep LSD radix sort (kernels/radix.cu); launch_sort picks it for large arrays.
 bool launch_radix_sort(Workspace& ws, DType t, void* d_data, size_t n);
 bool launch_map(Workspace& ws, MapOp op, const void* d_in, void* d_out, size_t n,

@@ -117,7 +117,7 @@ class Server {
         if (c) cfg = *c;
         if (cfg.lanes == 0) cfg.lanes = 8;
         if (cfg.max_batch == 0) cfg.max_batch = 1024;
-        if (cfg.solo_elements == 0) cfg.solo_elements = 1ull << 22;
+        if (cfg.solo_elements == 0) cfg.solo_elements = 1ull << 18;
         if (cfg.inflight_bytes == 0) cfg.inflight_bytes = parallax_arena_capacity() / 2;
         lanes.resize(cfg.lanes);
         for (Lane& l : lanes) {
@@ -139,6 +139,8 @@ class Server {
 
     void submit(Request* r) {
         r->coalescible = r->coalescible && r->n <= cfg.solo_elements;
+        // a sort long enough for the radix path runs alone: the segmented sort merges
+        if (r->op == ReqOp::SORT && r->n >= sort_radix_min(r->t)) r->coalescible = false;
         {
             std::lock_guard<std::mutex> g(mu);
             queue.push_back(r);
