@@ -196,7 +196,7 @@ __device__ __forceinline__ void compact_tile(T* buf, uint64_t* bars, uint32_t pa
         for (int s = 0; s < kSub; ++s) woff[s] = shfl_idx(vex, s * WARPS + warp);
     }
     const uint64_t prefix =
-        lookback_cta<uint64_t, kBlock>(ts, tile, (uint64_t)tile_kept, sm.red, sm.first);
+        lookback_cta<uint64_t, kBlock, true>(ts, tile, (uint64_t)tile_kept, sm.red, sm.first);
     if (MODE != 2 && last_tile && tid == 0) *count_out = prefix + tile_kept;
 
     if constexpr (MODE == 2) {

@@ -113,7 +113,7 @@ __device__ __forceinline__ void scan_tile(T* buf, uint64_t* bars, uint32_t parit
 #pragma unroll
         for (int s = 0; s < kSub; ++s) woff[s] = shfl_idx(vex, s * WARPS + warp);
     }
-    const A prefix = lookback_cta<A, kBlock>(ts, tile, agg, red, first);
+    const A prefix = lookback_cta<A, kBlock, true>(ts, tile, agg, red, first);
 
     // ---- phase 2: scan each row and write the results in place ----
 #pragma unroll

@@ -127,7 +127,31 @@ __device__ __forceinline__ A lookback(const TileStatus<A>& ts, uint64_t tile, A 
 // `lo` is the first index of the chain (0 for a whole array, a segment's first tile for the
 // segmented kernels): that tile publishes its inclusive prefix at once, and indices below
 // it are never polled.
-template <typename A, int BLOCK>
+// Waits (bounded) until predecessor idx has published, then returns its state (1 AGG,
+// 2 INC) and value; a wait that gives up records the error and reads as INC with value 0.
+template <typename A>
+__device__ __forceinline__ uint32_t poll_status(const TileStatus<A>& ts, int64_t idx, uint32_t ep,
+                                                A* v) {
+    uint32_t f = 0, spins = 0;
+    for (;;) {
+        f = ld_acquire_u32(&ts.e[idx].flag);
+        if ((f & ~3u) == ep && (f & 3u) != 0u) break;
+        if (++spins > kSpinLimit) {
+            *ts.err = 1;
+            *v = A(0);
+            return 2u;
+        }
+        if (spins > 16) nanosleep_ns(64);
+    }
+    const uint32_t state = f & 3u;
+    *v = state == 2u ? get_val<A>(&ts.e[idx].inc) : get_val<A>(&ts.e[idx].agg);
+    return state;
+}
+
+// NEAR_FIRST: warp 0 alone inspects the 32 nearest predecessors first, and the CTA-wide
+// rounds run only when none of them holds an inclusive prefix (in the steady state one of
+// them does, and 32 polls cost far less than BLOCK).
+template <typename A, int BLOCK, bool NEAR_FIRST = false>
 __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile, A agg, A* red,
                                           int* first, uint64_t lo = 0) {
     constexpr int WARPS = BLOCK / 32;
@@ -146,6 +170,33 @@ __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile
     }
     A excl = A(0);
     int64_t pred = (int64_t)tile - 1;
+    if constexpr (NEAR_FIRST) {
+        if (warp == 0) {
+            const int64_t idx = pred - lane;
+            A v = A(0);
+            const uint32_t state = idx >= (int64_t)lo ? poll_status(ts, idx, ep, &v) : 2u;
+            const unsigned m = __ballot_sync(0xffffffffu, state == 2u);
+            const int f = m ? __ffs(m) - 1 : 32;
+            A c = lane <= f ? v : A(0);
+            c = warp_reduce(c, OpSum());
+            if (lane == 0) {
+                red[0] = c;
+                first[0] = m != 0u;
+            }
+        }
+        __syncthreads();
+        excl = red[0];
+        const bool done = first[0] != 0;
+        __syncthreads();  // red / first reusable
+        if (done) {
+            if (tid == 0) {
+                put_val(&ts.e[tile].inc, excl + agg);
+                st_release_u32(&ts.e[tile].flag, ep | 2u);
+            }
+            return excl;
+        }
+        pred -= 32;
+    }
     for (;;) {
         const int64_t idx = pred - tid;
         uint32_t state = 2u;
