@@ -48,9 +48,12 @@ template <typename K> struct RadixShape;
 template <> struct RadixShape<uint32_t> { static constexpr int BLOCK = 512, ITEMS = 16; };
 template <> struct RadixShape<uint64_t> { static constexpr int BLOCK = 512, ITEMS = 8; };
 
-// Each warp ranks its keys as kSubs independent streams (the first and second half of its
-// keys), each with its own count and mask tables, so the two dependency chains overlap.
-constexpr int kSubs = 2;
+// Each warp may rank its keys as kSubs independent streams (consecutive parts of its keys),
+// each with its own count and mask tables, so the dependency chains overlap. Measured on a
+// 2^26-key pass: one stream at three CTAs per SM (0.338 ms, some registers spilled to fit)
+// beats two streams at two CTAs per SM (0.362 ms) and at three (0.378 ms).
+constexpr int kSubs = 1;
+constexpr int kPassCtasPerSm = 3;
 
 template <typename K>
 constexpr size_t radix_smem() {
@@ -151,13 +154,13 @@ __device__ __forceinline__ T digit_exclusive_scan(T v, T* part) {
 // XF_IN transforms keys as they are read (the first pass reads the caller's values),
 // XF_OUT restores them as they are written (the last pass writes the caller's values).
 template <typename K, int XF_IN, int XF_OUT>
-__global__ void __launch_bounds__(RadixShape<K>::BLOCK, 2)
+__global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     k_radix_pass(const K* __restrict__ in, K* __restrict__ out, uint64_t n, int shift,
                  const unsigned long long* __restrict__ hist, uint64_t* status, uint32_t epoch,
                  uint64_t tiles, uint32_t* counters, volatile int32_t* err) {
     constexpr int BLOCK = RadixShape<K>::BLOCK, ITEMS = RadixShape<K>::ITEMS;
     constexpr int TILE = BLOCK * ITEMS, WARPS = BLOCK / 32;
-    constexpr int TABLES = WARPS * kSubs, HALF = ITEMS / kSubs;
+    constexpr int TABLES = WARPS * kSubs, STREAM_ITEMS = ITEMS / kSubs;
     static_assert(BLOCK >= kBins, "one thread per digit");
     static_assert(ITEMS % kSubs == 0, "whole streams");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -215,16 +218,16 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, 2)
     // stream's running count of its digit plus its lower peers, and the highest peer
     // advances the count. This keeps the ranking off the SM's narrow branch unit (where match-any
     // issues) and off the ALU (eight ballots per key cost more than the whole pass).
-    static_assert(ITEMS % 2 == 0 && 32 * HALF <= 0xffff, "two 16-bit ranks per register");
+    static_assert(ITEMS % 2 == 0 && 32 * STREAM_ITEMS <= 0xffff, "two 16-bit ranks per register");
     uint32_t rk[ITEMS / 2];  // rank within the item's stream, two per register
     const uint32_t lt = lanemask_lt();
     const uint32_t le = lt | (1u << lane);
 #pragma unroll
-    for (int j = 0; j < HALF; ++j) {  // item j of every stream
+    for (int j = 0; j < STREAM_ITEMS; ++j) {  // item j of every stream
         uint32_t d[kSubs], peers[kSubs], c[kSubs];
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
-            d[t] = digit_of(k[t * HALF + j], shift) + t * kBins;
+            d[t] = digit_of(k[t * STREAM_ITEMS + j], shift) + t * kBins;
             atomicOr(&mm[d[t]], 1u << lane);
         }
         __syncwarp();
@@ -244,7 +247,7 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, 2)
         __syncwarp();
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
-            const int i = t * HALF + j;
+            const int i = t * STREAM_ITEMS + j;
             if (i % 2 == 0) rk[i / 2] = c[t];
             else rk[i / 2] |= c[t] << 16;
         }
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, 2)
     for (int i = 0; i < ITEMS; ++i) {
         const uint32_t r = (i % 2 == 0) ? (rk[i / 2] & 0xffffu) : (rk[i / 2] >> 16);
         const uint32_t d = digit_of(k[i], shift);
-        s_keys[s_loc[d] + wh[(i / HALF) * kBins + d] + r] = k[i];
+        s_keys[s_loc[d] + wh[(i / STREAM_ITEMS) * kBins + d] + r] = k[i];
     }
 
     // 3b. look-back, one thread per digit. The words of the kLookWindow nearest unvisited
