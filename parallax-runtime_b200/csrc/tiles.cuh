@@ -1,7 +1,7 @@
 // Tile staging shared by the single-pass scan and compaction kernels.
 //
 // A tile is NSUB sub-tiles of kBlock x ITEMS elements. One thread issues one 1-D bulk copy
-// (cp.async.bulk, CTA-local, no multicast) per sub-tile, each completing on its own
+// (cp.async.bulk into the CTA's own shared memory) per sub-tile, each completing on its own
 // mbarrier, so work starts when the first sub-tile lands and the whole tile's bytes are in
 // flight at once. The bulk-copied part of a tile is its 16-byte-aligned prefix; the ragged
 // end of the last tile and the padding up to the tile size are filled with plain loads

@@ -1,6 +1,6 @@
 // Thin wrappers over the sm_90+/sm_100a bulk-copy (TMA, non-tensor) and mbarrier PTX
-// used to stage whole tiles in shared memory. All copies are 1-D, CTA-local, and never
-// use cluster multicast.
+// used to stage whole tiles in shared memory. All copies are 1-D and CTA-local: each one
+// moves data between global memory and the issuing CTA's own shared memory only.
 //
 // Alignment rules the callers guarantee: global and shared addresses 16-byte aligned,
 // sizes multiples of 16 bytes.
