@@ -58,7 +58,8 @@ constexpr int kPassCtasPerSm = 3;
 template <typename K>
 constexpr size_t radix_smem() {
     return (size_t)RadixShape<K>::BLOCK * RadixShape<K>::ITEMS * sizeof(K) +
-           (size_t)(RadixShape<K>::BLOCK / 32) * kSubs * kBins * sizeof(uint32_t);
+           (size_t)(RadixShape<K>::BLOCK / 32) * kSubs * kBins * sizeof(uint32_t) +
+           (size_t)RadixShape<K>::BLOCK * RadixShape<K>::ITEMS * sizeof(uint16_t);
 }
 
 template <typename K>
@@ -166,6 +167,8 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K* const s_keys = reinterpret_cast<K*>(smem_raw);
     uint32_t* const s_wh = reinterpret_cast<uint32_t*>(smem_raw + (size_t)TILE * sizeof(K));
+    // each key's rank within its stream, at the key's tile position (kept out of registers)
+    uint16_t* const s_rank = reinterpret_cast<uint16_t*>(s_wh + TABLES * kBins);
     __shared__ uint64_t s_goff[kBins];
     __shared__ uint32_t s_loc[kBins];
     __shared__ uint64_t s_part64[kBins / 32];
@@ -218,8 +221,8 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     // stream's running count of its digit plus its lower peers, and the highest peer
     // advances the count. This keeps the ranking off the SM's narrow branch unit (where match-any
     // issues) and off the ALU (eight ballots per key cost more than the whole pass).
-    static_assert(ITEMS % 2 == 0 && 32 * STREAM_ITEMS <= 0xffff, "two 16-bit ranks per register");
-    uint32_t rk[ITEMS / 2];  // rank within the item's stream, two per register
+    static_assert(32 * STREAM_ITEMS <= 0xffff, "ranks fit 16 bits");
+
     const uint32_t lt = lanemask_lt();
     const uint32_t le = lt | (1u << lane);
 #pragma unroll
@@ -248,8 +251,7 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
             const int i = t * STREAM_ITEMS + j;
-            if (i % 2 == 0) rk[i / 2] = c[t];
-            else rk[i / 2] |= c[t] << 16;
+            s_rank[w0 + 32 * i] = (uint16_t)c[t];
         }
     }
     __syncthreads();
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     // 4a. keys in digit order in shared memory
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-        const uint32_t r = (i % 2 == 0) ? (rk[i / 2] & 0xffffu) : (rk[i / 2] >> 16);
+        const uint32_t r = s_rank[w0 + 32 * i];
         const uint32_t d = digit_of(k[i], shift);
         s_keys[s_loc[d] + wh[(i / STREAM_ITEMS) * kBins + d] + r] = k[i];
     }
