@@ -368,11 +368,18 @@ bool scan_copies_typed(Workspace& ws, bool exclusive, const void* h_in, const vo
     const T* in = static_cast<const T*>(d_in);
     T* out = static_cast<T*>(d_out);
     cudaStream_t s = ws.stream();
+    // On a failure part way, no copy may outlive the call: wait for both copy streams.
+    auto fail = [&]() {
+        cudaStreamSynchronize(ws.copy_up);
+        cudaStreamSynchronize(ws.copy_down);
+        cudaGetLastError();
+        return false;
+    };
     // the copy streams start after everything already queued on the workspace stream
     if (!cuda_ok(cudaEventRecord(ws.ev_copy[0], s), "copy event") ||
         !cuda_ok(cudaStreamWaitEvent(ws.copy_up, ws.ev_copy[0], 0), "copy wait") ||
         !cuda_ok(cudaStreamWaitEvent(ws.copy_down, ws.ev_copy[0], 0), "copy wait"))
-        return false;
+        return fail();
     uint64_t chunks = 0;
     for (uint64_t t0 = 0; t0 < tiles; t0 += kCopyChunkTiles, ++chunks) {
         const uint64_t t1 = t0 + kCopyChunkTiles < tiles ? t0 + kCopyChunkTiles : tiles;
@@ -383,25 +390,25 @@ bool scan_copies_typed(Workspace& ws, bool exclusive, const void* h_in, const vo
                                   bytes, true, ws.copy_up) ||
                 !cuda_ok(cudaEventRecord(ws.ev_copy[1], ws.copy_up), "copy event") ||
                 !cuda_ok(cudaStreamWaitEvent(s, ws.ev_copy[1], 0), "copy wait"))
-                return false;
+                return fail();
         }
         const bool ok =
             exclusive ? launch_tiles_single<T, true, true>(in, out, n, init, ts, t1 - t0, s, t0)
                       : launch_tiles_single<T, false, true>(in, out, n, init, ts, t1 - t0, s, t0);
-        if (!ok) return false;
+        if (!ok) return fail();
         if (h_out) {
             if (!cuda_ok(cudaEventRecord(ws.ev_copy[2], s), "copy event") ||
                 !cuda_ok(cudaStreamWaitEvent(ws.copy_down, ws.ev_copy[2], 0), "copy wait") ||
                 !arena_copy_async(static_cast<char*>(h_out) + off, out + e0, bytes, false,
                                   ws.copy_down))
-                return false;
+                return fail();
         }
     }
     count_launch((unsigned)chunks);
     // the workspace stream (what a synchronous call waits on) ends after the last download
     if (!cuda_ok(cudaEventRecord(ws.ev_copy[3], ws.copy_down), "copy event") ||
         !cuda_ok(cudaStreamWaitEvent(s, ws.ev_copy[3], 0), "copy wait"))
-        return false;
+        return fail();
     return cuda_ok(cudaGetLastError(), "k_scan launch");
 }
 
