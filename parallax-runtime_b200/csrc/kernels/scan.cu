@@ -70,7 +70,8 @@ __device__ __forceinline__ void scan_tile(T* buf, uint64_t* bars, uint32_t parit
                                           typename ScanTypes<T>::A* s_tot, uint64_t tile,
                                           typename ScanTypes<T>::A init,
                                           const TileStatus<typename ScanTypes<T>::A>& ts,
-                                          typename ScanTypes<T>::A* red, int* first) {
+                                          typename ScanTypes<T>::A* red, int* first,
+                                          T* sub_out = nullptr, uint32_t bulk = 0) {
     using L = typename ScanTypes<T>::L;
     using A = typename ScanTypes<T>::A;
     constexpr int V = ScanShape<T>::V;
@@ -143,9 +144,31 @@ __device__ __forceinline__ void scan_tile(T* buf, uint64_t* bars, uint32_t parit
             }
             row[v] = r;
         }
+        if constexpr (BULK) {
+            // with sub_out: each sub-tile's bulk store leaves as soon as the sub-tile is
+            // written, so its shared-memory read overlaps the next sub-tile's rescan
+            if (sub_out && s + 1 < kSub) {
+                fence_proxy_async_smem();
+                __syncthreads();
+                const uint32_t lo = (uint32_t)s * SUB, hi = bulk < lo + SUB ? bulk : lo + SUB;
+                if (tid == 0 && hi > lo) {
+                    bulk_store(sub_out + lo, buf + lo, (hi - lo) * (uint32_t)sizeof(T));
+                    bulk_commit();
+                }
+            }
+        }
     }
     if constexpr (BULK) fence_proxy_async_smem();
     __syncthreads();
+    if constexpr (BULK) {
+        if (sub_out) {
+            const uint32_t lo = (uint32_t)(kSub - 1) * SUB;
+            if (tid == 0 && bulk > lo) {
+                bulk_store(sub_out + lo, buf + lo, (bulk - lo) * (uint32_t)sizeof(T));
+                bulk_commit();
+            }
+        }
+    }
 }
 
 // One CTA per 112 KiB tile, in blockIdx order: unaligned operands (BULK = false) and the
@@ -173,13 +196,8 @@ k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan
     const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
     const uint32_t bulk = stage_tile<T, SUB, kSub, kBlock, BULK>(buf, bars, in, base, cnt);
     __syncthreads();
-    scan_tile<T, EXCL, BULK>(buf, bars, 0, s_tot, tile, init, ts, s_red, s_first);
-    if constexpr (BULK) {
-        if (tid == 0 && bulk) {
-            bulk_store(out + base, buf, bulk * (uint32_t)sizeof(T));
-            bulk_commit();
-        }
-    }
+    scan_tile<T, EXCL, BULK>(buf, bars, 0, s_tot, tile, init, ts, s_red, s_first,
+                             BULK ? out + base : nullptr, bulk);
     for (uint32_t e = bulk + tid; e < cnt; e += kBlock) out[base + e] = buf[e];
     if constexpr (BULK) {
         if (tid == 0 && bulk) bulk_wait_read_all();
