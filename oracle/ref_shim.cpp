@@ -3,55 +3,17 @@
 //
 // include/parallax/stdpar.hpp (parallax-runtime) offloads every algorithm through
 // parallax_kernel_lookup() and runs its ISO host loop when the lookup misses
-// (stdpar.hpp:46-394). This file supplies an ABI whose lookup always misses, so each
-// parallax::* call below executes exactly the reference's host fallback:
+// (stdpar.hpp:46-394). This file is linked with an ABI whose lookup always misses
+// (abi_stub.cpp), so each parallax::* call below executes exactly the reference's host
+// fallback:
 //   reduce stdpar.hpp:146-148, inclusive_scan :209-210, exclusive_scan :237-238,
 //   sort :178, copy_if :319-321, remove_if :343-345, partition :369-370, unique :392-393.
 // Built by oracle/Makefile against -I <reference>/include into oracle/_ref/.
 #include <parallax/stdpar.hpp>
 
 #include <stdint.h>
-#include <stdio.h>
-#include <stdlib.h>
 
-#define HID __attribute__((visibility("hidden")))
 #define RX extern "C" __attribute__((visibility("default")))
-
-// ---- stub ABI: every lookup misses -------------------------------------------------------
-extern "C" {
-HID parallax_kernel_t parallax_kernel_lookup(const char*) { return nullptr; }
-HID void parallax_kernel_register(const char*, const unsigned int*, size_t) {}
-HID int parallax_arena_contains(const void*) { return 0; }
-HID void* parallax_arena_alloc(size_t, size_t) { return nullptr; }
-HID void parallax_arena_free(void*) {}
-static void unreachable(const char* f) {
-    fprintf(stderr, "ref_shim: %s reached (lookups miss, so this is a bug)\n", f);
-    abort();
-}
-HID void parallax_kernel_launch(parallax_kernel_t, ...) { unreachable("launch"); }
-HID void parallax_kernel_launch_with_captures(parallax_kernel_t, void*, size_t, void*, size_t,
-                                              size_t) { unreachable("launch_with_captures"); }
-HID void parallax_kernel_launch_transform2(parallax_kernel_t, void*, void*, size_t, size_t,
-                                           size_t) { unreachable("transform2"); }
-HID void parallax_kernel_launch_transform2_captures(parallax_kernel_t, void*, void*, size_t,
-                                                    size_t, size_t, void*, size_t) {
-    unreachable("transform2_captures");
-}
-HID void parallax_reduce(parallax_kernel_t, void*, size_t, size_t, void*) { unreachable("reduce"); }
-HID void parallax_scan(parallax_kernel_t, parallax_kernel_t, void*, size_t, size_t) {
-    unreachable("scan");
-}
-HID void parallax_exclusive_scan(parallax_kernel_t, parallax_kernel_t, parallax_kernel_t, void*,
-                                 void*, size_t, size_t, const void*) {
-    unreachable("exclusive_scan");
-}
-HID void parallax_sort(parallax_kernel_t, void*, size_t, size_t) { unreachable("sort"); }
-HID size_t parallax_copy_if(parallax_kernel_t, parallax_kernel_t, parallax_kernel_t,
-                            parallax_kernel_t, void*, void*, size_t, size_t, int) {
-    unreachable("copy_if");
-    return 0;
-}
-}
 
 namespace {
 struct Mod3 { bool operator()(int32_t x) const { return x % 3 == 0; } };

@@ -395,14 +395,24 @@ PXB_EXPORT void parallax_sort(parallax_kernel_t kernel, void* data, size_t count
 
 // ---- compaction -------------------------------------------------------------------------------
 
+namespace {
+
+// A handle registered under a key of the named stdpar funnel (e.g. "device_partition").
+bool from_funnel(const Handle* h, const char* funnel) {
+    return h && h->name.find(funnel) != std::string::npos;
+}
+
+}  // namespace
+
 PXB_EXPORT size_t parallax_copy_if(parallax_kernel_t flags_kernel, parallax_kernel_t scan_kernel,
                                    parallax_kernel_t add_kernel, parallax_kernel_t scatter_kernel,
                                    void* input, void* output, size_t count, size_t elem_size,
                                    int elem_is_float) {
-    (void)elem_is_float;  // the element type is carried by the handle
+    (void)elem_is_float;  // the element type is carried by the handle (or elem_size)
     Handle* h = as_handle(flags_kernel);
     Workspace* ws = begin(h, "parallax_copy_if", elem_size,
-                          {Kind::COMPACT_FLAGS, Kind::UNIQUE_FLAGS, Kind::PARTITION_SCATTER});
+                          {Kind::COMPACT_FLAGS, Kind::UNIQUE_FLAGS, Kind::PARTITION_SCATTER,
+                           Kind::USER});
     if (!ws) return 0;
     Handle* sc = as_handle(scatter_kernel);
     if (!as_handle(scan_kernel) || !as_handle(add_kernel) || !sc) {
@@ -410,19 +420,50 @@ PXB_EXPORT size_t parallax_copy_if(parallax_kernel_t flags_kernel, parallax_kern
         return 0;
     }
     if (count == 0) return 0;
+    // A registered `:flags` image (a compiler-emitted predicate, reference
+    // src/kernel/kernel_launcher.cpp:1734-1738) writes one byte per element, nonzero = keep
+    // (for remove_if the compiler's flags kernel already flags the elements to keep); the
+    // built-in single-pass compaction then consumes those bytes in place of its own
+    // predicate. Partition is recognised by its scatter handle (built-in partition scatter,
+    // or any handle registered under a device_partition key), as in the reference, where
+    // the scatter kernel decides whether rejected elements are written
+    // (kernel_launcher.cpp:1778-1785).
+    const bool user = h->kind == Kind::USER;
     CompactMode mode = CompactMode::SELECT;
     Pred pred = h->pred;
     if (h->kind == Kind::UNIQUE_FLAGS) mode = CompactMode::UNIQUE;
-    else if (h->kind == Kind::PARTITION_SCATTER || sc->kind == Kind::PARTITION_SCATTER)
+    else if (h->kind == Kind::PARTITION_SCATTER || sc->kind == Kind::PARTITION_SCATTER ||
+             (user && (from_funnel(h, "device_partition") || from_funnel(sc, "device_partition"))))
         mode = CompactMode::PARTITION;
     if (h->kind == Kind::COMPACT_FLAGS && h->remove) pred.negate = true;
-    size_t es = dtype_size(h->dtype);
+    DType t = h->dtype;
+    if (user) {
+        // the elements are moved as raw 4- or 8-byte words
+        if (elem_size != 4 && elem_size != 8) {
+            set_error(PARALLAX_ERR_UNSUPPORTED,
+                      "parallax_copy_if: a registered flags kernel needs 4- or 8-byte elements "
+                      "(got %zu)", elem_size);
+            return 0;
+        }
+        t = elem_size == 4 ? DType::U32 : DType::U64;
+    }
+    size_t es = dtype_size(t);
     size_t bytes = count * es;
+    const bool chase = user;  // the image may read through stored arena pointers
+    if (chase && !arena_sync_coherent(*ws, true)) return 0;
     Operand oi, oo;
-    if (!resolve_operand(*ws, input, bytes, true, 0, &oi)) return 0;
+    if (!resolve_operand(*ws, input, bytes, !(chase && arena_contains(input)), 0, &oi)) return 0;
     if (!resolve_operand(*ws, output, bytes, false, 1, &oo)) return 0;
+    if (user) {
+        uint8_t* d_flags = static_cast<uint8_t*>(ws->temp(compact_flags_padding(count)));
+        if (!d_flags) return 0;
+        if (!launch_user(*ws, h, oi.dev, d_flags, count, es, 1, nullptr, 0)) return 0;
+        pred = Pred();
+        pred.kind = PredKind::FLAGS;
+        pred.flags = d_flags;
+    }
     uint64_t* d_count = reinterpret_cast<uint64_t*>(ws->d_slot->count);
-    if (!launch_compact(*ws, h->dtype, mode, pred, oi.dev, oo.dev, count, d_count)) return 0;
+    if (!launch_compact(*ws, t, mode, pred, oi.dev, oo.dev, count, d_count)) return 0;
     if (ws->async) return std::numeric_limits<size_t>::max();
     if (sync_stream(*ws) != PARALLAX_OK) return 0;
     size_t kept = ws->h_slot->count[0];

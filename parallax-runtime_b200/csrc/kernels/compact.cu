@@ -49,7 +49,8 @@ struct PredDev {
     PredKind kind;
     bool negate;
     T c, m, r;
-    FastMod32 fm;  // 32-bit element types: m as an invariant divisor
+    FastMod32 fm;           // 32-bit element types: m as an invariant divisor
+    const uint8_t* fl;      // FLAGS: one byte per element, written by a registered image
     __device__ __forceinline__ bool operator()(T x) const {
         bool v;
         switch (kind) {
@@ -68,11 +69,36 @@ struct PredDev {
         }
         return v != negate;
     }
-    // Flag bits of one row: the switch on the (CTA-uniform) kind is taken once per row.
+    // Flag bits of one row whose first element has global index gi: the switch on the
+    // (CTA-uniform) kind is taken once per row.
     template <int ITEMS>
-    __device__ __forceinline__ uint32_t flags(const T (&x)[ITEMS]) const {
+    __device__ __forceinline__ uint32_t flags(const T (&x)[ITEMS], uint64_t gi) const {
         uint32_t f = 0;
         switch (kind) {
+            case PredKind::FLAGS:
+                // rows start at multiples of ITEMS (28 or 14), so the row's flag bytes are
+                // 4-byte (or 2-byte) aligned; the array is padded past the last tile
+                if constexpr (ITEMS % 4 == 0) {
+                    const uint32_t* w = reinterpret_cast<const uint32_t*>(fl + gi);
+#pragma unroll
+                    for (int v = 0; v < ITEMS / 4; ++v) {
+                        const uint32_t b = __ldg(w + v);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            f |= (uint32_t)((((b >> (8 * k)) & 0xffu) != 0u) != negate) << (4 * v + k);
+                    }
+                } else {
+                    static_assert(ITEMS % 2 == 0, "rows of an even number of elements");
+                    const uint16_t* w = reinterpret_cast<const uint16_t*>(fl + gi);
+#pragma unroll
+                    for (int v = 0; v < ITEMS / 2; ++v) {
+                        const uint32_t b = __ldg(w + v);
+#pragma unroll
+                        for (int k = 0; k < 2; ++k)
+                            f |= (uint32_t)((((b >> (8 * k)) & 0xffu) != 0u) != negate) << (2 * v + k);
+                    }
+                }
+                break;
 #define PXB_ROW(KIND, EXPR)                                              \
             case PredKind::KIND:                                          \
                 _Pragma("unroll") for (int j = 0; j < ITEMS; ++j)          \
@@ -172,7 +198,7 @@ __device__ __forceinline__ void compact_tile(T* buf, uint64_t* bars, uint32_t pa
                 if (e0 + j < cnt && keep) f |= 1u << j;
             }
         } else {
-            f = pred.template flags<ITEMS>(x);
+            f = pred.template flags<ITEMS>(x, base + e0);
             if (e0 + ITEMS > cnt) f &= e0 >= cnt ? 0u : (1u << (cnt - e0)) - 1u;
         }
         fl[s] = f;
@@ -362,6 +388,7 @@ PredDev<T> make_pred(const Pred& p) {
     e.m = (T)p.mod_m;
     e.r = (T)p.mod_r;
     if (std::is_integral<T>::value && sizeof(T) == 4) e.fm = FastMod32::make((int64_t)e.m);
+    e.fl = p.flags;
     return e;
 }
 
@@ -406,10 +433,16 @@ bool compact_typed(Workspace& ws, CompactMode mode, const Pred& pr, const void* 
     char* scratch = ws.scratch(tiles);
     if (!scratch) return false;
     auto* nt = reinterpret_cast<unsigned long long*>(scratch + ScratchOff::num_true);
+    if (pr.kind == PredKind::FLAGS && (!pr.flags || reinterpret_cast<uintptr_t>(pr.flags) % 4)) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "compaction: flags array missing or unaligned");
+        return false;
+    }
     if (mode == CompactMode::PARTITION) {
         // count pass: k = |{i : pred(in[i])}| into device scratch
-        if (!launch_count_if(ws, dtype_of<T>(), pr, d_in, n, reinterpret_cast<uint64_t*>(nt)))
-            return false;
+        const bool ok = pr.kind == PredKind::FLAGS
+            ? launch_count_flags(ws, pr.flags, n, reinterpret_cast<uint64_t*>(nt))
+            : launch_count_if(ws, dtype_of<T>(), pr, d_in, n, reinterpret_cast<uint64_t*>(nt));
+        if (!ok) return false;
     }
     auto ts = tile_status_at<uint64_t>(scratch, ws.next_epoch(), &ws.d_slot->spin_error);
     const bool bulk = reinterpret_cast<uintptr_t>(d_in) % 16 == 0;
@@ -441,6 +474,12 @@ bool compact_typed(Workspace& ws, CompactMode mode, const Pred& pr, const void* 
 }
 
 }  // namespace
+
+size_t compact_flags_padding(size_t n) {
+    constexpr size_t kTile = Shape<uint32_t>::TILE;  // the largest tile, in elements
+    static_assert(Shape<uint32_t>::TILE % Shape<uint64_t>::TILE == 0, "tile sizes nest");
+    return (n + kTile - 1) / kTile * kTile + 16;
+}
 
 bool launch_compact(Workspace& ws, DType t, CompactMode mode, const Pred& p, const void* d_in,
                     void* d_out, size_t n, uint64_t* d_count) {

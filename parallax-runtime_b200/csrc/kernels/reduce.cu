@@ -290,6 +290,12 @@ bool reduce_typed(Workspace& ws, RedOp op, const void* d_in, uint64_t n, void* d
     return run<T, T, T>(ws, "k_reduce_min", d_in, n, XfValue<T, T>{}, OpMin{}, ident, out);
 }
 
+struct XfNonzeroByte {
+    __device__ __forceinline__ unsigned long long operator()(uint8_t x, uint64_t) const {
+        return x != 0 ? 1ull : 0ull;
+    }
+};
+
 template <typename T>
 bool count_typed(Workspace& ws, const Pred& p, const void* d_in, uint64_t n, uint64_t* d_out) {
     return run<T, unsigned long long, unsigned long long>(
@@ -425,6 +431,12 @@ bool launch_mismatch(Workspace& ws, DType t, const void* d_a, const void* d_b, s
     PXB_DISPATCH(t, mismatch_typed<T>(ws, d_a, d_b, n, d_index));
     set_error(PARALLAX_ERR_INVALID_ARGUMENT, "mismatch: unsupported element type");
     return false;
+}
+
+bool launch_count_flags(Workspace& ws, const uint8_t* d_flags, size_t n, uint64_t* d_count) {
+    return run<uint8_t, unsigned long long, unsigned long long>(
+        ws, "k_count_flags", d_flags, n, XfNonzeroByte{}, OpSum{}, 0ull,
+        reinterpret_cast<unsigned long long*>(d_count));
 }
 
 }  // namespace pxb

@@ -188,8 +188,31 @@ Handle* funnel_builtin(const std::string& key) {
         else return nullptr;
         return intern("funnel:unique:" + suffix + ":" + dt, proto);
     }
-    // copy_if / remove_if / partition / count_if / transform / invoke / transform_reduce
-    // carry a user functor: they need a registered sm_100a image.
+    // copy_if / remove_if / partition carry a user predicate: their `:flags` kernel must be
+    // a registered sm_100a image (parallax_copy_if runs it, then the built-in compaction).
+    // The other three keys of these funnels name generic kernels (scan of the flags, add,
+    // scatter) and resolve to built-in handles, so a compiler registers only `:flags`.
+    if (funnel == "copy_if" || funnel == "remove_if" || funnel == "partition") {
+        if (suffix == "scan") proto.kind = Kind::SCAN;
+        else if (suffix == "add") proto.kind = Kind::SCAN_ADD;
+        else if (suffix == "scatter")
+            proto.kind = funnel == "partition" ? Kind::PARTITION_SCATTER : Kind::COMPACT_SCATTER;
+        else return nullptr;
+        return intern("funnel:" + funnel + ":" + suffix + ":" + dt, proto);
+    }
+    // count_if / transform_reduce: the `:pred` / `:xform` transform is a registered image;
+    // the `:reduce` kernel is the built-in '+' reduce of the transform's result type (int
+    // for count_if, stdpar.hpp:271-293; U for transform_reduce, stdpar.hpp:245-267).
+    if ((funnel == "count_if" || funnel == "transform_reduce") && suffix == "reduce") {
+        const DType r = funnel == "count_if" ? DType::I32 : dtype_from_cxx(template_arg(key, "U"));
+        if (r == DType::INVALID) return nullptr;
+        proto.kind = Kind::REDUCE;
+        proto.op = RedOp::SUM;
+        proto.dtype = r;
+        return intern("funnel:" + funnel + ":reduce:" + std::to_string((int)r), proto);
+    }
+    // transform / invoke and the `:flags`, `:pred`, `:xform` kernels carry a user functor:
+    // they need a registered sm_100a image.
     return nullptr;
 }
 

@@ -210,7 +210,9 @@ enum class Kind : int {
     USER,              // sm_100a image loaded from a registered / loaded cubin
 };
 enum class RedOp : int { SUM = 0, MAX = 1, MIN = 2 };
-enum class PredKind : int { NONE = 0, GT, GE, LT, LE, EQ, NE, MOD, NONZERO, ODD_NONZERO };
+// FLAGS: the element is kept when its byte in a flags array (written by a registered
+// `:flags` image, one byte per element, nonzero = keep) is nonzero.
+enum class PredKind : int { NONE = 0, GT, GE, LT, LE, EQ, NE, MOD, NONZERO, ODD_NONZERO, FLAGS };
 struct Pred {
     PredKind kind = PredKind::NONE;
     bool negate = false;   // remove_if keeps elements for which the predicate is false
@@ -218,6 +220,7 @@ struct Pred {
     int64_t i = 0;         // operand for signed integer element types
     uint64_t u = 0;        // operand for unsigned integer element types
     int64_t mod_m = 1, mod_r = 0;
+    const uint8_t* flags = nullptr;  // FLAGS: device array of one byte per element
 };
 enum class MapOp : int { NONE = 0, SAXPY_GATHER_F32, AFFINE_F32, DOUBLE_PLUS_ONE_F32 };
 
@@ -254,6 +257,11 @@ bool launch_compact(Workspace& ws, DType t, CompactMode mode, const Pred& p, con
                     void* d_out, size_t n, uint64_t* d_count);
 bool launch_count_if(Workspace& ws, DType t, const Pred& p, const void* d_in, size_t n,
                      uint64_t* d_count);
+// Number of nonzero bytes of a flags array (partition with a registered `:flags` image).
+bool launch_count_flags(Workspace& ws, const uint8_t* d_flags, size_t n, uint64_t* d_count);
+// Elements a flags array written for launch_compact with PredKind::FLAGS must be padded to
+// (the compaction reads whole rows of flags; bytes past n are ignored).
+size_t compact_flags_padding(size_t n);
 bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n);
 // Smallest array launch_sort gives to the radix sort (by default; PARALLAX_SORT overrides).
 size_t sort_radix_min(DType t);

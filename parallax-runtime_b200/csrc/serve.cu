@@ -82,6 +82,14 @@ void finish(Request* r, int status) {
     r->cv.notify_one();
 }
 
+// Blocks until the request has been finished; returns its status.
+int wait_request(Request* r, uint64_t* done_ns) {
+    std::unique_lock<std::mutex> lk(r->m);
+    r->cv.wait(lk, [&] { return r->done; });
+    if (done_ns) *done_ns = r->done_ns;
+    return r->status;
+}
+
 bool same_kind(const Request& a, const Request& b) {
     return a.op == b.op && a.t == b.t && a.red == b.red && a.mode == b.mode &&
            a.exclusive == b.exclusive && a.init_bits == b.init_bits &&
@@ -147,13 +155,6 @@ class Server {
             ++stats.requests;
         }
         cv_sched.notify_one();
-    }
-
-    int wait(Request* r, uint64_t* done_ns) {
-        std::unique_lock<std::mutex> lk(r->m);
-        r->cv.wait(lk, [&] { return r->done; });
-        if (done_ns) *done_ns = r->done_ns;
-        return r->status;
     }
 
     void stop() {
@@ -486,21 +487,15 @@ PXB_EXPORT int parallax_serve_wait(uint64_t ticket, uint64_t* done_ns) {
         set_error(PARALLAX_ERR_INVALID_ARGUMENT, "parallax_serve_wait: null ticket");
         return PARALLAX_ERR_INVALID_ARGUMENT;
     }
+    // The request carries its own completion state, so waiting needs no server: a request
+    // submitted before parallax_serve_stop() has been finished by the time stop returns
+    // (stop drains the queue), and its status is returned here as usual.
     int st;
     if (r->n == 0) {  // finished at submission by this thread
         st = r->status;
         if (done_ns) *done_ns = r->done_ns;
     } else {
-        Server* s;
-        {
-            std::lock_guard<std::mutex> g(g_srv_mu);
-            s = g_srv;
-        }
-        if (!s) {
-            set_error(PARALLAX_ERR_SHUTDOWN, "parallax_serve_wait: the serving loop is not running");
-            return PARALLAX_ERR_SHUTDOWN;
-        }
-        st = s->wait(r, done_ns);
+        st = wait_request(r, done_ns);
     }
     delete r;
     if (st != PARALLAX_OK) set_error(st, "served request failed (status %d)", st);

@@ -15,6 +15,8 @@
 // waits end whatever CTAs happen to be resident.
 #pragma once
 
+#include <mutex>
+
 #include "common.cuh"
 #include "lookback.cuh"
 #include "tma.cuh"
@@ -86,13 +88,29 @@ __device__ __forceinline__ void wait_sub(uint64_t* bars, int s, volatile int32_t
     if constexpr (BULK) wait_bar(&bars[s], 0, err);
 }
 
-// Opts a kernel into `bytes` of dynamic shared memory (above the 48 KiB default). Host
-// side; each kernel instantiation has its own template instance, so this runs once each.
+// Opts a kernel into `bytes` of dynamic shared memory (above the 48 KiB default) on the
+// current device. Host side. The attribute belongs to each device's context, so the size
+// already set is remembered per device (per kernel instantiation) and the attribute is set
+// again on a device that has not seen it, or when a larger size is asked for. A failed
+// attempt is not remembered: the next call tries again. On failure the CUDA error stays
+// pending for the caller's cudaGetLastError().
+constexpr int kSmemOptInDevices = 64;
 template <auto Kernel>
 inline bool smem_opt_in(size_t bytes) {
-    static const bool ok = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)bytes) == cudaSuccess;
-    return ok;
+    static std::mutex mu;
+    static size_t set_bytes[kSmemOptInDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (dev < 0 || dev >= kSmemOptInDevices)  // not remembered: set on every call
+        return cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)bytes) == cudaSuccess;
+    std::lock_guard<std::mutex> g(mu);
+    if (set_bytes[dev] >= bytes) return true;
+    if (cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+        cudaSuccess)
+        return false;
+    set_bytes[dev] = bytes;
+    return true;
 }
 
 // Waits until the bulk stores issued by this thread have finished reading shared memory

@@ -1,0 +1,45 @@
+"""Compiles every test image source here (*.cu) into an sm_100a fatbin under _build/.
+
+Each image is one translation unit exporting parallax_entry (include/parallax/kernel_abi.h),
+compiled the way a compiler targeting this runtime would embed its kernels:
+    nvcc -fatbin -gencode arch=compute_100a,code=sm_100a -I include -o _build/<name>.fatbin <name>.cu
+Rebuilt when the source, image_common.cuh or kernel_abi.h is newer than the fatbin.
+
+    python tests/images/build_images.py
+"""
+from __future__ import annotations
+
+import shutil
+import subprocess
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+OUT = HERE / "_build"
+
+
+def fatbin(name: str) -> Path:
+    return OUT / f"{name}.fatbin"
+
+
+def build() -> list[Path]:
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    OUT.mkdir(exist_ok=True)
+    deps = [HERE / "image_common.cuh", ROOT / "include" / "parallax" / "kernel_abi.h"]
+    newest_dep = max(d.stat().st_mtime for d in deps)
+    built = []
+    for src in sorted(HERE.glob("*.cu")):
+        out = fatbin(src.stem)
+        if (not out.exists() or out.stat().st_mtime < max(src.stat().st_mtime, newest_dep)):
+            cmd = [nvcc, "-fatbin", "-gencode", "arch=compute_100a,code=sm_100a", "-O3",
+                   "-I", str(ROOT / "include"), "-o", str(out), str(src)]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")
+        built.append(out)
+    return built
+
+
+if __name__ == "__main__":
+    for p in build():
+        print(p)

@@ -90,6 +90,32 @@ def test_functor_funnels_miss_without_an_image(lib):
     assert not lib.parallax_kernel_lookup(None)
 
 
+@pytest.mark.parametrize("funnel,sig", [
+    ("copy_if", "std::size_t parallax::detail::device_copy_if(const T*, T*, std::size_t, Pred)"),
+    ("remove_if", "std::size_t parallax::detail::device_remove_if(T*, std::size_t, Pred)"),
+    ("partition", "std::size_t parallax::detail::device_partition(T*, std::size_t, Pred)"),
+])
+def test_compaction_funnels_need_only_a_flags_image(lib, funnel, sig):
+    """The scan / add / scatter kernels of a compaction funnel are generic and resolve to
+    built-ins; only the predicate's `:flags` kernel needs a registered image, and without
+    one it misses (so the funnel's `kf && ks && ka && kc` test sends it to the host)."""
+    base = f"{sig} [with T = int; Pred = P{funnel}; std::size_t = long unsigned int]"
+    for sfx in (":scan", ":add", ":scatter"):
+        assert lib.parallax_kernel_lookup((base + sfx).encode()), sfx
+    assert not lib.parallax_kernel_lookup((base + ":flags").encode())
+
+
+def test_count_if_and_transform_reduce_reduce_keys_resolve(lib):
+    cnt = ("long int parallax::detail::device_count_if(const T*, std::size_t, Pred) "
+           "[with T = float; Pred = G; std::size_t = long unsigned int]")
+    assert lib.parallax_kernel_lookup((cnt + ":reduce").encode())
+    assert not lib.parallax_kernel_lookup((cnt + ":pred").encode())
+    tr = ("U parallax::detail::device_transform_reduce(const T*, std::size_t, F) "
+          "[with T = float; U = double; F = Sq; std::size_t = long unsigned int]")
+    assert lib.parallax_kernel_lookup((tr + ":reduce").encode())
+    assert not lib.parallax_kernel_lookup((tr + ":xform").encode())
+
+
 def test_registered_spirv_for_fixed_funnel_still_resolves(lib):
     # A SPIR-V image cannot run here; a fixed primitive funnel key resolves to the
     # built-in sm_100a kernel, a functor funnel key misses (host fallback).

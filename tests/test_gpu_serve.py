@@ -259,3 +259,26 @@ def test_zz_stop_then_submit_is_refused(lib, px, dev):
     t = C.c_uint64()
     assert lib.parallax_serve_submit(C.byref(r), C.byref(t)) == px.ERR_SHUTDOWN
     lib.parallax_clear_error()
+
+
+def test_zz_wait_after_stop_returns_the_status(lib, px, ox, dev):
+    """A request submitted before parallax_serve_stop() is finished by stop; waiting on its
+    ticket afterwards returns its status and result (and frees it) instead of failing."""
+    cfg = px.ServeConfig()
+    assert lib.parallax_serve_start(C.byref(cfg)) == px.OK
+    x = make(ox, "i32", 70001, 91)
+    d = dev.put(x)
+    dev.torch.cuda.synchronize()
+    out = (C.c_ubyte * 8)()
+    r = px.Request()
+    r.kernel = px.builtin("reduce:sum:i32")
+    r.input = d.data_ptr()
+    r.count = x.size
+    r.result = C.cast(out, C.c_void_p)
+    t = C.c_uint64()
+    assert lib.parallax_serve_submit(C.byref(r), C.byref(t)) == px.OK
+    assert lib.parallax_serve_stop() == px.OK
+    done = C.c_uint64()
+    assert lib.parallax_serve_wait(t.value, C.byref(done)) == px.OK
+    assert done.value > 0
+    assert np.frombuffer(bytes(out), np.int32, 1)[0] == ox.reduce_sum(x)
