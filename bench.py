@@ -306,85 +306,210 @@ class ClockSampler:
 
 
 # ---- CPU baseline (the reference's own CPU path) ----------------------------------------------
-def cpu_baseline(x: dict, log2sample: int, sort_log2sample: int) -> dict:
-    import oracle
-    ref = oracle.ref()
-    kind = "reference" if ref is not None else "port"
-    ns, nss = 1 << log2sample, 1 << sort_log2sample
+def host_info() -> dict:
+    """Host threads this process may use, the CPU model, and the C++ library's view."""
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    model = None
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"threads": int(threads or 1), "cpu_model": model}
+
+
+class CpuPrim:
+    """One primitive of the CPU sample: `call(lo, hi, bufs)` runs the host code on elements
+    [lo, hi) of its input; in-place primitives get fresh copies (untimed) before each run."""
+
+    def __init__(self, name, src, nbytes, call, inplace=False, out=False):
+        self.name, self.src, self.nbytes, self.call = name, src, nbytes, call
+        self.inplace, self.out = inplace, out
+
+
+def cpu_prims(fns, x: dict, ns: int, nss: int, prefix: str) -> list[CpuPrim]:
+    """The step's primitives over the first ns elements of each array (nss of each sort),
+    calling `prefix`_* functions of the library `fns` (the reference's compiled host
+    fallbacks, or the std::execution::par versions)."""
+    def p(a):
+        return C.c_void_p(a.ctypes.data)
+
+    ct = {"f32": C.c_float, "f64": C.c_double, "i32": C.c_int32, "i64": C.c_int64}
+    prims = []
+    for t, s in (("f32", 4), ("f64", 8), ("i32", 4), ("i64", 8)):
+        a = np.ascontiguousarray(x[t][:ns])
+        f = getattr(fns, f"{prefix}_reduce_{t}")
+        f.restype = ct[t]
+        prims.append(CpuPrim(f"reduce_sum_{t}", a, ns * s,
+                             lambda lo, hi, b, a=a, f=f: f(p(a[lo:hi]), hi - lo)))
+        fi = getattr(fns, f"{prefix}_inclusive_scan_{t}")
+        prims.append(CpuPrim(f"inclusive_scan_{t}", a, 2 * ns * s,
+                             lambda lo, hi, b, a=a, fi=fi: fi(p(a[lo:hi]), p(b[lo:hi]), hi - lo),
+                             out=True))
+        fe = getattr(fns, f"{prefix}_exclusive_scan_{t}")
+        prims.append(CpuPrim(f"exclusive_scan_{t}", a, 2 * ns * s,
+                             lambda lo, hi, b, a=a, fe=fe, c=ct[t]:
+                             fe(p(a[lo:hi]), p(b[lo:hi]), hi - lo, c(0)), out=True))
+    for t, key in (("u32", "sort_u32"), ("f32", "sort_f32")):
+        f = getattr(fns, f"{prefix}_sort_{t}")
+        prims.append(CpuPrim(f"sort_{t}", np.ascontiguousarray(x[key][:nss]), 2 * nss * 4,
+                             lambda lo, hi, b, f=f: f(p(b[lo:hi]), hi - lo), inplace=True))
+    f = getattr(fns, f"{prefix}_partition_neg_i32")
+    prims.append(CpuPrim("partition_i32", np.ascontiguousarray(x["part_i32"][:ns]), 2 * ns * 4,
+                         lambda lo, hi, b, f=f: f(p(b[lo:hi]), hi - lo), inplace=True))
+    a = np.ascontiguousarray(x["uniq_i32"][:ns])
+    f = getattr(fns, f"{prefix}_unique_i32")
+    f.restype = C.c_size_t
+    k_u = int(np.count_nonzero(np.diff(a)) + 1)
+    prims.append(CpuPrim("unique_i32", a, (ns + k_u) * 4,
+                         lambda lo, hi, b, f=f: f(p(b[lo:hi]), hi - lo), inplace=True))
+    a = np.ascontiguousarray(x["i32"][:ns])
+    f = getattr(fns, f"{prefix}_copy_if_mod3_i32")
+    k_c = int(np.count_nonzero(a % 3 == 0))
+    prims.append(CpuPrim("copy_if_i32", a, (ns + k_c) * 4,
+                         lambda lo, hi, b, a=a, f=f: f(p(a[lo:hi]), p(b[lo:hi]), hi - lo),
+                         out=True))
+    return prims
+
+
+def cpu_time(prims: list[CpuPrim], threads: int, pool=None) -> dict:
+    """Runs every primitive once on `threads` host threads at the same time, each on its own
+    contiguous slice (the calls release the GIL), and returns aggregate GB/s; one thread
+    runs the whole sample."""
+    total_bytes, total_s, parts = 0, 0.0, {}
+    for pr in prims:
+        n = pr.src.size
+        cuts = [n * i // threads for i in range(threads + 1)]
+        bufs = pr.src.copy() if pr.inplace else (np.empty_like(pr.src) if pr.out else None)
+        t0 = time.perf_counter()
+        if threads == 1:
+            pr.call(0, n, bufs)
+        else:
+            list(pool.map(lambda i: pr.call(cuts[i], cuts[i + 1], bufs), range(threads)))
+        dt = time.perf_counter() - t0
+        total_bytes += pr.nbytes
+        total_s += dt
+        parts[pr.name] = round(pr.nbytes / dt / 1e9, 3)
+    return {"value": round(total_bytes / total_s / 1e9, 3), "seconds": round(total_s, 3),
+            "per_primitive_gbs": parts}
+
+
+def cpu_c1(ref) -> dict:
+    """The reference's own CPU configuration, 2^20 elements (seed 0): reduce sum and
+    inclusive_scan of fp32 U[0,1) and int32 U[-1000,1000], sort of uint32 keys over the full
+    range, copy_if of int32 with x % 3 == 0, through its host fallbacks on one thread (best
+    of 5 after a warm-up)."""
+    n = 1 << 20
 
     def p(a):
         return C.c_void_p(a.ctypes.data)
 
-    total_bytes, total_s = 0, 0.0
-    parts = {}
+    f32, i32, u32 = gen("f32_unit", 0, n), gen("i32_pm1000", 0, n), gen("u32_full", 0, n)
+    ref.ref_reduce_f32.restype = C.c_float
+    ref.ref_reduce_i32.restype = C.c_int32
+    out32 = np.empty(n, np.float32)
+    outi = np.empty(n, np.int32)
+    k_c = int(np.count_nonzero(i32 % 3 == 0))
+    cases = {
+        "reduce_sum_f32": (n * 4, lambda: ref.ref_reduce_f32(p(f32), n), None),
+        "reduce_sum_i32": (n * 4, lambda: ref.ref_reduce_i32(p(i32), n), None),
+        "inclusive_scan_f32": (2 * n * 4, lambda: ref.ref_inclusive_scan_f32(p(f32), p(out32), n), None),
+        "inclusive_scan_i32": (2 * n * 4, lambda: ref.ref_inclusive_scan_i32(p(i32), p(outi), n), None),
+        "sort_u32": (2 * n * 4, None, u32),
+        "copy_if_i32": ((n + k_c) * 4, lambda: ref.ref_copy_if_mod3_i32(p(i32), p(outi), n), None),
+    }
+    res = {}
+    for name, (nbytes, fn, sort_src) in cases.items():
+        best = float("inf")
+        for _ in range(6):
+            if sort_src is not None:
+                a = sort_src.copy()
+                fn = (lambda a=a: ref.ref_sort_u32(p(a), n))
+            t0 = time.perf_counter()
+            fn()
+            best = min(best, time.perf_counter() - t0)
+        res[name] = {"ms": round(best * 1e3, 3), "GB_s": round(nbytes / best / 1e9, 3)}
+    return {"elements": n, "seed": 0, "threads": 1, "per_primitive": res}
 
-    def timed(name, nbytes, fn):
-        nonlocal total_bytes, total_s
-        t0 = time.perf_counter()
-        fn()
-        dt = time.perf_counter() - t0
-        total_bytes += nbytes
-        total_s += dt
-        parts[name] = round(nbytes / dt / 1e9, 3)
 
-    if ref is not None:
-        for t, s in (("f32", 4), ("f64", 8), ("i32", 4), ("i64", 8)):
-            a = np.ascontiguousarray(x[t][:ns])
-            out = np.empty_like(a)
-            getattr(ref, f"ref_reduce_{t}").restype = {"f32": C.c_float, "f64": C.c_double,
-                                                        "i32": C.c_int32, "i64": C.c_int64}[t]
-            # (the reference's reduce funnel has no custom-op path, so only '+' is timed)
-            timed(f"reduce_sum_{t}", ns * s, lambda a=a, t=t: getattr(ref, f"ref_reduce_{t}")(p(a), ns))
-            timed(f"inclusive_scan_{t}", 2 * ns * s,
-                  lambda a=a, out=out, t=t: getattr(ref, f"ref_inclusive_scan_{t}")(p(a), p(out), ns))
-            ct = {"f32": C.c_float, "f64": C.c_double, "i32": C.c_int32, "i64": C.c_int64}[t]
-            timed(f"exclusive_scan_{t}", 2 * ns * s,
-                  lambda a=a, out=out, t=t, ct=ct: getattr(ref, f"ref_exclusive_scan_{t}")(p(a), p(out), ns, ct(0)))
-        for t, key in (("u32", "sort_u32"), ("f32", "sort_f32")):
-            a = np.ascontiguousarray(x[key][:nss]).copy()
-            timed(f"sort_{t}", 2 * nss * 4, lambda a=a, t=t: getattr(ref, f"ref_sort_{t}")(p(a), nss))
-        a = np.ascontiguousarray(x["part_i32"][:ns]).copy()
-        timed("partition_i32", 2 * ns * 4, lambda a=a: ref.ref_partition_neg_i32(p(a), ns))
-        a = np.ascontiguousarray(x["uniq_i32"][:ns]).copy()
-        ref.ref_unique_i32.restype = C.c_size_t
-        k_u = int(np.count_nonzero(np.diff(a)) + 1)
-        timed("unique_i32", (ns + k_u) * 4, lambda a=a: ref.ref_unique_i32(p(a), ns))
+def cpu_baseline(x: dict, log2sample: int, sort_log2sample: int, full: bool = True,
+                 pool=None, threads: int | None = None) -> dict:
+    """The reference's own CPU path (its stdpar.hpp host fallbacks, compiled unmodified into
+    oracle/_ref) on a bounded sample of the step: `value` with every host thread busy
+    (disjoint slices of the sample, one concurrent fallback call per thread); with `full`
+    also the fallback on one thread, the primitives under std::execution::par, and the
+    reference's own 2^20 configuration."""
+    import concurrent.futures as cf
+    import oracle
+    ref = oracle.ref()
+    info = host_info()
+    threads = threads or info["threads"]
+    ns, nss = 1 << log2sample, 1 << sort_log2sample
+    if ref is None:  # the oracle port: single-threaded restatement
         a = np.ascontiguousarray(x["i32"][:ns])
-        out = np.empty_like(a)
-        k_c = int(np.count_nonzero(a % 3 == 0))
-        timed("copy_if_i32", (ns + k_c) * 4, lambda a=a, out=out: ref.ref_copy_if_mod3_i32(p(a), p(out), ns))
-    else:
-        for t, s in (("f32", 4), ("i32", 4)):
-            a = np.ascontiguousarray(x[t][:ns])
-            timed(f"reduce_sum_{t}", ns * s, lambda a=a: oracle.reduce_sum(a))
-            timed(f"inclusive_scan_{t}", 2 * ns * s, lambda a=a: oracle.scan(a))
-        a = np.ascontiguousarray(x["sort_u32"][:nss])
-        timed("sort_u32", 2 * nss * 4, lambda a=a: oracle.sort(a))
-    return {"value": round(total_bytes / total_s / 1e9, 3), "unit": "GB/s", "cores": 1,
-            "kind": kind, "seconds": round(total_s, 3),
-            "sample": (f"first 2^{log2sample} elements of each array primitive and 2^{sort_log2sample} "
-                       f"of each sort, single-threaded host fallbacks of stdpar.hpp "
-                       f"(std::execution::par has no parallel backend without TBB)"),
-            "per_primitive_gbs": parts}
+        t0 = time.perf_counter()
+        oracle.reduce_sum(a)
+        oracle.scan(a)
+        dt = time.perf_counter() - t0
+        return {"value": round(3 * ns * 4 / dt / 1e9, 3), "unit": "GB/s", "cores": 1,
+                "kind": "port", "sample": f"reduce + inclusive scan of 2^{log2sample} int32"}
+    own_pool = pool is None and threads > 1
+    if own_pool:
+        pool = cf.ThreadPoolExecutor(threads)
+    try:
+        prims = cpu_prims(ref, x, ns, nss, "ref")
+        par = cpu_time(prims, threads, pool)
+        out = {"value": par["value"], "unit": "GB/s", "cores": threads, "kind": "reference",
+               "sample": (f"first 2^{log2sample} elements of each array primitive and "
+                          f"2^{sort_log2sample} of each sort; the reference's host fallbacks "
+                          f"(stdpar.hpp) on {threads} host threads at once, one contiguous slice "
+                          f"each (sorts, partition and unique on their slices independently)"),
+               "seconds": par["seconds"], "per_primitive_gbs": par["per_primitive_gbs"],
+               "cpu_model": info["cpu_model"]}
+        if full:
+            one = cpu_time(prims, 1)
+            out["single_thread"] = {"value": one["value"], "cores": 1,
+                                    "per_primitive_gbs": one["per_primitive_gbs"]}
+            lib = oracle.pstl()
+            if lib is not None:
+                pst = cpu_time(cpu_prims(lib, x, ns, nss, "pstl"), 1)
+                out["std_execution_par"] = {
+                    "value": pst["value"], "backend": lib.pstl_backend().decode(),
+                    "hardware_concurrency": int(lib.pstl_threads()),
+                    "per_primitive_gbs": pst["per_primitive_gbs"]}
+            out["c1"] = cpu_c1(ref)
+        return out
+    finally:
+        if own_pool:
+            pool.shutdown()
 
 
 # ---- main --------------------------------------------------------------------------------------------
 def run_reference_arm(args, rank: int) -> None:
+    """The reference's own CPU path on every host thread, one step = one pass over the
+    bounded sample; the single-thread, std::execution::par and 2^20 figures once after."""
     if rank != 0:
         return
+    import concurrent.futures as cf
     import oracle
     oracle.ox()
     log2 = min(args.log2n, args.ref_log2)
-    x = make_inputs(log2, min(args.log2sort, args.ref_log2 - 2))
+    log2s = min(args.log2sort, args.ref_log2 - 2)
+    x = make_inputs(log2, log2s)
+    threads = host_info()["threads"]
+    pool = cf.ThreadPoolExecutor(threads) if threads > 1 else None
     for _ in range(args.warmup):
-        cpu_baseline(x, log2, min(args.log2sort, args.ref_log2 - 2))
+        cpu_baseline(x, log2, log2s, full=False, pool=pool)
     vals = []
     t0 = time.perf_counter()
-    last = None
     for _ in range(args.steps):
-        last = cpu_baseline(x, log2, min(args.log2sort, args.ref_log2 - 2))
-        vals.append(last["value"])
+        vals.append(cpu_baseline(x, log2, log2s, full=False, pool=pool)["value"])
     wall = time.perf_counter() - t0
+    last = cpu_baseline(x, log2, log2s, full=True, pool=pool)
+    if pool:
+        pool.shutdown()
     value = statistics.median(vals)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s",
@@ -393,7 +518,7 @@ def run_reference_arm(args, rank: int) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32,f64,i32,i64,u32",
         "data": "synthetic (seeded splitmix64; the large single-array configuration's distributions)",
         "config": config_dict(args, sample_log2=log2),
-        "cpu_baseline": {k: last[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "cpu_baseline": dict(last, value=value),
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

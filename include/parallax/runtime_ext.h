@@ -91,15 +91,24 @@ size_t parallax_last_count(void);
 /* No counterpart in the reference. `offsets` holds num_segments + 1 element offsets
  * (offsets[0] = 0, offsets[num_segments] = count) cutting `data` into segments; all
  * operands are DEVICE pointers (or PARALLAX_DEVICE_RESIDENT arena blocks). Each call is
- * one persistent launch over a tile work list (plus a one-CTA planner), tile shape
- * chosen by an autotuner on first use, captured as a CUDA graph per argument set and
- * replayed afterwards. Return a parallax_status; synchronous unless async mode is on.
- *   reduce: results[s] = sum of segment s (0 for an empty segment); reduce:sum handle.
+ * one persistent launch over a tile work list (plus a one-CTA planner; partition adds a
+ * count pass), tile shape (threads x vectors per thread) chosen by an autotuner on first
+ * use, captured as a CUDA graph per argument set and replayed afterwards. Each returns a
+ * parallax_status; synchronous unless async mode is on. Per segment, the result is the
+ * plain primitive's result for that segment alone.
+ *   reduce: results[s] = sum, max or min of segment s (0 for an empty segment);
+ *     reduce:<sum|max|min> handle.
  *   exclusive_scan: per segment, output[i] = init + sum of the segment's earlier
- *     elements; scan handle.
+ *     elements; inclusive_scan: output[i] = sum of the segment's elements up to i; scan
+ *     handle.
  *   copy_if: the kept elements of segment s are written, in order, to
- *     output[offsets[s] ...]; counts[s] = how many; copy_if / remove_if handle with a
- *     comparison predicate.
+ *     output[offsets[s] ...]; counts[s] = how many; copy_if / remove_if handle (any
+ *     predicate, x % m == r included).
+ *   partition: segment s of output holds the elements of segment s that satisfy the
+ *     predicate, in order, then the others, in order (stable); counts[s] = how many
+ *     satisfy it; partition handle.
+ *   unique: the first element of every run of equal elements of segment s is written, in
+ *     order, to output[offsets[s] ...]; counts[s] = how many; unique handle.
  *   sort: each segment sorted ascending in place (sort:<dtype> handle), or 8-byte
  *     (key << 32 | value) records sorted stably by key (sort_kv:u32 handle). */
 int parallax_segmented_reduce(parallax_kernel_t kernel, const void* data, size_t count,
@@ -107,9 +116,18 @@ int parallax_segmented_reduce(parallax_kernel_t kernel, const void* data, size_t
 int parallax_segmented_exclusive_scan(parallax_kernel_t kernel, const void* input,
                                       void* output, size_t count, const uint64_t* offsets,
                                       size_t num_segments, const void* init);
+int parallax_segmented_inclusive_scan(parallax_kernel_t kernel, const void* input,
+                                      void* output, size_t count, const uint64_t* offsets,
+                                      size_t num_segments);
 int parallax_segmented_copy_if(parallax_kernel_t kernel, const void* input, void* output,
                                size_t count, const uint64_t* offsets, size_t num_segments,
                                uint64_t* counts);
+int parallax_segmented_partition(parallax_kernel_t kernel, const void* input, void* output,
+                                 size_t count, const uint64_t* offsets, size_t num_segments,
+                                 uint64_t* counts);
+int parallax_segmented_unique(parallax_kernel_t kernel, const void* input, void* output,
+                              size_t count, const uint64_t* offsets, size_t num_segments,
+                              uint64_t* counts);
 int parallax_segmented_sort(parallax_kernel_t kernel, void* data, size_t count,
                             const uint64_t* offsets, size_t num_segments);
 
@@ -123,7 +141,7 @@ int parallax_segmented_sort(parallax_kernel_t kernel, void* data, size_t count,
  * (NULL = the legacy default stream); returns when the result is ready, with a
  * parallax_status.
  * The runtime allocates nothing for it: the look-back status lives in one static device
- * array of 576.25 KiB that every GPU loading this library holds until the process exits.
+ * array of 384.25 KiB that every GPU loading this library holds until the process exits.
  * That caps count at 24576 tiles: 704,643,072 elements of a 4-byte type, 352,321,536 of
  * an 8-byte type; larger counts return PARALLAX_ERR_INVALID_ARGUMENT and touch nothing.
  * The first call on a device looks up that array's device address (once per device, with
@@ -185,6 +203,18 @@ int parallax_serve_call(const parallax_request* req);
 int parallax_serve_get_stats(parallax_serve_stats* out);
 /* CLOCK_MONOTONIC in nanoseconds (the clock of parallax_serve_wait's done_ns). */
 uint64_t parallax_clock_ns(void);
+
+/* ---- bounded in-kernel waits ------------------------------------------------------ */
+/* Every in-kernel wait (look-back on a predecessor tile, a bulk copy's arrival) gives up
+ * after a bounded number of polls, records a code the host reads, and lets the kernel
+ * return: the call then fails with PARALLAX_ERR_DEVICE_SPIN and the CUDA context stays
+ * usable. PARALLAX_WAIT_LIMIT=<polls> (read once per process) lowers the look-back limit
+ * from its default of 4,194,304 polls. No counterpart in the reference, whose fence waits
+ * have no limit (src/kernel/kernel_launcher.cpp:438-443).
+ * parallax_check_bounded_wait runs one look-back whose predecessor never publishes, with
+ * its wait limited to `polls` (1 .. 4,194,304) polls, and returns what the host read:
+ * PARALLAX_ERR_DEVICE_SPIN when the wait gave up and the kernel returned as designed. */
+int parallax_check_bounded_wait(uint32_t polls);
 
 /* ---- instrumentation ------------------------------------------------------------- */
 /* Number of runtime kernel launches issued by this process so far. */

@@ -2,7 +2,8 @@
 
 Loads oracle/liboracle.so (the CPU restatement in oracle.cpp) and, when present,
 oracle/_ref/libparallax_ref.so (the reference's own stdpar.hpp host fallbacks, built by
-oracle/Makefile from the reference tree). Only tests, __graft_entry__.smoke() and
+oracle/Makefile from the reference tree) and oracle/libpstl_baseline.so (the primitives
+under std::execution::par, a timed baseline). Only tests, __graft_entry__.smoke() and
 bench.py's CPU-baseline leg use this module, and only as the checker or the timed CPU
 baseline; the runtime never calls it.
 """
@@ -41,6 +42,20 @@ def ox() -> C.CDLL:
             build()
         _ox = C.CDLL(str(ORACLE_SO))
     return _ox
+
+
+PSTL_SO = HERE / "libpstl_baseline.so"
+_pstl = None
+
+
+def pstl() -> C.CDLL | None:
+    """The primitives under std::execution::par (host C++ library), or None when not built."""
+    global _pstl
+    if _pstl is None and PSTL_SO.exists():
+        _pstl = C.CDLL(str(PSTL_SO))
+        _pstl.pstl_backend.restype = C.c_char_p
+        _pstl.pstl_threads.restype = C.c_uint
+    return _pstl
 
 
 def ref() -> C.CDLL | None:

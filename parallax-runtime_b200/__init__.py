@@ -110,9 +110,13 @@ _SIGNATURES = {
     "parallax_profile_json": (sz, [C.c_char_p, sz]),
     "parallax_profile_reset": (None, []),
     "parallax_scan_noalloc": (C.c_int, [vp, vp, vp, sz, sz, vp, vp]),
+    "parallax_check_bounded_wait": (C.c_int, [C.c_uint32]),
     "parallax_segmented_reduce": (C.c_int, [vp, vp, sz, vp, sz, vp]),
     "parallax_segmented_exclusive_scan": (C.c_int, [vp, vp, vp, sz, vp, sz, vp]),
+    "parallax_segmented_inclusive_scan": (C.c_int, [vp, vp, vp, sz, vp, sz]),
     "parallax_segmented_copy_if": (C.c_int, [vp, vp, vp, sz, vp, sz, vp]),
+    "parallax_segmented_partition": (C.c_int, [vp, vp, vp, sz, vp, sz, vp]),
+    "parallax_segmented_unique": (C.c_int, [vp, vp, vp, sz, vp, sz, vp]),
     "parallax_segmented_sort": (C.c_int, [vp, vp, sz, vp, sz]),
     "parallax_device_info": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p, sz]),
     "parallax_serve_start": (C.c_int, [C.POINTER(ServeConfig)]),

@@ -17,6 +17,7 @@
 #include <thread>
 #include <vector>
 
+#include "lookback.cuh"
 #include "runtime.hpp"
 
 namespace pxb {
@@ -126,7 +127,7 @@ Workspace* new_workspace() {
 // Bytes of one look-back status entry (lookback.cuh): {u32 flag, u32 pad, u64 agg,
 // u64 inc} for every accumulator type, so flag words sit at the same addresses in every
 // launch.
-static constexpr size_t kStatusEntry = 24;
+static constexpr size_t kStatusEntry = sizeof(StatusEntry);
 
 char* Workspace::scratch(uint64_t tiles) {
     size_t bytes = kScratchSmall + tiles * kStatusEntry;
@@ -362,6 +363,15 @@ ProfScope::~ProfScope() {
     std::lock_guard<std::mutex> g(g_prof_mu);
     if (!g_prof) g_prof = new std::vector<ProfRecord>();
     g_prof->push_back({name_, bytes_, start_, stop});
+}
+
+uint32_t wait_limit() {
+    static const uint32_t v = [] {
+        const char* e = getenv("PARALLAX_WAIT_LIMIT");
+        const long long t = e ? atoll(e) : 0;
+        return t > 0 && t < (long long)kSpinLimit ? (uint32_t)t : kSpinLimit;
+    }();
+    return v;
 }
 
 static long sync_timeout_ms() {

@@ -469,7 +469,42 @@ bool launch_scan(Workspace& ws, DType t, bool exclusive, const void* d_in, void*
     return false;
 }
 
+// One scan tile launched as tile 1 of a fresh look-back epoch: tile 0 never publishes in
+// that epoch, so the tile's look-back wait can only end by giving up after `polls` polls.
+int check_bounded_wait(uint32_t polls) {
+    using T = int32_t;
+    using A = ScanTypes<T>::A;
+    constexpr uint64_t TILE = ScanShape<T>::TILE;
+    Workspace* ws = workspace();
+    if (!ws) {
+        set_error(PARALLAX_ERR_NO_DEVICE, "parallax_check_bounded_wait: no CUDA device");
+        return PARALLAX_ERR_NO_DEVICE;
+    }
+    char* scratch = ws->scratch(2);
+    T* buf = static_cast<T*>(ws->temp(2 * TILE * sizeof(T) * 2));
+    if (!scratch || !buf) return last_error();
+    cudaStream_t s = ws->stream();
+    if (!cuda_ok(cudaMemsetAsync(buf, 0, 2 * TILE * sizeof(T), s), "check_bounded_wait: input"))
+        return PARALLAX_ERR_CUDA;
+    auto ts = tile_status_at<A>(scratch, ws->next_epoch(), &ws->d_slot->spin_error);
+    ts.limit = polls;
+    if (!launch_tiles_single<T, false, true>(buf, buf + 2 * TILE, 2 * TILE, A(0), ts, 1, s, 1))
+        return last_error() ? last_error() : PARALLAX_ERR_CUDA;
+    count_launch();
+    return sync_stream(*ws);
+}
+
 }  // namespace pxb
+
+PXB_EXPORT int parallax_check_bounded_wait(uint32_t polls) {
+    pxb::set_ok();
+    if (polls == 0 || polls > pxb::kSpinLimit) {
+        pxb::set_error(PARALLAX_ERR_INVALID_ARGUMENT,
+                       "parallax_check_bounded_wait: polls must be in [1, %u]", pxb::kSpinLimit);
+        return PARALLAX_ERR_INVALID_ARGUMENT;
+    }
+    return pxb::check_bounded_wait(polls);
+}
 
 // ---- allocation-free scan -----------------------------------------------------------------
 // Some callers cannot allocate device memory at all: code that runs inside an allocation
@@ -477,7 +512,7 @@ bool launch_scan(Workspace& ws, DType t, bool exclusive, const void* d_in, void*
 // re-enter itself if the runtime allocated), or a process whose device memory has been
 // handed to its own pool. parallax_scan_noalloc gives them the single-pass scan with no
 // allocation by the runtime: the look-back status lives in the fixed static device array
-// below (576.25 KiB, held on every GPU that loads this library until the process exits),
+// below (384.25 KiB, held on every GPU that loads this library until the process exits),
 // the caller passes device buffers for input and output and a stream, and no workspace,
 // stream, event or pinned slot is created.
 namespace pxb {

@@ -1,32 +1,50 @@
 // Segmented primitives: thousands of uneven segments in ONE persistent launch.
 //
 // No reference counterpart (the reference dispatches one primitive call per array,
-// src/kernel/kernel_launcher.cpp); this is the batching path of the B200 design.
+// src/kernel/kernel_launcher.cpp); this is the batching path of the B200 design. Per
+// segment, each primitive computes exactly what the reference's primitive computes for one
+// array: reduce (sum / max / min), inclusive and exclusive scan, copy_if / remove_if,
+// stable partition, unique (kernel_launcher.cpp:819-1791).
 //
 // Segments are either CSR (`offsets`, device, num_segments + 1 entries, cut one input
-// array) or descriptors (one device-resident SegDesc per segment with its own addresses,
-// used by the serving loop to coalesce requests without moving their operands). A one-CTA
-// planner kernel turns the segment lengths into a tile work list (item_start[s] = first work
-// item of segment s; a segment of L elements has ceil(L / TILE) items) and writes the
-// results of empty segments; a second small kernel inverts it (item -> segment). The
-// persistent kernel's CTAs then claim work items from an atomic counter in order, look up
-// their segment, and process one tile each:
-//   reduce   tile sum -> per-item partial; the last tile of a segment to finish (per-
-//            segment ticket) folds the segment's partials in item order (deterministic)
-//   scan     tile scan + decoupled look-back that stops at the segment's first tile
-//            (exclusive with an init value, or inclusive)
-//   copy_if  flags + tile ranks + look-back on kept counts within the segment; kept
-//            elements of segment s land at the start of its output, its count in its slot
-// TILE = 256 threads x ITEMS; ITEMS (4, 8 or 16) is picked per (primitive, element type,
-// average segment length bucket) by timing the candidates on the first call (autotuner).
-// Every CSR launch sequence (planner + persistent kernel) is captured once per argument
-// set as a CUDA graph and replayed; the look-back epoch lives in device memory and is
-// advanced by the planner, so a replay never reads status words of an earlier replay.
+// array and the output array at the same offsets) or descriptors (one device-resident
+// SegDesc per segment with its own addresses, used by the serving loop to coalesce
+// requests without moving their operands). A one-CTA planner kernel turns the segment
+// lengths into a tile work list (item_start[s] = first work item of segment s; a segment of
+// L elements has ceil(L / tile) items) and writes the results of empty segments; the
+// persistent kernel's CTAs then claim work items from an atomic counter in order and
+// process one tile each. While a CTA works on a tile, the claim and the segment
+// description of its next item are already on their way (prefetched by thread 0), so the
+// dependent loads that locate a tile overlap the work of the previous one.
+//
+// A tile is staged in shared memory with 16-byte vector loads (striped: consecutive
+// threads read consecutive vectors), at the segment's own 16-byte phase: element e of the
+// tile sits at slot e + mis, mis = the start's misalignment in elements, so every vector
+// inside the tile is one aligned load and only the (at most two) ragged vectors at its ends
+// are read element by element. Each thread then owns a row of VPT consecutive vectors; VPT
+// is odd, so the 16-byte row reads of a warp hit every bank once. Tiles hold
+// BLOCK x VPT vectors minus one (room for the phase shift).
+//   reduce     per-tile sum (max, min, or predicate count) -> per-item partial; the last
+//              tile of a segment to finish (per-segment ticket) folds the partials in item
+//              order (deterministic)
+//   scan       row scans + warp shuffles + decoupled look-back that stops at the segment's
+//              first tile; results written back into the staged rows and stored with
+//              16-byte stores when the output has the input's phase
+//   select     predicate (or adjacent-difference for unique) flags, ranks by shuffle scans,
+//              look-back on kept counts within the segment, packed output
+//   partition  select's ranks for both runs: kept elements to the front of the segment's
+//              output, rejected ones after the segment's kept total (a count pass first)
+// The tile shape (BLOCK x VPT) is picked per (operation, element type, log2 of the mean
+// segment length) by timing the candidates on the first call (the autotuner); every CSR
+// launch sequence is captured once per argument set as a CUDA graph and replayed; the
+// look-back epoch lives in device memory and is advanced by the planner, so a replay never
+// reads status words of an earlier replay.
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include <limits>
 #include <map>
 #include <mutex>
 #include <string>
@@ -41,17 +59,30 @@
 namespace pxb {
 namespace {
 
-constexpr int kBlock = 256;
-constexpr int kCandidates[3] = {4, 8, 16};
+// Tile shapes the autotuner chooses from: (threads per CTA, 16-byte vectors per thread).
+struct TileShape {
+    int block, vpt;
+};
+constexpr TileShape kShapes[] = {{256, 3}, {256, 7}, {512, 7}};
+constexpr int kNumShapes = 3;
 
-constexpr int SEG_REDUCE = (int)SegKind::REDUCE;
-constexpr int SEG_SCAN = (int)SegKind::SCAN;
-constexpr int SEG_COPY_IF = (int)SegKind::COPY_IF;
+enum SegOp : int { SEG_REDUCE = 0, SEG_SCAN = 1, SEG_SELECT = 2, SEG_PARTITION = 3 };
+// reduce flavours
+enum SegRed : int { RED_SUM = 0, RED_MAX = 1, RED_MIN = 2, RED_COUNT = 3 };
+
+template <typename T, int BLOCK, int VPT>
+struct SegShape {
+    static constexpr int V = 16 / sizeof(T);
+    static constexpr int ITEMS = VPT * V;            // elements per thread row
+    static constexpr int SLOTS = BLOCK * ITEMS;      // staged slots
+    static constexpr int TILE = SLOTS - V;           // tile elements (room for the phase)
+    static constexpr size_t SMEM = SLOTS * sizeof(T);
+};
 
 // Device buffers of one segmented launch (the workspace's segment and status buffers).
 struct SegBuffers {
     uint32_t* item_start;  // num_segments + 1
-    uint32_t* item_seg;    // one per work item: its segment (k_seg_map)
+    uint32_t* item_seg;    // one per work item: its segment
     uint32_t* tickets;     // num_segments, zeroed by the planner
     uint64_t* partials;    // one per work item
     StatusEntry* status;   // one per work item (a buffer of its own)
@@ -59,36 +90,14 @@ struct SegBuffers {
     uint32_t* counters;    // [0] claim, [1] exit, [2] epoch, [3] error
 };
 
-// ---- tile loads ----------------------------------------------------------------------------------
-// Loads `len` (<= 256 * ITEMS) elements starting at `src` into shared memory, striped (coalesced),
-// padding with `pad`; afterwards thread t's row is sm[t*ITEMS, t*ITEMS + ITEMS).
-template <typename T, int ITEMS>
-__device__ __forceinline__ void load_tile(T* sm, const T* src, uint32_t len, T pad) {
-#pragma unroll
-    for (int k = 0; k < ITEMS; ++k) {
-        const uint32_t e = (uint32_t)k * kBlock + threadIdx.x;
-        sm[e] = e < len ? src[e] : pad;
-    }
-}
-
-template <typename T, typename A>
-__device__ __forceinline__ A block_sum(A v, A* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = warp_reduce(v, OpSum());
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    A t = A(0);
-#pragma unroll
-    for (int w = 0; w < kBlock / 32; ++w) t = t + red[w];
-    __syncthreads();
-    return t;
-}
-
+// Predicate of the segmented select / partition / count: comparisons, x % m == r on
+// integers (32-bit element types by the invariant-divisor remainder), nonzero.
 template <typename T>
 struct SegPred {
     PredKind kind;
     bool negate;
-    T c;
+    T c, m, r;
+    FastMod32 fm;
     __device__ __forceinline__ bool operator()(T x) const {
         bool v;
         switch (kind) {
@@ -99,6 +108,15 @@ struct SegPred {
             case PredKind::EQ: v = x == c; break;
             case PredKind::NE: v = x != c; break;
             case PredKind::NONZERO: v = x != T(0); break;
+            case PredKind::MOD:
+                if constexpr (std::is_integral<T>::value && sizeof(T) == 4) {
+                    v = fm.eq(x, r);
+                } else if constexpr (std::is_integral<T>::value) {
+                    v = (std::is_signed<T>::value && m == T(-1)) ? r == T(0) : x % m == r;
+                } else {
+                    v = false;
+                }
+                break;
             default: v = false; break;
         }
         return v != negate;
@@ -106,22 +124,167 @@ struct SegPred {
 };
 
 template <typename T> struct SegAcc { using type = typename SumAcc<T>::type; };
+// Type of a row's running sum in the scan: fp32 rows sum in fp32 (at most 28 terms), and
+// rows, warps and tiles are carried in fp64; integers wrap in their unsigned type.
+template <typename T> struct SegRow { using type = typename SumAcc<T>::type; };
+template <> struct SegRow<float> { using type = float; };
+
+// Per-launch parameters.
+template <typename T>
+struct SegArgs {
+    SegSrc src;
+    uint64_t S;
+    T init;            // exclusive scan init
+    bool inclusive;    // scan flavour
+    bool unique;       // select: adjacent-difference flags instead of the predicate
+    int red;           // reduce flavour (SegRed)
+    SegPred<T> pred;
+};
+
+// Claimed work item and where its tile lives; thread 0 fills it (prefetched one item
+// ahead), every thread reads it from shared memory.
+struct ItemInfo {
+    uint32_t item, seg, first_item, seg_items;
+    uint64_t len, in, out, aux;
+};
+
+__device__ __forceinline__ void load_item(ItemInfo& it, const SegSrc& src, const SegBuffers& b,
+                                          uint32_t total, uint32_t item) {
+    it.item = item;
+    if (item >= total) return;
+    const uint32_t seg = __ldg(&b.item_seg[item]);
+    it.seg = seg;
+    it.first_item = __ldg(&b.item_start[seg]);
+    it.seg_items = __ldg(&b.item_start[seg + 1]) - it.first_item;
+    it.len = src.len(seg);
+    it.in = src.in_addr(seg);
+    it.out = src.out_addr(seg);
+    it.aux = src.aux_addr(seg);
+}
+
+// Stages tile elements [begin, begin + len) of `in` so that slot e + mis holds element e
+// (mis = the misalignment of in + begin in elements); other slots get `pad`. Vectors
+// entirely inside the tile are single 16-byte loads; the ragged ones element by element.
+template <typename T, int BLOCK, int VPT>
+__device__ __forceinline__ void stage(T* sm, const T* in, uint64_t begin, uint32_t len,
+                                      uint32_t mis, T pad) {
+    using Sh = SegShape<T, BLOCK, VPT>;
+    constexpr int V = Sh::V;
+    const T* base = in + begin - mis;  // 16-byte aligned when in is element-aligned
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) {
+        const int j = k * BLOCK + threadIdx.x;
+        const int e0 = j * V - (int)mis;  // tile index of the vector's first slot
+        uint4 v;
+        if (e0 >= 0 && e0 + V <= (int)len) {
+            v = *reinterpret_cast<const uint4*>(base + j * V);
+        } else {
+            T* e = reinterpret_cast<T*>(&v);
+#pragma unroll
+            for (int q = 0; q < V; ++q) {
+                const int i = e0 + q;
+                e[q] = (i >= 0 && i < (int)len) ? base[j * V + q] : pad;
+            }
+        }
+        *reinterpret_cast<uint4*>(sm + j * V) = v;
+    }
+}
+
+// Writes slots [mis, mis + len) of sm to out[begin ...]: 16-byte stores when the output
+// start has the same phase as the staged tile, element stores otherwise.
+template <typename T, int BLOCK, int VPT>
+__device__ __forceinline__ void unstage(const T* sm, T* out, uint64_t begin, uint32_t len,
+                                        uint32_t mis) {
+    using Sh = SegShape<T, BLOCK, VPT>;
+    constexpr int V = Sh::V;
+    const uint32_t omis = (uint32_t)((reinterpret_cast<uintptr_t>(out + begin) % 16) / sizeof(T));
+    if (omis == mis && reinterpret_cast<uintptr_t>(out) % sizeof(T) == 0) {
+        T* base = out + begin - mis;
+#pragma unroll
+        for (int k = 0; k < VPT; ++k) {
+            const int j = k * BLOCK + threadIdx.x;
+            const int e0 = j * V - (int)mis;
+            if (e0 >= 0 && e0 + V <= (int)len) {
+                *reinterpret_cast<uint4*>(base + j * V) = *reinterpret_cast<const uint4*>(sm + j * V);
+            } else {
+#pragma unroll
+                for (int q = 0; q < V; ++q) {
+                    const int i = e0 + q;
+                    if (i >= 0 && i < (int)len) base[j * V + q] = sm[j * V + q];
+                }
+            }
+        }
+    } else {
+        for (uint32_t e = threadIdx.x; e < len; e += BLOCK) out[begin + e] = sm[e + mis];
+    }
+}
+
+template <int BLOCK, typename A, typename Op>
+__device__ __forceinline__ A block_fold(A v, A* red, Op op) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_reduce(v, op);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    A t = red[0];
+#pragma unroll
+    for (int w = 1; w < BLOCK / 32; ++w) t = op(t, red[w]);
+    __syncthreads();
+    return t;
+}
+
+template <typename T>
+__device__ __forceinline__ T red_identity(int red) {
+    if (red == RED_MAX)
+        return std::numeric_limits<T>::has_infinity ? -std::numeric_limits<T>::infinity()
+                                                    : std::numeric_limits<T>::lowest();
+    if (red == RED_MIN)
+        return std::numeric_limits<T>::has_infinity ? std::numeric_limits<T>::infinity()
+                                                    : std::numeric_limits<T>::max();
+    return T(0);
+}
+
+// Rank scan of a row's kept-flag count over the CTA: this row's kept elements start at
+// woff + tex within the tile; returns the tile's kept total.
+template <int BLOCK>
+__device__ __forceinline__ uint32_t tile_ranks(uint32_t cnt, uint32_t* wcnt, uint32_t* start) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t incl = warp_inclusive_scan(cnt, OpSum());
+    if (lane == 31) wcnt[warp] = incl;
+    __syncthreads();
+    uint32_t woff = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < BLOCK / 32; ++w) {
+        const uint32_t v = wcnt[w];
+        if (w < warp) woff += v;
+        tot += v;
+    }
+    *start = woff + incl - cnt;
+    return tot;
+}
 
 // ---- the persistent kernel -------------------------------------------------------------------------
-template <typename T, int ITEMS, int OP>
-__global__ void __launch_bounds__(kBlock)
-k_segmented(SegSrc src, uint64_t S, SegBuffers b, T init, bool inclusive, SegPred<T> pred,
-            volatile int32_t* err) {
+template <typename T, int BLOCK, int VPT, int OP>
+__global__ void __launch_bounds__(BLOCK)
+k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
+    using Sh = SegShape<T, BLOCK, VPT>;
     using A = typename SegAcc<T>::type;
-    constexpr int TILE = kBlock * ITEMS;
-    __shared__ __align__(16) T sm[TILE];
-    __shared__ A red[kBlock / 32 + 1];
-    __shared__ uint64_t red64[kBlock / 32 + 1];
-    __shared__ int first[kBlock / 32];
-    __shared__ uint32_t s_item;
-    __shared__ uint32_t s_seg;
+    constexpr int V = Sh::V;
+    constexpr int ITEMS = Sh::ITEMS;
+    constexpr int TILE = Sh::TILE;
+    constexpr int WARPS = BLOCK / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    __shared__ A red[WARPS + 1];
+    __shared__ uint64_t red64[WARPS + 1];
+    __shared__ T redT[WARPS + 1];
+    __shared__ int first[WARPS];
+    __shared__ uint32_t wcnt[WARPS];
+    __shared__ uint32_t wcnt2[WARPS];
+    __shared__ ItemInfo s_it;
+    __shared__ T s_prev;
+    __shared__ bool s_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t total = b.item_start[S];
+    const uint32_t total = b.item_start[a.S];
     TileStatus<A> ts;
     ts.e = b.status;
     ts.epoch = b.counters[2];
@@ -131,128 +294,210 @@ k_segmented(SegSrc src, uint64_t S, SegBuffers b, T init, bool inclusive, SegPre
     tsk.epoch = b.counters[2];
     tsk.err = err;
 
+    ItemInfo next;  // thread 0: the next item, claimed and described one tile ahead
+    if (tid == 0) load_item(next, a.src, b, total, atomicAdd(&b.counters[0], 1u));
     for (;;) {
         if (tid == 0) {
-            const uint32_t item = atomicAdd(&b.counters[0], 1u);
-            s_item = item;
-            s_seg = item < total ? b.item_seg[item] : 0u;
+            s_it = next;
+            if (next.item < total) load_item(next, a.src, b, total, atomicAdd(&b.counters[0], 1u));
         }
         __syncthreads();
-        const uint32_t item = s_item;
-        const uint32_t seg = s_seg;
-        __syncthreads();
-        if (item >= total) break;
-        const uint32_t first_item = b.item_start[seg];
-        const uint32_t seg_items = b.item_start[seg + 1] - first_item;
-        const uint32_t k = item - first_item;  // tile index within the segment
-        const uint64_t seg_len = src.len(seg);
-        const T* in = reinterpret_cast<const T*>(src.in_addr(seg));
-        T* out = reinterpret_cast<T*>(src.out_addr(seg));
-        const uint64_t begin = (uint64_t)k * TILE;  // within the segment
-        const uint32_t len = (uint32_t)min((uint64_t)TILE, seg_len - begin);
+        const ItemInfo it = s_it;
+        if (it.item >= total) break;
+        const uint32_t k = it.item - it.first_item;  // tile index within the segment
+        const uint64_t begin = (uint64_t)k * TILE;   // within the segment
+        const uint32_t len = (uint32_t)min((uint64_t)TILE, it.len - begin);
+        const T* in = reinterpret_cast<const T*>(it.in);
+        T* out = reinterpret_cast<T*>(it.out);
+        const uint32_t mis = (reinterpret_cast<uintptr_t>(in) % sizeof(T)) ? 0u
+            : (uint32_t)((reinterpret_cast<uintptr_t>(in + begin) % 16) / sizeof(T));
+        const bool vec_ok = reinterpret_cast<uintptr_t>(in) % sizeof(T) == 0;
 
         if constexpr (OP == SEG_REDUCE) {
+            // straight from global memory: each thread folds VPT vectors; sums and counts
+            // accumulate in A, max / min in T
+            const bool mm = a.red == RED_MAX || a.red == RED_MIN;
             A acc = A(0);
+            T accm = red_identity<T>(a.red);
+            const T* base = in + begin - mis;
 #pragma unroll
-            for (int j = 0; j < ITEMS; ++j) {
-                const uint32_t e = (uint32_t)j * kBlock + tid;
-                if (e < len) acc = acc + (A)in[begin + e];
+            for (int q = 0; q < VPT; ++q) {
+                const int j = q * BLOCK + tid;
+                const int e0 = j * V - (int)mis;
+                T x[V];
+                const bool full = vec_ok && e0 >= 0 && e0 + V <= (int)len;
+                if (full) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(base + j * V);
+                    memcpy(x, &v, 16);
+                }
+#pragma unroll
+                for (int e = 0; e < V; ++e) {
+                    const int i = e0 + e;
+                    const bool in_tile = i >= 0 && i < (int)len;
+                    if (!full && in_tile) x[e] = in[begin + i];
+                    if (full || in_tile) {
+                        if (a.red == RED_SUM) acc = acc + (A)x[e];
+                        else if (a.red == RED_COUNT) acc = acc + (A)(a.pred(x[e]) ? 1 : 0);
+                        else if (a.red == RED_MAX) accm = OpMax()(accm, x[e]);
+                        else accm = OpMin()(accm, x[e]);
+                    }
+                }
             }
-            const A sum = block_sum<T, A>(acc, red);
-            T* res = reinterpret_cast<T*>(src.aux_addr(seg));
-            if (seg_items == 1) {
-                if (tid == 0) *res = (T)sum;
+            const bool count = a.red == RED_COUNT;
+            A tot = A(0);
+            T totm = accm;
+            if (a.red == RED_MAX) totm = block_fold<BLOCK>(accm, redT, OpMax());
+            else if (a.red == RED_MIN) totm = block_fold<BLOCK>(accm, redT, OpMin());
+            else tot = block_fold<BLOCK>(acc, red, OpSum());
+            auto write = [&](A sum, T m) {
+                if (count) *reinterpret_cast<uint64_t*>(it.aux) = (uint64_t)sum;
+                else *reinterpret_cast<T*>(it.aux) = mm ? m : (T)sum;
+            };
+            if (it.seg_items == 1) {
+                if (tid == 0) write(tot, totm);
             } else {
-                __shared__ bool s_last;
                 if (tid == 0) {
-                    put_val(&b.partials[item], sum);
+                    if (mm) put_val(&b.partials[it.item], totm);
+                    else put_val(&b.partials[it.item], tot);
                     __threadfence();
-                    s_last = atomicAdd(&b.tickets[seg], 1u) == seg_items - 1;
+                    s_last = atomicAdd(&b.tickets[it.seg], 1u) == it.seg_items - 1;
                 }
                 __syncthreads();
                 if (s_last) {  // fold the segment's partials in item order
                     __threadfence();
                     A f = A(0);
-                    for (uint32_t i = tid; i < seg_items; i += kBlock)
-                        f = f + get_val<A>(&b.partials[first_item + i]);
-                    const A t = block_sum<T, A>(f, red);
-                    if (tid == 0) *res = (T)t;
+                    T fm = red_identity<T>(a.red);
+                    for (uint32_t i = tid; i < it.seg_items; i += BLOCK) {
+                        if (a.red == RED_MAX) fm = OpMax()(fm, get_val<T>(&b.partials[it.first_item + i]));
+                        else if (a.red == RED_MIN) fm = OpMin()(fm, get_val<T>(&b.partials[it.first_item + i]));
+                        else f = f + get_val<A>(&b.partials[it.first_item + i]);
+                    }
+                    if (a.red == RED_MAX) fm = block_fold<BLOCK>(fm, redT, OpMax());
+                    else if (a.red == RED_MIN) fm = block_fold<BLOCK>(fm, redT, OpMin());
+                    else f = block_fold<BLOCK>(f, red, OpSum());
+                    if (tid == 0) write(f, fm);
+                }
+            }
+            __syncthreads();
+        } else {
+            if (vec_ok) {
+                stage<T, BLOCK, VPT>(sm, in, begin, len, mis, T(0));
+            } else {  // element-misaligned pointer: element loads only
+                for (int s = tid; s < Sh::SLOTS; s += BLOCK) sm[s] = s < (int)len ? in[begin + s] : T(0);
+            }
+            if (OP == SEG_SELECT && a.unique && tid == 0)
+                s_prev = begin > 0 ? in[begin - 1] : T(0);
+            __syncthreads();
+            // this thread's row: slots [tid * ITEMS, +ITEMS) = tile indices from r0
+            const int r0 = tid * ITEMS - (int)mis;
+            T x[ITEMS];
+            {
+                const uint4* row = reinterpret_cast<const uint4*>(sm + tid * ITEMS);
+#pragma unroll
+                for (int v = 0; v < VPT; ++v) {
+                    const uint4 q = row[v];
+                    memcpy(&x[v * V], &q, 16);
+                }
+            }
+            if constexpr (OP == SEG_SCAN) {
+                using L = typename SegRow<T>::type;
+                L p[ITEMS];
+                p[0] = (L)x[0];
+#pragma unroll
+                for (int j = 1; j < ITEMS; ++j) p[j] = p[j - 1] + (L)x[j];
+                const A incl = warp_inclusive_scan((A)p[ITEMS - 1], OpSum());
+                A tex = shfl_up(incl, 1);
+                if (lane == 0) tex = A(0);
+                if (lane == 31) red[warp] = incl;
+                __syncthreads();
+                A woff = A(0), agg = A(0);
+#pragma unroll
+                for (int w = 0; w < WARPS; ++w) {
+                    if (w < warp) woff = woff + red[w];
+                    agg = agg + red[w];
+                }
+                __syncthreads();
+                const A prefix =
+                    lookback_cta<A, BLOCK>(ts, it.item, agg, red, first, it.first_item);
+                const A tb = (A)a.init + ((prefix + woff) + tex);
+                uint4* row = reinterpret_cast<uint4*>(sm + tid * ITEMS);
+#pragma unroll
+                for (int v = 0; v < VPT; ++v) {
+                    T o[V];
+#pragma unroll
+                    for (int q = 0; q < V; ++q) {
+                        const int j = v * V + q;
+                        o[q] = a.inclusive ? (T)(tb + (A)p[j]) : (T)(j == 0 ? tb : tb + (A)p[j - 1]);
+                    }
+                    uint4 w;
+                    memcpy(&w, o, 16);
+                    row[v] = w;
+                }
+                __syncthreads();
+                if (reinterpret_cast<uintptr_t>(out) % sizeof(T) == 0 && vec_ok)
+                    unstage<T, BLOCK, VPT>(sm, out, begin, len, mis);
+                else
+                    for (uint32_t e = tid; e < len; e += BLOCK) out[begin + e] = sm[e + mis];
+                __syncthreads();
+            } else {  // SEG_SELECT / SEG_PARTITION
+                uint32_t f = 0;
+#pragma unroll
+                for (int j = 0; j < ITEMS; ++j) {
+                    const int i = r0 + j;
+                    bool keep;
+                    if (OP == SEG_SELECT && a.unique) {
+                        const T prev = i == 0 ? s_prev : j > 0 ? x[j - 1] : sm[tid * ITEMS - 1];
+                        keep = (begin == 0 && i == 0) || !(x[j] == prev);
+                    } else {
+                        keep = a.pred(x[j]);
+                    }
+                    if (i >= 0 && i < (int)len && keep) f |= 1u << j;
+                }
+                uint32_t kstart;
+                const uint32_t kept = tile_ranks<BLOCK>(__popc(f), wcnt, &kstart);
+                const uint64_t prefix =
+                    lookback_cta<uint64_t, BLOCK>(tsk, it.item, (uint64_t)kept, red64, first,
+                                                  it.first_item);
+                if constexpr (OP == SEG_SELECT) {
+                    // pack the kept elements at the front of the staged tile, then store
+                    uint32_t r = kstart;
+#pragma unroll
+                    for (int j = 0; j < ITEMS; ++j)
+                        if (f >> j & 1u) sm[r++] = x[j];  // rows were read before the barriers
+                    __syncthreads();
+                    for (uint32_t i = tid; i < kept; i += BLOCK) {
+                        if (prefix + i < it.len) out[prefix + i] = sm[i];
+                        else *err = 3;
+                    }
+                    if (tid == 0 && k == it.seg_items - 1)
+                        *reinterpret_cast<uint64_t*>(it.aux) = prefix + kept;
+                } else {
+                    // rejected elements of this row follow the kept run of the tile
+                    uint32_t valid = 0;
+#pragma unroll
+                    for (int j = 0; j < ITEMS; ++j) valid += (r0 + j >= 0 && r0 + j < (int)len);
+                    uint32_t rstart;
+                    tile_ranks<BLOCK>(valid - __popc(f), wcnt2, &rstart);
+                    uint32_t rk = kstart, rr = kept + rstart;
+#pragma unroll
+                    for (int j = 0; j < ITEMS; ++j) {
+                        const int i = r0 + j;
+                        if (i < 0 || i >= (int)len) continue;
+                        if (f >> j & 1u) sm[rk++] = x[j];
+                        else sm[rr++] = x[j];
+                    }
+                    __syncthreads();
+                    // the segment's kept total, written by the count pass
+                    const uint64_t seg_true = *reinterpret_cast<const uint64_t*>(it.aux);
+                    const uint64_t rej_base = seg_true + (begin - prefix);
+                    for (uint32_t i = tid; i < len; i += BLOCK) {
+                        const uint64_t dst = i < kept ? prefix + i : rej_base + (i - kept);
+                        if (dst < it.len) out[dst] = sm[i];
+                        else *err = 3;
+                    }
                 }
                 __syncthreads();
             }
-        } else if constexpr (OP == SEG_SCAN) {
-            load_tile<T, ITEMS>(sm, in + begin, len, T(0));
-            __syncthreads();
-            A x[ITEMS];
-#pragma unroll
-            for (int j = 0; j < ITEMS; ++j) x[j] = (A)sm[tid * ITEMS + j];
-#pragma unroll
-            for (int j = 1; j < ITEMS; ++j) x[j] = x[j - 1] + x[j];
-            const A incl = warp_inclusive_scan(x[ITEMS - 1], OpSum());
-            A tex = shfl_up(incl, 1);
-            if (lane == 0) tex = A(0);
-            if (lane == 31) red[warp] = incl;
-            __syncthreads();
-            A woff = A(0), agg = A(0);
-#pragma unroll
-            for (int w = 0; w < kBlock / 32; ++w) {
-                if (w < warp) woff = woff + red[w];
-                agg = agg + red[w];
-            }
-            __syncthreads();
-            const A prefix = lookback_cta<A, kBlock>(ts, item, agg, red, first, first_item);
-            const A tb = (A)init + ((prefix + woff) + tex);
-            if (inclusive) {
-#pragma unroll
-                for (int j = 0; j < ITEMS; ++j) sm[tid * ITEMS + j] = (T)(tb + x[j]);
-            } else {
-#pragma unroll
-                for (int j = 0; j < ITEMS; ++j) sm[tid * ITEMS + j] = (T)(j == 0 ? tb : tb + x[j - 1]);
-            }
-            __syncthreads();
-#pragma unroll
-            for (int j = 0; j < ITEMS; ++j) {
-                const uint32_t e = (uint32_t)j * kBlock + tid;
-                if (e < len) out[begin + e] = sm[e];
-            }
-            __syncthreads();
-        } else {  // SEG_COPY_IF
-            load_tile<T, ITEMS>(sm, in + begin, len, T(0));
-            __syncthreads();
-            T x[ITEMS];
-            uint32_t f = 0;
-#pragma unroll
-            for (int j = 0; j < ITEMS; ++j) {
-                x[j] = sm[tid * ITEMS + j];
-                if ((uint32_t)(tid * ITEMS + j) < len && pred(x[j])) f |= 1u << j;
-            }
-            const uint32_t c = __popc(f);
-            const uint32_t incl = warp_inclusive_scan(c, OpSum());
-            uint32_t tex = shfl_up(incl, 1);
-            if (lane == 0) tex = 0;
-            __shared__ uint32_t wcnt[kBlock / 32];
-            if (lane == 31) wcnt[warp] = incl;
-            __syncthreads();
-            uint32_t woff = 0, kept = 0;
-#pragma unroll
-            for (int w = 0; w < kBlock / 32; ++w) {
-                if (w < warp) woff += wcnt[w];
-                kept += wcnt[w];
-            }
-            const uint64_t prefix =
-                lookback_cta<uint64_t, kBlock>(tsk, item, (uint64_t)kept, red64, first, first_item);
-            uint32_t r = woff + tex;
-#pragma unroll
-            for (int j = 0; j < ITEMS; ++j)
-                if (f >> j & 1u) sm[r++] = x[j];  // rows were read before the barriers above
-            __syncthreads();
-            for (uint32_t i = tid; i < kept; i += kBlock) {
-                if (prefix + i < seg_len) out[prefix + i] = sm[i];
-                else *err = 3;
-            }
-            if (tid == 0 && k == seg_items - 1)
-                *reinterpret_cast<uint64_t*>(src.aux_addr(seg)) = prefix + kept;
-            __syncthreads();
         }
     }
     if (tid == 0) persistent_exit(b.counters);
@@ -260,6 +505,11 @@ k_segmented(SegSrc src, uint64_t S, SegBuffers b, T init, bool inclusive, SegPre
 
 // ---- host side: buffers, tuner, graphs ------------------------------------------------------------
 size_t up256(size_t v) { return (v + 255) / 256 * 256; }
+
+template <typename T>
+constexpr int min_tile() {  // the smallest tile of any shape, in elements of T
+    return 256 * 3 * (16 / (int)sizeof(T)) - 16 / (int)sizeof(T);
+}
 
 // Carves the buffers for S segments and at most `items` work items out of the workspace's
 // segment buffer (zeroed when it is (re)allocated).
@@ -283,90 +533,121 @@ bool seg_buffers(Workspace& ws, uint64_t S, uint64_t items, SegBuffers* out) {
 }
 
 struct SegCall {
-    int op;            // SEG_REDUCE / SEG_SCAN / SEG_COPY_IF
+    int op;            // SegOp
+    int red;           // SegRed (reduce)
     DType t;
     SegSrc src;
     uint64_t S;
     uint64_t count;    // CSR: elements of the input array; descriptors: sum of lengths
     uint64_t init_bits;
     bool inclusive;
+    bool unique;
     bool tune;         // may time the tile candidates (launches must be idempotent)
     Pred pred;
 };
 
-template <typename T, int ITEMS>
-bool enqueue_typed(Workspace& ws, const SegCall& c, const SegBuffers& b) {
-    constexpr int TILE = kBlock * ITEMS;
-    cudaStream_t s = ws.stream();
-    volatile int32_t* err = &ws.d_slot->spin_error;
-    const uint64_t items_cap = c.S + c.count / TILE + 1;  // bound on the planner's items
-    const SegEmpty empty = c.op == SEG_REDUCE ? SegEmpty::ZERO_RESULT
-                         : c.op == SEG_COPY_IF ? SegEmpty::ZERO_COUNT : SegEmpty::NONE;
-    k_seg_plan<kBlock><<<1, kBlock, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE, b.item_start,
-                                            b.counters, empty,
-                                            c.op == SEG_REDUCE ? b.tickets : nullptr, b.status,
-                                            b.status_cap, err,
-                                            items_cap <= kInlineItems ? b.item_seg : nullptr);
-    if (items_cap > kInlineItems)
-        k_seg_map<256><<<seg_map_grid(c.S), 256, 0, s>>>(b.item_start, c.S, b.item_seg);
-    T init;
-    memcpy(&init, &c.init_bits, sizeof(T));
-    SegPred<T> pr;
-    pr.kind = c.pred.kind;
-    pr.negate = c.pred.negate;
-    pr.c = std::is_floating_point<T>::value ? (T)c.pred.f
-         : std::is_signed<T>::value ? (T)c.pred.i : (T)c.pred.u;
-    // resident CTAs per SM of this instantiation (queried once), and no more CTAs than work
-    // items: a small batch launches a small grid
-    static int per_sm_of[3] = {0, 0, 0};
-    int& per_sm = per_sm_of[c.op];
+uint64_t items_bound(const SegCall& c, uint64_t tile) { return c.S + c.count / tile + 1; }
+
+template <typename T>
+SegPred<T> make_seg_pred(const Pred& p) {
+    SegPred<T> e;
+    e.kind = p.kind;
+    e.negate = p.negate;
+    e.c = std::is_floating_point<T>::value ? (T)p.f : std::is_signed<T>::value ? (T)p.i : (T)p.u;
+    e.m = (T)p.mod_m;
+    e.r = (T)p.mod_r;
+    if (std::is_integral<T>::value && sizeof(T) == 4) e.fm = FastMod32::make((int64_t)e.m);
+    return e;
+}
+
+template <typename T, int BLOCK, int VPT, int OP>
+bool launch_kernel(Workspace& ws, const SegArgs<T>& args, const SegBuffers& b, uint64_t items) {
+    using Sh = SegShape<T, BLOCK, VPT>;
+    auto kfn = k_segmented<T, BLOCK, VPT, OP>;
+    const size_t smem = OP == SEG_REDUCE ? 0 : Sh::SMEM;
+    if (smem > (48u << 10) && !smem_opt_in<k_segmented<T, BLOCK, VPT, OP>>(smem))
+        return cuda_ok(cudaGetLastError(), "segmented shared-memory opt-in");
+    // resident CTAs per SM of this instantiation (queried once per device), and no more
+    // CTAs than work items: a small batch launches a small grid
+    static int per_sm_of[kSmemOptInDevices] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& per_sm = per_sm_of[dev < kSmemOptInDevices && dev >= 0 ? dev : 0];
     if (per_sm == 0) {
-        void* kfn = nullptr;
-        switch (c.op) {
-            case SEG_REDUCE: kfn = (void*)k_segmented<T, ITEMS, SEG_REDUCE>; break;
-            case SEG_SCAN: kfn = (void*)k_segmented<T, ITEMS, SEG_SCAN>; break;
-            default: kfn = (void*)k_segmented<T, ITEMS, SEG_COPY_IF>; break;
-        }
         int v = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kfn, kBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kfn, BLOCK, smem);
         per_sm = v < 1 ? 1 : v;
     }
     const uint64_t resident = (uint64_t)per_sm * device_info().sm_count;
-    const unsigned grid = (unsigned)(items_cap < resident ? items_cap : resident);
-    switch (c.op) {
-        case SEG_REDUCE:
-            k_segmented<T, ITEMS, SEG_REDUCE><<<grid, kBlock, 0, s>>>(c.src, c.S, b, init, false, pr, err);
-            break;
-        case SEG_SCAN:
-            k_segmented<T, ITEMS, SEG_SCAN><<<grid, kBlock, 0, s>>>(c.src, c.S, b, init, c.inclusive, pr, err);
-            break;
-        default:
-            k_segmented<T, ITEMS, SEG_COPY_IF><<<grid, kBlock, 0, s>>>(c.src, c.S, b, init, false, pr, err);
-            break;
-    }
+    const unsigned grid = (unsigned)(items < resident ? items : resident);
+    kfn<<<grid ? grid : 1, BLOCK, smem, ws.stream()>>>(args, b, &ws.d_slot->spin_error);
     return cuda_ok(cudaGetLastError(), "segmented launch");
 }
 
-template <typename T>
-bool enqueue_items(Workspace& ws, const SegCall& c, int items) {
-    const uint64_t tile_min = (uint64_t)kBlock * kCandidates[0];
-    SegBuffers b;
-    if (!seg_buffers(ws, c.S, c.S + c.count / tile_min + 1, &b)) return false;
-    switch (items) {
-        case 4: return enqueue_typed<T, 4>(ws, c, b);
-        case 8: return enqueue_typed<T, 8>(ws, c, b);
-        default: return enqueue_typed<T, 16>(ws, c, b);
+template <typename T, int BLOCK, int VPT>
+bool enqueue_shape(Workspace& ws, const SegCall& c, const SegBuffers& b) {
+    using Sh = SegShape<T, BLOCK, VPT>;
+    constexpr int TILE = Sh::TILE;
+    cudaStream_t s = ws.stream();
+    volatile int32_t* err = &ws.d_slot->spin_error;
+    const uint64_t items_cap = items_bound(c, TILE);
+    SegArgs<T> args;
+    args.src = c.src;
+    args.S = c.S;
+    memcpy(&args.init, &c.init_bits, sizeof(T));
+    args.inclusive = c.inclusive;
+    args.unique = c.unique;
+    args.red = c.red;
+    args.pred = make_seg_pred<T>(c.pred);
+    auto plan = [&](SegEmpty empty, bool tickets) {
+        k_seg_plan<256><<<1, 256, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE, b.item_start,
+                                          b.counters, empty, tickets ? b.tickets : nullptr,
+                                          b.status, b.status_cap, err,
+                                          items_cap <= kInlineItems ? b.item_seg : nullptr);
+        if (items_cap > kInlineItems)
+            k_seg_map<256><<<seg_map_grid(c.S), 256, 0, s>>>(b.item_start, c.S, b.item_seg);
+    };
+    switch (c.op) {
+        case SEG_REDUCE:
+            plan(c.red == RED_COUNT ? SegEmpty::ZERO_COUNT : SegEmpty::ZERO_RESULT, true);
+            return launch_kernel<T, BLOCK, VPT, SEG_REDUCE>(ws, args, b, items_cap);
+        case SEG_SCAN:
+            plan(SegEmpty::NONE, false);
+            return launch_kernel<T, BLOCK, VPT, SEG_SCAN>(ws, args, b, items_cap);
+        case SEG_SELECT:
+            plan(SegEmpty::ZERO_COUNT, false);
+            return launch_kernel<T, BLOCK, VPT, SEG_SELECT>(ws, args, b, items_cap);
+        default: {
+            // count pass (per-segment kept totals into the counts), then the scatter; the
+            // count pass uses no look-back status, so the scatter takes the plan's epoch
+            SegArgs<T> cnt = args;
+            cnt.red = RED_COUNT;
+            plan(SegEmpty::ZERO_COUNT, true);
+            if (!launch_kernel<T, BLOCK, VPT, SEG_REDUCE>(ws, cnt, b, items_cap)) return false;
+            return launch_kernel<T, BLOCK, VPT, SEG_PARTITION>(ws, args, b, items_cap);
+        }
     }
 }
 
-bool enqueue(Workspace& ws, const SegCall& c, int items) {
+template <typename T>
+bool enqueue_typed(Workspace& ws, const SegCall& c, int shape) {
+    SegBuffers b;
+    if (!seg_buffers(ws, c.S, items_bound(c, min_tile<T>()), &b)) return false;
+    switch (shape) {
+        case 0: return enqueue_shape<T, 256, 3>(ws, c, b);
+        case 1: return enqueue_shape<T, 256, 7>(ws, c, b);
+        default: return enqueue_shape<T, 512, 7>(ws, c, b);
+    }
+}
+
+bool enqueue(Workspace& ws, const SegCall& c, int shape) {
     switch (c.t) {
-        case DType::F32: return enqueue_items<float>(ws, c, items);
-        case DType::F64: return enqueue_items<double>(ws, c, items);
-        case DType::I32: return enqueue_items<int32_t>(ws, c, items);
-        case DType::I64: return enqueue_items<int64_t>(ws, c, items);
-        case DType::U32: return enqueue_items<uint32_t>(ws, c, items);
-        case DType::U64: return enqueue_items<uint64_t>(ws, c, items);
+        case DType::F32: return enqueue_typed<float>(ws, c, shape);
+        case DType::F64: return enqueue_typed<double>(ws, c, shape);
+        case DType::I32: return enqueue_typed<int32_t>(ws, c, shape);
+        case DType::I64: return enqueue_typed<int64_t>(ws, c, shape);
+        case DType::U32: return enqueue_typed<uint32_t>(ws, c, shape);
+        case DType::U64: return enqueue_typed<uint64_t>(ws, c, shape);
         default: break;
     }
     set_error(PARALLAX_ERR_INVALID_ARGUMENT, "segmented: unsupported element type");
@@ -374,10 +655,17 @@ bool enqueue(Workspace& ws, const SegCall& c, int items) {
 }
 
 // ---- autotuner -----------------------------------------------------------------------------------
-// Choice per (op, dtype, log2 of the average segment length); timed on the first call with
-// those parameters, optionally persisted in PARALLAX_TUNE_CACHE ("op dtype bucket items").
+// Shape per (op, dtype, log2 of the average segment length); timed on the first call with
+// those parameters, optionally persisted in PARALLAX_TUNE_CACHE, one line per choice:
+// "op dtype bucket block vpt".
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int>, int>* g_tune = nullptr;
+
+int shape_index(int block, int vpt) {
+    for (int i = 0; i < kNumShapes; ++i)
+        if (kShapes[i].block == block && kShapes[i].vpt == vpt) return i;
+    return -1;
+}
 
 void tune_load_locked() {
     if (g_tune) return;
@@ -386,9 +674,11 @@ void tune_load_locked() {
     if (!path) return;
     FILE* f = fopen(path, "r");
     if (!f) return;
-    int op, t, bucket, items;
-    while (fscanf(f, "%d %d %d %d", &op, &t, &bucket, &items) == 4)
-        (*g_tune)[std::make_tuple(op, t, bucket)] = items;
+    int op, t, bucket, block, vpt;
+    while (fscanf(f, "%d %d %d %d %d", &op, &t, &bucket, &block, &vpt) == 5) {
+        const int i = shape_index(block, vpt);
+        if (i >= 0) (*g_tune)[std::make_tuple(op, t, bucket)] = i;
+    }
     fclose(f);
 }
 
@@ -398,8 +688,8 @@ void tune_store_locked() {
     FILE* f = fopen(path, "w");
     if (!f) return;
     for (auto& kv : *g_tune)
-        fprintf(f, "%d %d %d %d\n", std::get<0>(kv.first), std::get<1>(kv.first),
-                std::get<2>(kv.first), kv.second);
+        fprintf(f, "%d %d %d %d %d\n", std::get<0>(kv.first), std::get<1>(kv.first),
+                std::get<2>(kv.first), kShapes[kv.second].block, kShapes[kv.second].vpt);
     fclose(f);
 }
 
@@ -410,9 +700,10 @@ int bucket_of(const SegCall& c) {
     return b;
 }
 
-// Returns the tile choice, timing the candidates (and leaving valid results) when unknown.
-int tuned_items(Workspace& ws, const SegCall& c) {
-    const auto key = std::make_tuple((int)c.op, (int)c.t, bucket_of(c));
+// Returns the shape choice, timing the candidates (and leaving valid results) when unknown.
+int tuned_shape(Workspace& ws, const SegCall& c) {
+    const int opkey = c.op * 8 + c.red * 2 + (c.unique ? 1 : 0);
+    const auto key = std::make_tuple(opkey, (int)c.t, bucket_of(c));
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         tune_load_locked();
@@ -421,15 +712,15 @@ int tuned_items(Workspace& ws, const SegCall& c) {
     }
     if (!c.tune || (getenv("PARALLAX_TUNE") && atoi(getenv("PARALLAX_TUNE")) == 0)) {
         const uint64_t avg = c.S ? c.count / c.S : 0;  // untuned: by average segment length
-        return avg >= (16u << 10) ? 16 : avg >= (2u << 10) ? 8 : 4;
+        return avg >= (16u << 10) ? 2 : avg >= (2u << 10) ? 1 : 0;
     }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    int best = 8;
+    int best = 1;
     float best_ms = 1e30f;
     cudaStream_t s = ws.stream();
-    for (int cand : kCandidates) {
+    for (int cand = 0; cand < kNumShapes; ++cand) {
         if (!enqueue(ws, c, cand)) break;  // warm-up (first-touch, module load)
         cudaEventRecord(e0, s);
         if (!enqueue(ws, c, cand)) break;
@@ -448,44 +739,55 @@ int tuned_items(Workspace& ws, const SegCall& c) {
     (*g_tune)[key] = best;
     tune_store_locked();
     if (getenv("PARALLAX_DEBUG"))
-        fprintf(stderr, "[parallax] tuned segmented op %d dtype %d bucket %d -> %d items/thread (%.3f ms)\n",
-                (int)c.op, (int)c.t, bucket_of(c), best, best_ms);
+        fprintf(stderr,
+                "[parallax] tuned segmented op %d dtype %d bucket %d -> %d threads x %d vectors "
+                "(%.3f ms)\n",
+                opkey, (int)c.t, bucket_of(c), kShapes[best].block, kShapes[best].vpt, best_ms);
     return best;
 }
 
 // ---- graph capture and replay -----------------------------------------------------------------
-std::string graph_key(const SegCall& c, int items) {
+std::string graph_key(const SegCall& c, int shape) {
     char k[512];
-    snprintf(k, sizeof k, "%d/%d/%llx/%llx/%p/%llx/%llu/%llu/%llx/%d/%d/%d/%g/%lld/%llu/%d", c.op,
-             (int)c.t, (unsigned long long)c.src.in, (unsigned long long)c.src.out,
-             (const void*)c.src.offsets, (unsigned long long)c.src.aux, (unsigned long long)c.S,
-             (unsigned long long)c.count, (unsigned long long)c.init_bits, (int)c.inclusive,
-             (int)c.pred.kind, (int)c.pred.negate, c.pred.f, (long long)c.pred.i,
-             (unsigned long long)c.pred.u, items);
+    snprintf(k, sizeof k, "%d/%d/%d/%d/%llx/%llx/%p/%llx/%llu/%llu/%llx/%d/%d/%d/%g/%lld/%llu/%lld/%lld/%d",
+             c.op, c.red, (int)c.unique, (int)c.t, (unsigned long long)c.src.in,
+             (unsigned long long)c.src.out, (const void*)c.src.offsets,
+             (unsigned long long)c.src.aux, (unsigned long long)c.S, (unsigned long long)c.count,
+             (unsigned long long)c.init_bits, (int)c.inclusive, (int)c.pred.kind,
+             (int)c.pred.negate, c.pred.f, (long long)c.pred.i, (unsigned long long)c.pred.u,
+             (long long)c.pred.mod_m, (long long)c.pred.mod_r, shape);
     return k;
 }
 
-const char* op_name(int op) {
-    return op == SEG_REDUCE ? "segmented_reduce"
-         : op == SEG_SCAN ? "segmented_scan" : "segmented_copy_if";
+const char* op_name(const SegCall& c) {
+    switch (c.op) {
+        case SEG_REDUCE: return "segmented_reduce";
+        case SEG_SCAN: return "segmented_scan";
+        case SEG_SELECT: return c.unique ? "segmented_unique" : "segmented_copy_if";
+        default: return "segmented_partition";
+    }
 }
 
 // Sizes the buffers for the smallest tile before any capture (growth would invalidate a
 // captured graph).
 bool reserve(Workspace& ws, const SegCall& c) {
-    const uint64_t tile_min = (uint64_t)kBlock * kCandidates[0];
     SegBuffers b;
-    return seg_buffers(ws, c.S, c.S + c.count / tile_min + 1, &b);
+    const uint64_t tile = c.t == DType::F64 || c.t == DType::I64 || c.t == DType::U64
+        ? (uint64_t)min_tile<uint64_t>() : (uint64_t)min_tile<uint32_t>();
+    return seg_buffers(ws, c.S, items_bound(c, tile), &b);
 }
 
 bool run(Workspace& ws, const SegCall& c, bool graph) {
-    const int items = tuned_items(ws, c);
+    const int shape = tuned_shape(ws, c);
     if (!reserve(ws, c)) return false;
     const size_t es = dtype_size(c.t);
-    ProfScope prof(ws, op_name(c.op), (c.op == SEG_SCAN ? 2 : 1) * c.count * es);
-    count_launch(3);
-    if (!graph) return enqueue(ws, c, items);
-    return graph_launch(ws, graph_key(c, items), [&] { return enqueue(ws, c, items); });
+    // algorithmic bytes: input read (+ output written for scans; compaction outputs are
+    // data-dependent and partition writes every element)
+    const uint64_t bytes = (c.op == SEG_SCAN || c.op == SEG_PARTITION ? 2 : 1) * c.count * es;
+    ProfScope prof(ws, op_name(c), bytes);
+    count_launch(c.op == SEG_PARTITION ? 4 : 3);
+    if (!graph) return enqueue(ws, c, shape);
+    return graph_launch(ws, graph_key(c, shape), [&] { return enqueue(ws, c, shape); });
 }
 
 int seg_entry(SegCall c, const void* in, void* out, const uint64_t* offsets, void* aux,
@@ -503,33 +805,40 @@ int seg_entry(SegCall c, const void* in, void* out, const uint64_t* offsets, voi
     const void* d_off = device_operand(offsets, fn, "offsets");
     if (!d_off) return last_error();
     if (c.op != SEG_REDUCE && data && !(d_out = device_operand(out, fn, "output"))) return last_error();
-    void* d_aux = nullptr;  // results (reduce) or counts (copy_if); scans have none
+    void* d_aux = nullptr;  // results (reduce) or counts (compaction); scans have none
     if (c.op != SEG_SCAN &&
         !(d_aux = device_operand(aux, fn, c.op == SEG_REDUCE ? "results" : "counts")))
         return last_error();
-    if (c.S >= 0xffffffffull || c.count / ((uint64_t)kBlock * kCandidates[0]) + c.S >= 0xffffffffull) {
+    if (c.S >= 0xffffffffull || c.count / 1000 + c.S >= 0xffffffffull) {
         set_error(PARALLAX_ERR_INVALID_ARGUMENT, "%s: too many segments / elements", fn);
         return PARALLAX_ERR_INVALID_ARGUMENT;
     }
     const uint32_t es = (uint32_t)dtype_size(c.t);
+    const uint32_t aux_stride = c.op == SEG_REDUCE && c.red != RED_COUNT ? es : 8u;
     c.src = SegSrc{static_cast<const uint64_t*>(d_off), nullptr, (uint64_t)d_in, (uint64_t)d_out,
-                   (uint64_t)d_aux, c.op == SEG_COPY_IF ? 8u : es, es};
+                   (uint64_t)d_aux, aux_stride, es};
     if (!run(*ws, c, true)) return last_error() ? last_error() : PARALLAX_ERR_CUDA;
     return ws->async ? PARALLAX_OK : sync_stream(*ws);
 }
+
+Handle* seg_handle(parallax_kernel_t k) { return as_handle(k); }
 
 }  // namespace
 
 bool launch_segmented_descs(Workspace& ws, SegKind op, DType t, const Pred& p, bool inclusive,
                             uint64_t init_bits, const SegDesc* d_descs, uint64_t S,
-                            uint64_t total) {
+                            uint64_t total, RedOp red, CompactMode mode) {
     if (S == 0) return true;
-    if (S >= 0xffffffffull || total / ((uint64_t)kBlock * kCandidates[0]) + S >= 0xffffffffull) {
+    if (S >= 0xffffffffull || total / 1000 + S >= 0xffffffffull) {
         set_error(PARALLAX_ERR_INVALID_ARGUMENT, "batched launch: too many segments / elements");
         return false;
     }
     SegCall c{};
-    c.op = (int)op;
+    c.op = op == SegKind::REDUCE ? SEG_REDUCE
+         : op == SegKind::SCAN ? SEG_SCAN
+         : mode == CompactMode::PARTITION ? SEG_PARTITION : SEG_SELECT;
+    c.red = red == RedOp::MAX ? RED_MAX : red == RedOp::MIN ? RED_MIN : RED_SUM;
+    c.unique = op == SegKind::COPY_IF && mode == CompactMode::UNIQUE;
     c.t = t;
     c.src = SegSrc{nullptr, d_descs, 0, 0, 0, 0, (uint32_t)dtype_size(t)};
     c.S = S;
@@ -571,13 +880,14 @@ using namespace pxb;
 PXB_EXPORT int parallax_segmented_reduce(parallax_kernel_t kernel, const void* data, size_t count,
                                          const uint64_t* offsets, size_t num_segments,
                                          void* results) {
-    Handle* h = as_handle(kernel);
-    if (!h || h->kind != Kind::REDUCE || h->op != RedOp::SUM) {
-        set_error(PARALLAX_ERR_INVALID_HANDLE, "parallax_segmented_reduce: needs a reduce:sum handle");
+    Handle* h = seg_handle(kernel);
+    if (!h || h->kind != Kind::REDUCE) {
+        set_error(PARALLAX_ERR_INVALID_HANDLE, "parallax_segmented_reduce: needs a reduce handle");
         return PARALLAX_ERR_INVALID_HANDLE;
     }
     SegCall c{};
     c.op = SEG_REDUCE;
+    c.red = h->op == RedOp::MAX ? RED_MAX : h->op == RedOp::MIN ? RED_MIN : RED_SUM;
     c.t = h->dtype;
     c.count = count;
     c.S = num_segments;
@@ -585,13 +895,13 @@ PXB_EXPORT int parallax_segmented_reduce(parallax_kernel_t kernel, const void* d
     return seg_entry(c, data, nullptr, offsets, results, "parallax_segmented_reduce");
 }
 
-PXB_EXPORT int parallax_segmented_exclusive_scan(parallax_kernel_t kernel, const void* input,
-                                                 void* output, size_t count,
-                                                 const uint64_t* offsets, size_t num_segments,
-                                                 const void* init) {
-    Handle* h = as_handle(kernel);
+namespace {
+int seg_scan_entry(parallax_kernel_t kernel, const void* input, void* output, size_t count,
+                   const uint64_t* offsets, size_t num_segments, const void* init,
+                   bool inclusive, const char* fn) {
+    Handle* h = seg_handle(kernel);
     if (!h || h->kind != Kind::SCAN) {
-        set_error(PARALLAX_ERR_INVALID_HANDLE, "parallax_segmented_exclusive_scan: needs a scan handle");
+        set_error(PARALLAX_ERR_INVALID_HANDLE, "%s: needs a scan handle", fn);
         return PARALLAX_ERR_INVALID_HANDLE;
     }
     SegCall c{};
@@ -599,27 +909,70 @@ PXB_EXPORT int parallax_segmented_exclusive_scan(parallax_kernel_t kernel, const
     c.t = h->dtype;
     c.count = count;
     c.S = num_segments;
+    c.inclusive = inclusive;
     c.tune = input != output;  // timing the candidates in place would scan twice
-    if (init) memcpy(&c.init_bits, init, dtype_size(h->dtype));
-    return seg_entry(c, input, output, offsets, nullptr, "parallax_segmented_exclusive_scan");
+    if (init && !inclusive) memcpy(&c.init_bits, init, dtype_size(h->dtype));
+    return seg_entry(c, input, output, offsets, nullptr, fn);
+}
+
+int seg_compact_entry(parallax_kernel_t kernel, const void* input, void* output, size_t count,
+                      const uint64_t* offsets, size_t num_segments, uint64_t* counts,
+                      int which, const char* fn) {
+    // which: 0 copy_if / remove_if, 1 partition, 2 unique
+    Handle* h = seg_handle(kernel);
+    const bool ok = h && ((which == 0 && h->kind == Kind::COMPACT_FLAGS) ||
+                          (which == 1 && h->kind == Kind::PARTITION_SCATTER) ||
+                          (which == 2 && h->kind == Kind::UNIQUE_FLAGS));
+    if (!ok) {
+        set_error(PARALLAX_ERR_INVALID_HANDLE, "%s: needs a %s handle", fn,
+                  which == 0 ? "copy_if / remove_if" : which == 1 ? "partition" : "unique");
+        return PARALLAX_ERR_INVALID_HANDLE;
+    }
+    SegCall c{};
+    c.op = which == 1 ? SEG_PARTITION : SEG_SELECT;
+    c.unique = which == 2;
+    c.t = h->dtype;
+    c.count = count;
+    c.S = num_segments;
+    c.tune = which != 1 || input != output;
+    c.pred = h->pred;
+    if (h->kind == Kind::COMPACT_FLAGS && h->remove) c.pred.negate = !c.pred.negate;
+    return seg_entry(c, input, output, offsets, counts, fn);
+}
+}  // namespace
+
+PXB_EXPORT int parallax_segmented_exclusive_scan(parallax_kernel_t kernel, const void* input,
+                                                 void* output, size_t count,
+                                                 const uint64_t* offsets, size_t num_segments,
+                                                 const void* init) {
+    return seg_scan_entry(kernel, input, output, count, offsets, num_segments, init, false,
+                          "parallax_segmented_exclusive_scan");
+}
+
+PXB_EXPORT int parallax_segmented_inclusive_scan(parallax_kernel_t kernel, const void* input,
+                                                 void* output, size_t count,
+                                                 const uint64_t* offsets, size_t num_segments) {
+    return seg_scan_entry(kernel, input, output, count, offsets, num_segments, nullptr, true,
+                          "parallax_segmented_inclusive_scan");
 }
 
 PXB_EXPORT int parallax_segmented_copy_if(parallax_kernel_t kernel, const void* input,
                                           void* output, size_t count, const uint64_t* offsets,
                                           size_t num_segments, uint64_t* counts) {
-    Handle* h = as_handle(kernel);
-    if (!h || h->kind != Kind::COMPACT_FLAGS || h->pred.kind == PredKind::MOD) {
-        set_error(PARALLAX_ERR_INVALID_HANDLE,
-                  "parallax_segmented_copy_if: needs a copy_if / remove_if handle (comparison predicate)");
-        return PARALLAX_ERR_INVALID_HANDLE;
-    }
-    SegCall c{};
-    c.op = SEG_COPY_IF;
-    c.t = h->dtype;
-    c.count = count;
-    c.S = num_segments;
-    c.tune = true;
-    c.pred = h->pred;
-    if (h->remove) c.pred.negate = !c.pred.negate;
-    return seg_entry(c, input, output, offsets, counts, "parallax_segmented_copy_if");
+    return seg_compact_entry(kernel, input, output, count, offsets, num_segments, counts, 0,
+                             "parallax_segmented_copy_if");
+}
+
+PXB_EXPORT int parallax_segmented_partition(parallax_kernel_t kernel, const void* input,
+                                            void* output, size_t count, const uint64_t* offsets,
+                                            size_t num_segments, uint64_t* counts) {
+    return seg_compact_entry(kernel, input, output, count, offsets, num_segments, counts, 1,
+                             "parallax_segmented_partition");
+}
+
+PXB_EXPORT int parallax_segmented_unique(parallax_kernel_t kernel, const void* input,
+                                         void* output, size_t count, const uint64_t* offsets,
+                                         size_t num_segments, uint64_t* counts) {
+    return seg_compact_entry(kernel, input, output, count, offsets, num_segments, counts, 2,
+                             "parallax_segmented_unique");
 }

@@ -5,16 +5,25 @@
 // sums -> add-offsets pass, src/kernel/kernel_launcher.cpp:1280-1342,
 // shaders/scan.comp + scan_add.comp). Each tile publishes its aggregate as soon as it is
 // known (state AGG) and its inclusive prefix once its look-back completes (state INC).
-// A tile's look-back walks predecessors 32 at a time (one warp), summing aggregates until
-// it meets an inclusive prefix. Tiles are processed in blockIdx order, so every tile a
-// CTA waits on belongs to a CTA that was dispatched earlier: the waits always end.
-// Each wait is still bounded: after kSpinLimit polls the kernel records an error code in
-// host-visible memory and carries on with a zero contribution, so a fault can never
-// hang the GPU; the host turns the code into PARALLAX_ERR_DEVICE_SPIN.
+// A tile's look-back reads its predecessors' status entries, summing aggregates until it
+// meets an inclusive prefix. Tiles are processed in blockIdx order (or claimed in order
+// from an atomic counter), so every tile a CTA waits on belongs to a CTA that started
+// earlier: the waits always end.
+// Each wait is still bounded: after `limit` polls (kSpinLimit unless PARALLAX_WAIT_LIMIT
+// sets fewer) the kernel records an error code in host-visible memory and carries on with
+// a zero contribution, so a fault can never hang the GPU; the host turns the code into
+// PARALLAX_ERR_DEVICE_SPIN.
 //
-// Status words: bits [31:2] = launch epoch (30 bits), bits [1:0] = state
-// (0 none, 1 AGG, 2 INC). Words left by earlier launches carry an older epoch and read as
-// "none", so the status array is never cleared between launches.
+// Status entry: 16 bytes, two 8-byte words {low 32 bits of the value, flag} and {high 32
+// bits, flag}, written with one 16-byte store and read with one 16-byte load, so a poll is a
+// single round trip to L2 (under a saturated memory system that round trip queues behind
+// the SM's bulk loads, and it used to take two: flag, then value). Each 8-byte word is
+// written and read whole, so the value half in a word always belongs to that word's flag;
+// a read whose two flags differ (a load that met the store half-way, or AGG then INC)
+// counts as "not published yet" and polls again.
+// Flag: bits [31:2] = launch epoch (30 bits), bits [1:0] = state (0 none, 1 AGG, 2 INC).
+// Entries left by earlier launches carry an older epoch and read as "none", so the status
+// array is never cleared between launches.
 #pragma once
 
 #include <string.h>
@@ -26,22 +35,29 @@ namespace pxb {
 
 constexpr uint32_t kSpinLimit = 1u << 22;
 
-// One status entry per tile; the same 24-byte layout for every accumulator type keeps
+// One status entry per tile; the same 16-byte layout for every accumulator type keeps
 // flag words at fixed addresses across launches (see Workspace::scratch).
-struct StatusEntry {
-    uint32_t flag;
-    uint32_t pad;
-    uint64_t agg;
-    uint64_t inc;
+struct __align__(16) StatusEntry {
+    uint32_t lo;
+    uint32_t flag_lo;
+    uint32_t hi;
+    uint32_t flag_hi;
 };
-static_assert(sizeof(StatusEntry) == 24, "status entry layout");
+static_assert(sizeof(StatusEntry) == 16, "status entry layout");
 
 template <typename A>
 struct TileStatus {
     StatusEntry* e;
     uint32_t epoch;
     volatile int32_t* err;
+    uint32_t limit = kSpinLimit;  // polls of one predecessor before the wait gives up
+    bool near_first = false;      // EXPERIMENT: warp-first round (PARALLAX_LB_NEAR)
 };
+
+// Poll limit of the look-back waits launched from now on: kSpinLimit, or the smaller
+// number of polls given by PARALLAX_WAIT_LIMIT (read once; an opt-in for tests that make
+// a wait run out quickly).
+uint32_t wait_limit();
 
 template <typename A>
 __device__ __forceinline__ void put_val(uint64_t* p, A v) {
@@ -57,69 +73,54 @@ __device__ __forceinline__ A get_val(const uint64_t* p) {
     return v;
 }
 
-// Must be called by all 32 lanes of exactly one warp of the CTA. Returns the exclusive
-// prefix (sum of aggregates of tiles 0..tile-1) in every lane.
+// Publishes `v` with state 1 (AGG) or 2 (INC) in one 16-byte store.
 template <typename A>
-__device__ __forceinline__ A lookback(const TileStatus<A>& ts, uint64_t tile, A agg) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t ep = (ts.epoch & 0x3fffffffu) << 2;
-    if (tile == 0) {
-        if (lane == 0) {
-            put_val(&ts.e[0].inc, agg);
-            st_release_u32(&ts.e[0].flag, ep | 2u);
+__device__ __forceinline__ void publish(StatusEntry* e, uint32_t ep, uint32_t state, A v) {
+    uint64_t bits = 0;
+    memcpy(&bits, &v, sizeof(A));
+    const uint64_t f = (uint64_t)(ep | state) << 32;
+    const uint64_t w0 = (bits & 0xffffffffull) | f, w1 = (bits >> 32) | f;
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(e), "l"(w0), "l"(w1)
+                 : "memory");
+}
+// One 16-byte read of an entry: true with its state and value when both flags agree and
+// carry this launch's epoch with a published state.
+template <typename A>
+__device__ __forceinline__ bool read_status(const StatusEntry* e, uint32_t ep, uint32_t* state,
+                                            A* v) {
+    uint64_t w0, w1;
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(e)
+                 : "memory");
+    const uint32_t f0 = (uint32_t)(w0 >> 32), f1 = (uint32_t)(w1 >> 32);
+    if (f0 != f1 || (f0 & ~3u) != ep || (f0 & 3u) == 0u) return false;
+    const uint64_t bits = (w0 & 0xffffffffull) | (w1 << 32);
+    memcpy(v, &bits, sizeof(A));
+    *state = f0 & 3u;
+    return true;
+}
+
+// Waits (bounded) until predecessor idx has published, then returns its state (1 AGG,
+// 2 INC) and value; a wait that gives up records the error and reads as INC with value 0.
+template <typename A>
+__device__ __forceinline__ uint32_t poll_status(const TileStatus<A>& ts, int64_t idx, uint32_t ep,
+                                                A* v) {
+    uint32_t state = 0, spins = 0;
+    while (!read_status(&ts.e[idx], ep, &state, v)) {
+        if (++spins > ts.limit) {
+            *ts.err = 1;
+            *v = A(0);
+            return 2u;
         }
-        return A(0);
+        if (spins > 8) nanosleep_ns(64);
     }
-    if (lane == 0) {
-        put_val(&ts.e[tile].agg, agg);
-        st_release_u32(&ts.e[tile].flag, ep | 1u);
-    }
-    A excl = A(0);
-    int64_t pred = (int64_t)tile - 1;
-    for (;;) {
-        const int64_t idx = pred - lane;
-        uint32_t state = 2u;
-        A v = A(0);
-        if (idx >= 0) {
-            uint32_t f = 0, spins = 0;
-            bool gave_up = false;
-            for (;;) {
-                f = ld_acquire_u32(&ts.e[idx].flag);
-                if ((f & ~3u) == ep && (f & 3u) != 0u) break;
-                if (++spins > kSpinLimit) {
-                    *ts.err = 1;
-                    gave_up = true;
-                    break;
-                }
-                if (spins > 16) nanosleep_ns(64);
-            }
-            if (gave_up) {
-                state = 2u;
-            } else {
-                state = f & 3u;
-                v = state == 2u ? get_val<A>(&ts.e[idx].inc) : get_val<A>(&ts.e[idx].agg);
-            }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, state == 2u);
-        const int first = m ? __ffs(m) - 1 : 32;
-        A c = lane <= first ? v : A(0);
-        c = warp_reduce(c, OpSum());
-        excl = c + excl;
-        if (m) break;
-        pred -= 32;
-    }
-    if (lane == 0) {
-        put_val(&ts.e[tile].inc, excl + agg);
-        st_release_u32(&ts.e[tile].flag, ep | 2u);
-    }
-    return excl;
+    return state;
 }
 
 // CTA-wide look-back: called by ALL threads of a CTA of BLOCK threads (a multiple of 32),
 // with the tile aggregate in every thread. Each round, every thread inspects one
 // predecessor (tile - 1 - tid - round offset), so one round trip to L2 covers BLOCK
 // predecessors instead of 32: when hundreds of resident tiles stand between a tile and the
-// nearest published inclusive prefix, this takes a couple of round trips instead of ten.
+// nearest published inclusive prefix, this takes one round trip instead of ten.
 // `red` is shared scratch of at least BLOCK / 32 + 1 elements of A and `first` of BLOCK / 32
 // ints. Returns the exclusive prefix in every thread; the same contribution order for the
 // same status pattern, so integer results are exact and fp results deterministic given the
@@ -127,30 +128,8 @@ __device__ __forceinline__ A lookback(const TileStatus<A>& ts, uint64_t tile, A 
 // `lo` is the first index of the chain (0 for a whole array, a segment's first tile for the
 // segmented kernels): that tile publishes its inclusive prefix at once, and indices below
 // it are never polled.
-// Waits (bounded) until predecessor idx has published, then returns its state (1 AGG,
-// 2 INC) and value; a wait that gives up records the error and reads as INC with value 0.
-template <typename A>
-__device__ __forceinline__ uint32_t poll_status(const TileStatus<A>& ts, int64_t idx, uint32_t ep,
-                                                A* v) {
-    uint32_t f = 0, spins = 0;
-    for (;;) {
-        f = ld_acquire_u32(&ts.e[idx].flag);
-        if ((f & ~3u) == ep && (f & 3u) != 0u) break;
-        if (++spins > kSpinLimit) {
-            *ts.err = 1;
-            *v = A(0);
-            return 2u;
-        }
-        if (spins > 16) nanosleep_ns(64);
-    }
-    const uint32_t state = f & 3u;
-    *v = state == 2u ? get_val<A>(&ts.e[idx].inc) : get_val<A>(&ts.e[idx].agg);
-    return state;
-}
-
 // NEAR_FIRST: warp 0 alone inspects the 32 nearest predecessors first, and the CTA-wide
-// rounds run only when none of them holds an inclusive prefix (in the steady state one of
-// them does, and 32 polls cost far less than BLOCK).
+// rounds run only when none of them holds an inclusive prefix.
 template <typename A, int BLOCK, bool NEAR_FIRST = false>
 __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile, A agg, A* red,
                                           int* first, uint64_t lo = 0) {
@@ -158,19 +137,13 @@ __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t ep = (ts.epoch & 0x3fffffffu) << 2;
     if (tile == lo) {
-        if (tid == 0) {
-            put_val(&ts.e[tile].inc, agg);
-            st_release_u32(&ts.e[tile].flag, ep | 2u);
-        }
+        if (tid == 0) publish(&ts.e[tile], ep, 2u, agg);
         return A(0);
     }
-    if (tid == 0) {
-        put_val(&ts.e[tile].agg, agg);
-        st_release_u32(&ts.e[tile].flag, ep | 1u);
-    }
+    if (tid == 0) publish(&ts.e[tile], ep, 1u, agg);
     A excl = A(0);
     int64_t pred = (int64_t)tile - 1;
-    if constexpr (NEAR_FIRST) {
+    if (NEAR_FIRST && ts.near_first) {
         if (warp == 0) {
             const int64_t idx = pred - lane;
             A v = A(0);
@@ -189,36 +162,15 @@ __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile
         const bool done = first[0] != 0;
         __syncthreads();  // red / first reusable
         if (done) {
-            if (tid == 0) {
-                put_val(&ts.e[tile].inc, excl + agg);
-                st_release_u32(&ts.e[tile].flag, ep | 2u);
-            }
+            if (tid == 0) publish(&ts.e[tile], ep, 2u, excl + agg);
             return excl;
         }
         pred -= 32;
     }
     for (;;) {
         const int64_t idx = pred - tid;
-        uint32_t state = 2u;
         A v = A(0);
-        if (idx >= (int64_t)lo) {
-            uint32_t f = 0, spins = 0;
-            bool gave_up = false;
-            for (;;) {
-                f = ld_acquire_u32(&ts.e[idx].flag);
-                if ((f & ~3u) == ep && (f & 3u) != 0u) break;
-                if (++spins > kSpinLimit) {
-                    *ts.err = 1;
-                    gave_up = true;
-                    break;
-                }
-                if (spins > 16) nanosleep_ns(64);
-            }
-            if (!gave_up) {
-                state = f & 3u;
-                v = state == 2u ? get_val<A>(&ts.e[idx].inc) : get_val<A>(&ts.e[idx].agg);
-            }
-        }
+        const uint32_t state = idx >= (int64_t)lo ? poll_status(ts, idx, ep, &v) : 2u;
         // nearest inclusive prefix = the lowest thread index holding one
         const unsigned m = __ballot_sync(0xffffffffu, state == 2u);
         if (lane == 0) first[warp] = m ? warp * 32 + __ffs(m) - 1 : BLOCK;
@@ -238,10 +190,7 @@ __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile
         if (nearest < BLOCK) break;
         pred -= BLOCK;
     }
-    if (tid == 0) {
-        put_val(&ts.e[tile].inc, excl + agg);
-        st_release_u32(&ts.e[tile].flag, ep | 2u);
-    }
+    if (tid == 0) publish(&ts.e[tile], ep, 2u, excl + agg);
     return excl;
 }
 
@@ -252,6 +201,9 @@ inline TileStatus<A> tile_status_at(char* scratch, uint32_t epoch, int32_t* err)
     ts.e = reinterpret_cast<StatusEntry*>(scratch + kScratchSmall);
     ts.epoch = epoch;
     ts.err = err;
+    ts.limit = wait_limit();
+    static const bool near = getenv("PARALLAX_LB_NEAR") != nullptr;
+    ts.near_first = near;
     return ts;
 }
 

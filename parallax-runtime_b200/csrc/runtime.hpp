@@ -281,9 +281,12 @@ bool launch_mismatch(Workspace& ws, DType t, const void* d_a, const void* d_b, s
 // asynchronous on the workspace stream, no graph capture. Used by the serving loop.
 enum class SegKind : int { REDUCE = 0, SCAN = 1, COPY_IF = 2 };
 struct SegDesc;
+// `red` picks the reduce (sum / max / min); `mode` the compaction (select, unique,
+// partition; partition counts into each descriptor's aux slot, then scatters).
 bool launch_segmented_descs(Workspace& ws, SegKind op, DType t, const Pred& p, bool inclusive,
                             uint64_t init_bits, const SegDesc* d_descs, uint64_t S,
-                            uint64_t total);
+                            uint64_t total, RedOp red = RedOp::SUM,
+                            CompactMode mode = CompactMode::SELECT);
 // Sorts every descriptor's segment in place (aux = an n-element device temporary);
 // `max_len` bounds the segment lengths. `t` is U64 for sort_kv records.
 bool launch_segmented_sort_descs(Workspace& ws, DType t, const SegDesc* d_descs, uint64_t S,

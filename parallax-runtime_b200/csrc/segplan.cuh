@@ -154,7 +154,7 @@ k_seg_plan(SegSrc src, uint64_t S, uint64_t count, uint32_t tile,
     }
     __syncthreads();
     if (counters[2] == 0) {
-        for (uint64_t i = tid; i < status_cap; i += BLOCK) status[i].flag = 0;
+        for (uint64_t i = tid; i < status_cap; i += BLOCK) status[i] = StatusEntry{0u, 0u, 0u, 0u};
         __syncthreads();
         if (tid == 0) counters[2] = 1;
     }

@@ -16,10 +16,9 @@
 //   * coalescing: the head request and every queued request of the same kind (operation,
 //     element type, predicate, scan flavour) up to `solo_elements` long become ONE
 //     segmented launch over per-request descriptors (segmented.cu, sort.cu): a planner plus
-//     one persistent kernel, or the per-segment merge passes of the segmented sort. Longer
-//     requests, kinds without a segmented form (reduce max/min, modulo predicates, unique,
-//     partition), and a request that finds no partner run alone through the plain
-//     launchers.
+//     one persistent kernel (every reduce, scan and compaction kind has one), or the
+//     per-segment merge passes of the segmented sort. Longer requests and a request that
+//     finds no partner run alone through the plain launchers.
 // Requests that arrive while others are on the device are admitted into the next free
 // lane, so batches overlap on the device; a request's result does not depend on what it
 // was batched with (integer results are bit-exact, floating-point ones are within the
@@ -258,12 +257,14 @@ class Server {
             return false;
         switch (h.op) {
             case ReqOp::REDUCE:
-                return launch_segmented_descs(ws, SegKind::REDUCE, h.t, h.pred, false, 0, l.d_desc, S, total);
+                return launch_segmented_descs(ws, SegKind::REDUCE, h.t, h.pred, false, 0, l.d_desc,
+                                              S, total, h.red);
             case ReqOp::SCAN:
                 return launch_segmented_descs(ws, SegKind::SCAN, h.t, h.pred, !h.exclusive,
                                               h.exclusive ? h.init_bits : 0, l.d_desc, S, total);
             case ReqOp::COMPACT:
-                return launch_segmented_descs(ws, SegKind::COPY_IF, h.t, h.pred, false, 0, l.d_desc, S, total);
+                return launch_segmented_descs(ws, SegKind::COPY_IF, h.t, h.pred, false, 0, l.d_desc,
+                                              S, total, RedOp::SUM, h.mode);
             case ReqOp::SORT:
                 return launch_segmented_sort_descs(ws, h.t, l.d_desc, S, total, max_len);
         }
@@ -375,7 +376,7 @@ int make_request(const parallax_request* q, Request* r) {
         case Kind::REDUCE:
             r->op = ReqOp::REDUCE;
             r->red = h->op;
-            r->coalescible = h->op == RedOp::SUM;
+            r->coalescible = true;
             break;
         case Kind::SCAN:
             r->op = ReqOp::SCAN;
@@ -397,7 +398,7 @@ int make_request(const parallax_request* q, Request* r) {
             r->mode = h->kind == Kind::UNIQUE_FLAGS ? CompactMode::UNIQUE
                     : h->kind == Kind::PARTITION_SCATTER ? CompactMode::PARTITION
                                                          : CompactMode::SELECT;
-            r->coalescible = r->mode == CompactMode::SELECT && h->pred.kind != PredKind::MOD;
+            r->coalescible = true;
             break;
         default:
             set_error(PARALLAX_ERR_INVALID_HANDLE, "%s: no served form for this kernel", fn);

@@ -163,3 +163,9 @@ def test_kernel_abi_header_layout():
     from pathlib import Path
     src = (Path(__file__).resolve().parents[1] / "include/parallax/kernel_abi.h").read_text()
     assert "PARALLAX_MAX_CAPTURE_BYTES 256" in src
+
+
+def test_check_bounded_wait_rejects_a_poll_count_outside_its_range(lib, px):
+    assert lib.parallax_check_bounded_wait(0) == px.ERR_INVALID_ARGUMENT
+    assert lib.parallax_check_bounded_wait((1 << 22) + 1) == px.ERR_INVALID_ARGUMENT
+    lib.parallax_clear_error()

@@ -126,6 +126,130 @@ def test_segmented_copy_if(lib, px, ox, dev, t, layout, remove):
         assert np.array_equal(got[a:a + k], kept[s]), f"segment {s}"
 
 
+@pytest.mark.parametrize("op", ["max", "min"])
+@pytest.mark.parametrize("t", list(DTYPES))
+@pytest.mark.parametrize("layout", list(LAYOUTS))
+def test_segmented_reduce_max_min(lib, px, ox, dev, t, layout, op):
+    off = LAYOUTS[layout]
+    S = off.size - 1
+    x = make(ox, t, int(off[-1]), seed=13)
+    d, o = dev.put(x), dev.put(off)
+    r = dev.empty(max(S, 1) * x.itemsize)
+    lib.parallax_segmented_reduce(px.builtin(f"reduce:{op}:{t}"), d.data_ptr(), x.size,
+                                  o.data_ptr(), S, r.data_ptr())
+    px.check("segmented max/min")
+    got = dev.get(r, x.dtype, S)
+    for s_ in range(S):
+        a, b = int(off[s_]), int(off[s_ + 1])
+        want = ox.reduce_minmax(x[a:b], op == "max") if b > a else x.dtype.type(0)
+        assert got[s_] == want, (s_, got[s_], want)
+
+
+@pytest.mark.parametrize("t", list(DTYPES))
+@pytest.mark.parametrize("layout", list(LAYOUTS))
+def test_segmented_inclusive_scan(lib, px, ox, dev, t, layout):
+    off = LAYOUTS[layout]
+    x = make(ox, t, int(off[-1]), seed=14)
+    d, o = dev.put(x), dev.put(off)
+    out = dev.empty(x.nbytes)
+    lib.parallax_segmented_inclusive_scan(px.builtin(f"scan:{t}"), d.data_ptr(), out.data_ptr(),
+                                          x.size, o.data_ptr(), off.size - 1)
+    px.check("segmented inclusive scan")
+    got = dev.get(out, x.dtype, x.size)
+    fp = t in ("f32", "f64")
+    want = np.zeros(x.size, np.float64 if fp else x.dtype)
+    for s_ in range(off.size - 1):
+        a, b = int(off[s_]), int(off[s_ + 1])
+        if b > a:
+            want[a:b] = ox.scan(x[a:b])
+    if fp:
+        assert cases_rel(got, want) <= tol(t)
+    else:
+        assert np.array_equal(got, want)
+
+
+def seg_compact(lib, px, dev, fn, spec, x, off):
+    S = off.size - 1
+    d, o = dev.put(x), dev.put(off)
+    out = dev.put(np.full(x.nbytes, 0xAB, dtype=np.uint8)) if x.size else dev.empty(8)
+    cnt = dev.empty(max(S, 1) * 8)
+    cnt.fill_(0xFF)
+    dev.torch.cuda.synchronize()
+    getattr(lib, fn)(px.builtin(spec), d.data_ptr(), out.data_ptr(), x.size, o.data_ptr(), S,
+                     cnt.data_ptr())
+    px.check(fn)
+    return dev.get(out, x.dtype, x.size), dev.get(cnt, np.uint64, S)
+
+
+@pytest.mark.parametrize("t,m,r", [("i32", 3, 0), ("i32", 7, -2), ("u32", 5, 1), ("i64", 3, 0),
+                                   ("u64", 10, 3)])
+@pytest.mark.parametrize("layout", ["tile_edges", "big_and_small", "lognormal", "mixed_empty"])
+def test_segmented_copy_if_modulo(lib, px, ox, dev, t, m, r, layout):
+    off = LAYOUTS[layout]
+    x = make(ox, t, int(off[-1]), seed=15)
+    got, counts = seg_compact(lib, px, dev, "parallax_segmented_copy_if",
+                              f"copy_if:{t}:mod:{m}:{r}", x, off)
+    for s_ in range(off.size - 1):
+        a, b = int(off[s_]), int(off[s_ + 1])
+        want, wk = ox.compact(x[a:b], ox.COPY_IF, ox.P_MOD, 0.0, m, r)
+        assert counts[s_] == wk and np.array_equal(got[a:a + wk], want[:wk]), s_
+
+
+@pytest.mark.parametrize("t", list(DTYPES))
+@pytest.mark.parametrize("layout", list(LAYOUTS))
+def test_segmented_partition(lib, px, ox, dev, t, layout):
+    off = LAYOUTS[layout]
+    x = make(ox, t, int(off[-1]), seed=16)
+    pk, c = PREDS[t]
+    got, counts = seg_compact(lib, px, dev, "parallax_segmented_partition",
+                              f"partition:{t}:{pk}:{c}", x, off)
+    for s_ in range(off.size - 1):
+        a, b = int(off[s_]), int(off[s_ + 1])
+        want, wk = ox.compact(x[a:b], ox.PARTITION, PK[pk], c)
+        assert counts[s_] == wk, s_
+        assert np.array_equal(got[a:b], want), s_
+
+
+@pytest.mark.parametrize("t", list(DTYPES))
+@pytest.mark.parametrize("layout", list(LAYOUTS))
+def test_segmented_unique(lib, px, ox, dev, t, layout):
+    off = LAYOUTS[layout]
+    x = make(ox, t, int(off[-1]), seed=17)
+    # runs of equal values inside every segment (sorted per segment, values coarsened)
+    x = (x // x.dtype.type(97)) if t not in ("f32", "f64") else np.round(x * 40).astype(x.dtype)
+    x = ox.seg_sort(x, off)
+    got, counts = seg_compact(lib, px, dev, "parallax_segmented_unique", f"unique:{t}", x, off)
+    for s_ in range(off.size - 1):
+        a, b = int(off[s_]), int(off[s_ + 1])
+        want, wk = ox.compact(x[a:b], ox.UNIQUE)
+        assert counts[s_] == wk and np.array_equal(got[a:a + wk], want[:wk]), s_
+
+
+@pytest.mark.parametrize("shift", [1, 2, 3])
+def test_segmented_unaligned_arrays(lib, px, ox, dev, shift):
+    """Input and output arrays that start off a 16-byte boundary (and at different phases
+    from each other): tiles are staged at their own phase and stored element by element
+    when the phases differ."""
+    off = LAYOUTS["lognormal"]
+    n = int(off[-1])
+    x = make(ox, "i32", n, seed=18)
+    buf = dev.put(np.concatenate([np.zeros(shift, np.int32), x]))
+    o = dev.put(off)
+    out = dev.empty((n + 4) * 4)
+    lib.parallax_segmented_inclusive_scan(px.builtin("scan:i32"), buf.data_ptr() + 4 * shift,
+                                          out.data_ptr() + 4, n, o.data_ptr(), off.size - 1)
+    px.check("unaligned segmented scan")
+    got = out[4: 4 + n * 4].cpu().numpy().view(np.int32)
+    want = np.concatenate([ox.scan(x[int(off[i]):int(off[i + 1])]) for i in range(off.size - 1)
+                           if off[i + 1] > off[i]])
+    assert np.array_equal(got, want)
+    r = dev.empty((off.size - 1) * 4)
+    lib.parallax_segmented_reduce(px.builtin("reduce:sum:i32"), buf.data_ptr() + 4 * shift, n,
+                                  o.data_ptr(), off.size - 1, r.data_ptr())
+    px.check("unaligned segmented reduce")
+    assert np.array_equal(dev.get(r, np.int32, off.size - 1), ox.seg_sum(x, off))
+
+
 @pytest.mark.parametrize("t", list(DTYPES))
 @pytest.mark.parametrize("layout", list(LAYOUTS))
 def test_segmented_sort(lib, px, ox, dev, t, layout):
@@ -200,7 +324,7 @@ def test_many_calls_with_different_shapes(lib, px, ox, dev):
 
 
 def test_device_resident_arena_operands(lib, px, ox):
-    from test_gpu_abi import Arena
+    from helpers import Arena
     arena = Arena(lib)
     try:
         off = LAYOUTS["tile_edges"]
@@ -254,14 +378,20 @@ def test_rejects_host_and_coherent_operands(lib, px, ox):
 def test_rejects_wrong_handles(lib, px, dev):
     off = dev.put(cases.offsets_of([3, 4]))
     x = dev.put(np.arange(7, dtype=np.float32))
-    r = dev.empty(8)
-    assert lib.parallax_segmented_reduce(px.builtin("reduce:max:f32"), x.data_ptr(), 7,
+    r = dev.empty(64)
+    assert lib.parallax_segmented_reduce(px.builtin("sort:f32"), x.data_ptr(), 7,
                                          off.data_ptr(), 2, r.data_ptr()) == px.ERR_INVALID_HANDLE
     assert lib.parallax_segmented_sort(px.builtin("reduce:sum:f32"), x.data_ptr(), 7,
                                        off.data_ptr(), 2) == px.ERR_INVALID_HANDLE
-    assert lib.parallax_segmented_copy_if(px.builtin("copy_if:i32:mod:3:0"), x.data_ptr(),
+    assert lib.parallax_segmented_copy_if(px.builtin("scan:f32"), x.data_ptr(),
                                           r.data_ptr(), 7, off.data_ptr(), 2,
                                           r.data_ptr()) == px.ERR_INVALID_HANDLE
+    assert lib.parallax_segmented_partition(px.builtin("copy_if:f32:gt:0"), x.data_ptr(),
+                                            r.data_ptr(), 7, off.data_ptr(), 2,
+                                            r.data_ptr()) == px.ERR_INVALID_HANDLE
+    assert lib.parallax_segmented_unique(px.builtin("copy_if:f32:gt:0"), x.data_ptr(),
+                                         r.data_ptr(), 7, off.data_ptr(), 2,
+                                         r.data_ptr()) == px.ERR_INVALID_HANDLE
     lib.parallax_clear_error()
 
 
@@ -312,7 +442,8 @@ def test_tuner_cache_is_written_and_reused(tmp_path):
     assert r1.returncode == 0, r1.stderr[-2000:]
     assert "tuned segmented op 0" in r1.stderr
     entries = [ln.split() for ln in cache.read_text().splitlines() if ln.strip()]
-    assert entries and all(len(e) == 4 and e[3] in ("4", "8", "16") for e in entries)
+    assert entries and all(len(e) == 5 and e[3] in ("256", "512") and e[4] in ("3", "7")
+                           for e in entries)
     r2 = subprocess.run([sys.executable, str(script), pkg], env=env, capture_output=True,
                         text=True, timeout=300)
     assert r2.returncode == 0, r2.stderr[-2000:]
