@@ -154,10 +154,10 @@ int parallax_scan_noalloc(parallax_kernel_t scan_kernel, const void* input, void
 
 /* ---- serving loop (continuous batching) --------------------------------------------
  * No counterpart in the reference (its calls are synchronous, one at a time, and not
- * thread-safe: src/kernel/kernel_launcher.hpp:172-176). A scheduler thread takes requests
- * from any number of host threads, admits them in arrival order while the in-flight byte
- * budget and the arena (for sort temporaries) allow, coalesces queued requests of the same
- * kind into one segmented launch over per-request descriptors, and overlaps `lanes` such
+ * thread-safe: src/kernel/kernel_launcher.hpp:172-176). Scheduler threads take requests
+ * from any number of host threads, admit them in arrival order while the in-flight byte
+ * budget and the arena (for sort temporaries) allow, coalesce queued requests of the same
+ * kind into one segmented launch over per-request descriptors, and overlap `lanes` such
  * batches on the device. Operands stay where they are: PARALLAX_DEVICE_RESIDENT arena
  * blocks or device memory. A request's result does not depend on what it was batched with
  * (integers bit-exact; floating point within the primitives' tolerance). */
@@ -168,6 +168,9 @@ typedef struct parallax_serve_config {
                                 radix path (from 2^16 4-byte / 2^19 8-byte keys) always do */
     uint64_t inflight_bytes; /* admission budget: operand + temporary bytes of admitted,
                                 unfinished requests (0: half the arena capacity) */
+    uint32_t schedulers;     /* host threads that form and launch batches, each owning an
+                                equal share of the lanes (0: 4, at most `lanes`) */
+    uint32_t reserved;       /* 0 */
 } parallax_serve_config;
 
 #define PARALLAX_REQ_EXCLUSIVE 1u /* scan: exclusive with `init` (else inclusive) */

@@ -48,7 +48,8 @@ u64 = C.c_uint64
 class ServeConfig(C.Structure):
     """parallax_serve_config"""
     _fields_ = [("lanes", C.c_uint32), ("max_batch", C.c_uint32),
-                ("solo_elements", C.c_uint64), ("inflight_bytes", C.c_uint64)]
+                ("solo_elements", C.c_uint64), ("inflight_bytes", C.c_uint64),
+                ("schedulers", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class Request(C.Structure):

@@ -6,8 +6,9 @@
 //
 // Clients submit requests (reduce / scan / sort / copy_if over operands already resident on
 // the device: PARALLAX_DEVICE_RESIDENT arena blocks or device memory) from any number of
-// threads. One scheduler thread owns `lanes` independent device lanes (a workspace each:
-// stream, scratch, descriptor table, pinned result slots) and keeps them busy:
+// threads. `schedulers` host threads share one arrival queue; each owns an equal share of
+// `lanes` independent device lanes (a workspace each: stream, scratch, descriptor table,
+// pinned result slots) and keeps them busy:
 //   * completion: a lane whose batch finished (event query) hands every request its result
 //     and releases the request's admitted bytes and arena temporaries;
 //   * admission: requests are taken in arrival order while the in-flight byte budget
@@ -64,11 +65,13 @@ struct Request {
     uint64_t footprint = 0;    // admitted bytes (operands + temporaries)
     void* tmp = nullptr;       // sort temporary: arena block (host-side address)
     bool coalescible = false;
-    // completion: the finisher sets done under m and notifies while holding it, so the
-    // waiter (which then deletes the request) never races the notification
+    // completion: the finisher sets done under m and notifies while holding it, then sets
+    // `released` as its very last access to the request; the waiter (which deletes the
+    // request afterwards) returns only once `released` is set
     int status = PARALLAX_OK;
     uint64_t done_ns = 0;
     bool done = false;
+    std::atomic<bool> released{false};
     std::mutex m;
     std::condition_variable cv;
 };
@@ -76,15 +79,26 @@ struct Request {
 void finish(Request* r, int status) {
     r->status = status;
     r->done_ns = now_ns();
-    std::lock_guard<std::mutex> g(r->m);
-    r->done = true;
-    r->cv.notify_one();
+    {
+        std::lock_guard<std::mutex> g(r->m);
+        r->done = true;
+        r->cv.notify_one();
+    }
+    r->released.store(true, std::memory_order_release);
 }
 
-// Blocks until the request has been finished; returns its status.
+// Blocks until the request has been finished; returns its status. Short requests finish
+// within microseconds of their launch, so the waiter first polls the completion flag for a
+// few microseconds (no sleep / wake-up latency), then sleeps on the condition variable.
 int wait_request(Request* r, uint64_t* done_ns) {
-    std::unique_lock<std::mutex> lk(r->m);
-    r->cv.wait(lk, [&] { return r->done; });
+    constexpr int kPolls = 4000;
+    for (int i = 0; i < kPolls && !r->released.load(std::memory_order_acquire); ++i)
+        __builtin_ia32_pause();
+    if (!r->released.load(std::memory_order_acquire)) {
+        std::unique_lock<std::mutex> lk(r->m);
+        r->cv.wait(lk, [&] { return r->done; });
+    }
+    while (!r->released.load(std::memory_order_acquire)) std::this_thread::yield();
     if (done_ns) *done_ns = r->done_ns;
     return r->status;
 }
@@ -112,7 +126,7 @@ class Server {
   public:
     parallax_serve_config cfg{};
     std::vector<Lane> lanes;
-    std::thread thr;
+    std::vector<std::thread> thr;
     std::mutex mu;
     std::condition_variable cv_sched;
     std::deque<Request*> queue;
@@ -126,6 +140,8 @@ class Server {
         if (cfg.max_batch == 0) cfg.max_batch = 1024;
         if (cfg.solo_elements == 0) cfg.solo_elements = 1ull << 18;
         if (cfg.inflight_bytes == 0) cfg.inflight_bytes = parallax_arena_capacity() / 2;
+        if (cfg.schedulers == 0) cfg.schedulers = 4;
+        if (cfg.schedulers > cfg.lanes) cfg.schedulers = cfg.lanes;
         lanes.resize(cfg.lanes);
         for (Lane& l : lanes) {
             l.ws = new_workspace();
@@ -140,7 +156,12 @@ class Server {
                 !cuda_ok(cudaHostGetDevicePointer((void**)&l.d_res, l.h_res, 0), "serve results"))
                 return false;
         }
-        thr = std::thread([this] { loop(); });
+        // scheduler i owns lanes [i * L / N, (i + 1) * L / N); all take work from one queue
+        for (uint32_t i = 0; i < cfg.schedulers; ++i) {
+            const size_t lo = (size_t)i * lanes.size() / cfg.schedulers;
+            const size_t hi = (size_t)(i + 1) * lanes.size() / cfg.schedulers;
+            thr.emplace_back([this, lo, hi] { loop(lo, hi); });
+        }
         return true;
     }
 
@@ -161,8 +182,9 @@ class Server {
             std::lock_guard<std::mutex> g(mu);
             stopping = true;
         }
-        cv_sched.notify_one();
-        if (thr.joinable()) thr.join();
+        cv_sched.notify_all();
+        for (std::thread& t : thr)
+            if (t.joinable()) t.join();
     }
 
   private:
@@ -299,12 +321,13 @@ class Server {
         l.busy = false;
     }
 
-    void loop() {
+    void loop(size_t lo, size_t hi) {
         ensure_device();
         for (;;) {
             bool progress = false;
             bool any_busy = false;
-            for (Lane& l : lanes) {
+            for (size_t li = lo; li < hi; ++li) {
+                Lane& l = lanes[li];
                 if (!l.busy) continue;
                 const cudaError_t e = cudaEventQuery(l.done);
                 if (e == cudaErrorNotReady) {
@@ -316,7 +339,8 @@ class Server {
                 progress = true;
             }
             std::unique_lock<std::mutex> lk(mu);
-            for (Lane& l : lanes) {
+            for (size_t li = lo; li < hi; ++li) {
+                Lane& l = lanes[li];
                 if (l.busy || queue.empty()) continue;
                 std::vector<Request*> b = form_batch();
                 if (b.empty()) break;
@@ -343,7 +367,7 @@ class Server {
             }
             if (stopping && queue.empty() && !any_busy) {
                 bool busy = false;
-                for (Lane& l : lanes) busy |= l.busy;
+                for (size_t li = lo; li < hi; ++li) busy |= lanes[li].busy;
                 if (!busy) break;
             }
             if (progress) continue;
@@ -474,6 +498,7 @@ PXB_EXPORT int parallax_serve_submit(const parallax_request* req, uint64_t* tick
             memset(r->result, 0, r->op == ReqOp::REDUCE ? r->es : 8);
         r->done = true;
         r->done_ns = now_ns();
+        r->released.store(true, std::memory_order_release);
     } else {
         s->submit(r);
     }
