@@ -69,11 +69,13 @@ def compile_one(src: Path, newest_header: float, force: bool, extra: list[str]) 
 
 
 def build(force: bool = False, jobs: int | None = None, verbose: bool = False,
-          ptxas_verbose: bool = False) -> Path:
+          ptxas_verbose: bool = False, defines: list[str] | None = None) -> Path:
     BUILD.mkdir(exist_ok=True)
     LIB_DIR.mkdir(exist_ok=True)
     newest_header = max((h.stat().st_mtime for h in headers()), default=0.0)
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+    extra += [f"-D{d}" for d in (defines or [])]
+    force = force or bool(defines)
     srcs = sources()
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
     with cf.ThreadPoolExecutor(jobs) as ex:
@@ -121,8 +123,12 @@ def main() -> None:
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--jobs", type=int, default=None)
     ap.add_argument("--ptxas-verbose", action="store_true")
+    ap.add_argument("-D", dest="defines", action="append", default=[],
+                    help="preprocessor definition for every CUDA source (forces a rebuild), "
+                         "e.g. -D PXB_SCAN_VPT=5 to build a different scan tile shape")
     a = ap.parse_args()
-    print(build(force=a.force, jobs=a.jobs, verbose=True, ptxas_verbose=a.ptxas_verbose))
+    print(build(force=a.force, jobs=a.jobs, verbose=True, ptxas_verbose=a.ptxas_verbose,
+                defines=a.defines))
 
 
 if __name__ == "__main__":

@@ -31,9 +31,24 @@
 namespace pxb {
 namespace {
 
-constexpr int kBlock = 512;  // tile shape as in scan.cu (measured: 112 KiB tiles, 2 CTAs/SM)
-constexpr int kVpt = 7;
-constexpr int kSub = 2;
+// Tile shape (measured: 112 KiB tiles, 2 CTAs/SM); can be overridden at build time
+// (PXB_COMPACT_BLOCK / _VPT / _SUB / _CTAS) to sweep it; kSub x (kBlock / 32) must be 32.
+#ifndef PXB_COMPACT_BLOCK
+#define PXB_COMPACT_BLOCK 512
+#endif
+#ifndef PXB_COMPACT_VPT
+#define PXB_COMPACT_VPT 7
+#endif
+#ifndef PXB_COMPACT_SUB
+#define PXB_COMPACT_SUB 2
+#endif
+#ifndef PXB_COMPACT_CTAS
+#define PXB_COMPACT_CTAS 2
+#endif
+constexpr int kBlock = PXB_COMPACT_BLOCK;
+constexpr int kVpt = PXB_COMPACT_VPT;
+constexpr int kSub = PXB_COMPACT_SUB;
+constexpr int kCtasPerSm = PXB_COMPACT_CTAS;
 
 template <typename T>
 struct Shape {
@@ -293,7 +308,7 @@ __device__ __forceinline__ void compact_tile(T* buf, uint64_t* bars, uint32_t pa
 
 // One CTA per tile, in blockIdx order (unaligned input).
 template <typename T, int MODE, bool BULK>
-__global__ void __launch_bounds__(kBlock, 2)
+__global__ void __launch_bounds__(kBlock, kCtasPerSm)
 k_compact(const T* in, T* out, uint64_t n, PredDev<T> pred, TileStatus<uint64_t> ts,
           const unsigned long long* __restrict__ num_true,
           unsigned long long* __restrict__ count_out) {

@@ -37,8 +37,23 @@ namespace {
 // Tile shape, chosen by measurement on B200 (2^28 elements): 112 KiB tiles at two CTAs per
 // SM beat 48 KiB tiles at four per SM by 8-10 % (the look-back's fixed latency is paid per
 // tile), and 16 KiB or 80 KiB tiles were slower still.
-constexpr int kBlock = 512;
-constexpr int kVpt = 7;  // 16-byte vectors per thread; odd => conflict-free row reads
+// The shape can be overridden at build time (PXB_SCAN_BLOCK / _VPT / _SUB / _CTAS) to sweep
+// it; kSub x (kBlock / 32) must be 32.
+#ifndef PXB_SCAN_BLOCK
+#define PXB_SCAN_BLOCK 512
+#endif
+#ifndef PXB_SCAN_VPT
+#define PXB_SCAN_VPT 7
+#endif
+#ifndef PXB_SCAN_SUB
+#define PXB_SCAN_SUB 2
+#endif
+#ifndef PXB_SCAN_CTAS
+#define PXB_SCAN_CTAS 2
+#endif
+constexpr int kBlock = PXB_SCAN_BLOCK;
+constexpr int kVpt = PXB_SCAN_VPT;  // 16-byte vectors per thread; odd => conflict-free row reads
+constexpr int kCtasPerSm = PXB_SCAN_CTAS;
 
 template <typename T> struct ScanTypes;
 template <> struct ScanTypes<float> { using L = float; using A = double; };
@@ -48,7 +63,7 @@ template <> struct ScanTypes<uint32_t> { using L = uint32_t; using A = uint32_t;
 template <> struct ScanTypes<int64_t> { using L = uint64_t; using A = uint64_t; };
 template <> struct ScanTypes<uint64_t> { using L = uint64_t; using A = uint64_t; };
 
-constexpr int kSub = 2;   // sub-tiles per look-back tile; kSub x 16 warps = 32 lanes
+constexpr int kSub = PXB_SCAN_SUB;  // sub-tiles per look-back tile; kSub x warps = 32 lanes
 
 template <typename T>
 struct ScanShape {
@@ -177,7 +192,7 @@ __device__ __forceinline__ void scan_tile(T* buf, uint64_t* bars, uint32_t parit
 // overlap its tiles) passes each chunk's first tile, and every chunk shares one look-back
 // epoch, so the first tile of a chunk looks back into the chunks before it.
 template <typename T, bool EXCL, bool BULK>
-__global__ void __launch_bounds__(kBlock, 2)
+__global__ void __launch_bounds__(kBlock, kCtasPerSm)
 k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan)
        typename ScanTypes<T>::A init, TileStatus<typename ScanTypes<T>::A> ts, uint64_t tile0) {
     using A = typename ScanTypes<T>::A;

@@ -51,7 +51,6 @@ struct TileStatus {
     uint32_t epoch;
     volatile int32_t* err;
     uint32_t limit = kSpinLimit;  // polls of one predecessor before the wait gives up
-    bool near_first = false;      // EXPERIMENT: warp-first round (PARALLAX_LB_NEAR)
 };
 
 // Poll limit of the look-back waits launched from now on: kSpinLimit, or the smaller
@@ -129,7 +128,8 @@ __device__ __forceinline__ uint32_t poll_status(const TileStatus<A>& ts, int64_t
 // segmented kernels): that tile publishes its inclusive prefix at once, and indices below
 // it are never polled.
 // NEAR_FIRST: warp 0 alone inspects the 32 nearest predecessors first, and the CTA-wide
-// rounds run only when none of them holds an inclusive prefix.
+// rounds run only when none of them holds an inclusive prefix (measured on B200 with the
+// 16-byte entries: 2^28-element scans 0-5 % faster than CTA-wide rounds from the start).
 template <typename A, int BLOCK, bool NEAR_FIRST = false>
 __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile, A agg, A* red,
                                           int* first, uint64_t lo = 0) {
@@ -143,7 +143,7 @@ __device__ __forceinline__ A lookback_cta(const TileStatus<A>& ts, uint64_t tile
     if (tid == 0) publish(&ts.e[tile], ep, 1u, agg);
     A excl = A(0);
     int64_t pred = (int64_t)tile - 1;
-    if (NEAR_FIRST && ts.near_first) {
+    if constexpr (NEAR_FIRST) {
         if (warp == 0) {
             const int64_t idx = pred - lane;
             A v = A(0);
@@ -202,8 +202,6 @@ inline TileStatus<A> tile_status_at(char* scratch, uint32_t epoch, int32_t* err)
     ts.epoch = epoch;
     ts.err = err;
     ts.limit = wait_limit();
-    static const bool near = getenv("PARALLAX_LB_NEAR") != nullptr;
-    ts.near_first = near;
     return ts;
 }
 
