@@ -170,23 +170,22 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     // each key's rank within its stream, at the key's tile position (kept out of registers)
     uint16_t* const s_rank = reinterpret_cast<uint16_t*>(s_wh + TABLES * kBins);
     __shared__ uint64_t s_goff[kBins];
-    __shared__ uint32_t s_loc[kBins];
+    __shared__ uint32_t s_goff32[kBins];
     __shared__ uint64_t s_part64[kBins / 32];
     __shared__ uint32_t s_part32[kBins / 32];
     __shared__ uint32_t s_tile;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_tile = atomicAdd(&counters[0], 1u);
-    // count table of stream s of this warp: wh + s * kBins; its lane-mask table: mm + s * kBins
+    // offsets of stream s of this warp in the tile, per digit (filled in step 3a): wh + s * kBins
     uint32_t* const wh = s_wh + warp * kSubs * kBins;
-    // the ranking's lane-mask tables borrow the key buffer, which is free until step 4a
-    static_assert((size_t)TILE * sizeof(K) >= (size_t)TABLES * kBins * 4, "mask tables fit");
-    uint32_t* const mm = reinterpret_cast<uint32_t*>(s_keys) + warp * kSubs * kBins;
+    // the ranking's tables borrow the key buffer, which is free until step 4a: one 64-bit
+    // word per (stream, digit), high half the stream's running count of the digit, low half
+    // the lane mask of the current item's peers, so one load reads both
+    static_assert((size_t)TILE * sizeof(K) >= (size_t)TABLES * kBins * 8, "rank tables fit");
+    uint64_t* const wm = reinterpret_cast<uint64_t*>(s_keys) + warp * kSubs * kBins;
 #pragma unroll
-    for (int i = lane; i < kSubs * kBins; i += 32) {
-        wh[i] = 0u;
-        mm[i] = 0u;
-    }
+    for (int i = lane; i < kSubs * kBins; i += 32) wm[i] = 0ull;
     __syncthreads();
     const uint64_t tile = s_tile;
     if (tile >= tiles) {  // claim counter out of step: touch nothing
@@ -217,10 +216,12 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
 
     // 2. stable warp-level ranking by the current digit. Lanes holding the same digit find
     // each other through a per-stream table of 256 lane masks (shared-memory atomic OR of
-    // the lane's bit, read back, cleared by the group's highest lane); a key's rank is the
-    // stream's running count of its digit plus its lower peers, and the highest peer
-    // advances the count. This keeps the ranking off the SM's narrow branch unit (where match-any
-    // issues) and off the ALU (eight ballots per key cost more than the whole pass).
+    // the lane's bit into the low half of the digit's word, read back together with the
+    // count in the high half, then the group's highest lane writes count + peers with a
+    // cleared mask); a key's rank is the stream's running count of its digit plus its lower
+    // peers. This keeps the ranking off the SM's narrow branch unit (where match-any issues)
+    // and off the ALU (eight ballots per key cost more than the whole pass), with three
+    // shared-memory accesses per key.
     static_assert(32 * STREAM_ITEMS <= 0xffff, "ranks fit 16 bits");
 
     const uint32_t lt = lanemask_lt();
@@ -231,22 +232,19 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
             d[t] = digit_of(k[t * STREAM_ITEMS + j], shift) + t * kBins;
-            atomicOr(&mm[d[t]], 1u << lane);
+            atomicOr(reinterpret_cast<uint32_t*>(&wm[d[t]]), 1u << lane);  // low half
         }
         __syncwarp();
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
-            peers[t] = mm[d[t]];
-            c[t] = wh[d[t]] + __popc(peers[t] & lt);
+            const uint64_t v = wm[d[t]];
+            peers[t] = (uint32_t)v;
+            c[t] = (uint32_t)(v >> 32) + __popc(peers[t] & lt);
         }
         __syncwarp();
 #pragma unroll
-        for (int t = 0; t < kSubs; ++t) {
-            if ((peers[t] & ~le) == 0) {  // the highest peer
-                wh[d[t]] = c[t] + 1;
-                mm[d[t]] = 0u;
-            }
-        }
+        for (int t = 0; t < kSubs; ++t)
+            if ((peers[t] & ~le) == 0) wm[d[t]] = (uint64_t)(c[t] + 1) << 32;  // the highest peer
         __syncwarp();
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
@@ -257,12 +255,14 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     __syncthreads();
 
     // 3a. per digit: counts of the streams -> exclusive over streams (in key order); tile
-    // count; publish AGG
+    // count; publish AGG. Then the digit's start in the tile is added to every stream's
+    // offset, so step 4a finds a key's slot with one table read.
     uint32_t cnt = 0;
     if (tid < kBins) {
+        const uint64_t* const all = reinterpret_cast<const uint64_t*>(s_keys);
 #pragma unroll 8
         for (int w = 0; w < TABLES; ++w) {
-            const uint32_t c = s_wh[w * kBins + tid];
+            const uint32_t c = (uint32_t)(all[w * kBins + tid] >> 32);
             s_wh[w * kBins + tid] = cnt;
             cnt += c;
         }
@@ -275,7 +275,10 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     if (tile == 0)
         start = digit_exclusive_scan<uint64_t, BLOCK>(tid < kBins ? (uint64_t)hist[tid] : 0ull,
                                                       s_part64);
-    if (tid < kBins) s_loc[tid] = loc;
+    if (tid < kBins) {
+#pragma unroll 8
+        for (int w = 0; w < TABLES; ++w) s_wh[w * kBins + tid] += loc;
+    }
     __syncthreads();
 
     // 4a. keys in digit order in shared memory
@@ -283,7 +286,7 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     for (int i = 0; i < ITEMS; ++i) {
         const uint32_t r = s_rank[w0 + 32 * i];
         const uint32_t d = digit_of(k[i], shift);
-        s_keys[s_loc[d] + wh[(i / STREAM_ITEMS) * kBins + d] + r] = k[i];
+        s_keys[wh[(i / STREAM_ITEMS) * kBins + d] + r] = k[i];
     }
 
     // 3b. look-back, one thread per digit. The words of the kLookWindow nearest unvisited
@@ -320,17 +323,22 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
         }
         st_relaxed_u64(&status[tile * kBins + tid],
                        ((uint64_t)epoch << kEpochShift) | kStInc | ((excl + cnt) & kValMask));
-        s_goff[tid] = excl - loc;  // output position of tile-sorted index x: s_goff[d] + x
+        // output position of tile-sorted index x: goff[d] + x (excl >= loc always)
+        s_goff[tid] = excl - loc;
+        s_goff32[tid] = (uint32_t)(excl - loc);
     }
     __syncthreads();
 
-    // 4b. each digit's run to its global offset
+    // 4b. each digit's run to its global offset (32-bit offsets when they fit: one
+    // shared-memory wavefront per 32 keys instead of two)
+    const bool off32 = n <= 0xffffffffull;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const uint32_t x = (uint32_t)j * BLOCK + tid;
         if (x < valid) {
             const K key = s_keys[x];
-            const uint64_t pos = s_goff[digit_of(key, shift)] + x;
+            const uint32_t d = digit_of(key, shift);
+            const uint64_t pos = off32 ? (uint64_t)(s_goff32[d] + x) : s_goff[d] + x;
             if (pos < n) out[pos] = from_key<K, XF_OUT>(key);
             else *err = kErrRadixRange;
         }

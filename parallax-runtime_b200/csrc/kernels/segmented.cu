@@ -80,9 +80,18 @@ struct SegShape {
 };
 
 // Device buffers of one segmented launch (the workspace's segment and status buffers).
+// Everything a CTA needs to find its tile, precomputed per work item (48 bytes, read with
+// three 16-byte loads), so claiming an item costs one load after the claim, not a chain of
+// dependent loads (item -> segment -> segment bounds -> addresses).
+struct __align__(16) ItemDesc {
+    uint32_t seg, first_item, seg_items, k;  // segment, its first item and item count, k = item - first
+    uint64_t len, in, out, aux;              // segment length and addresses
+};
+static_assert(sizeof(ItemDesc) == 48, "item descriptor layout");
+
 struct SegBuffers {
     uint32_t* item_start;  // num_segments + 1
-    uint32_t* item_seg;    // one per work item: its segment
+    ItemDesc* items;       // one per work item
     uint32_t* tickets;     // num_segments, zeroed by the planner
     uint64_t* partials;    // one per work item
     StatusEntry* status;   // one per work item (a buffer of its own)
@@ -141,25 +150,36 @@ struct SegArgs {
     SegPred<T> pred;
 };
 
-// Claimed work item and where its tile lives; thread 0 fills it (prefetched one item
-// ahead), every thread reads it from shared memory.
-struct ItemInfo {
-    uint32_t item, seg, first_item, seg_items;
-    uint64_t len, in, out, aux;
-};
+// Writes the descriptor of every work item (one thread per item, grid-stride): the item's
+// segment is found by binary search over the planner's item_start.
+__global__ void __launch_bounds__(256)
+k_item_descs(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start,
+             ItemDesc* __restrict__ items) {
+    const uint32_t total = item_start[S];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += gridDim.x * blockDim.x) {
+        const uint32_t s = find_segment(item_start, S, i);
+        ItemDesc d;
+        d.seg = s;
+        d.first_item = item_start[s];
+        d.seg_items = item_start[s + 1] - d.first_item;
+        d.k = i - d.first_item;
+        d.len = src.len(s);
+        d.in = src.in_addr(s);
+        d.out = src.out_addr(s);
+        d.aux = src.aux_addr(s);
+        items[i] = d;
+    }
+}
 
-__device__ __forceinline__ void load_item(ItemInfo& it, const SegSrc& src, const SegBuffers& b,
-                                          uint32_t total, uint32_t item) {
-    it.item = item;
-    if (item >= total) return;
-    const uint32_t seg = __ldg(&b.item_seg[item]);
-    it.seg = seg;
-    it.first_item = __ldg(&b.item_start[seg]);
-    it.seg_items = __ldg(&b.item_start[seg + 1]) - it.first_item;
-    it.len = src.len(seg);
-    it.in = src.in_addr(seg);
-    it.out = src.out_addr(seg);
-    it.aux = src.aux_addr(seg);
+__device__ __forceinline__ ItemDesc load_desc(const ItemDesc* items, uint32_t i) {
+    const uint4* p = reinterpret_cast<const uint4*>(items + i);
+    uint4 w[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) w[q] = __ldg(p + q);
+    ItemDesc d;
+    memcpy(&d, w, sizeof d);
+    return d;
 }
 
 // Stages tile elements [begin, begin + len) of `in` so that slot e + mis holds element e
@@ -280,7 +300,8 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
     __shared__ int first[WARPS];
     __shared__ uint32_t wcnt[WARPS];
     __shared__ uint32_t wcnt2[WARPS];
-    __shared__ ItemInfo s_it;
+    __shared__ ItemDesc s_it;
+    __shared__ uint32_t s_item;
     __shared__ T s_prev;
     __shared__ bool s_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -294,17 +315,34 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
     tsk.epoch = b.counters[2];
     tsk.err = err;
 
-    ItemInfo next;  // thread 0: the next item, claimed and described one tile ahead
-    if (tid == 0) load_item(next, a.src, b, total, atomicAdd(&b.counters[0], 1u));
+    // Thread 0's two-stage pipeline: the item for the next tile is claimed two tiles ahead
+    // and its descriptor loaded one tile ahead, so no iteration waits on its own loads.
+    // Claims are made in order, so the lowest unfinished item is always the one its CTA is
+    // working on, and every look-back wait ends.
+    uint32_t c_next = 0, c_after = 0;
+    ItemDesc d_next;
+    if (tid == 0) {
+        c_next = atomicAdd(&b.counters[0], 1u);
+        c_after = atomicAdd(&b.counters[0], 1u);
+        if (c_next < total) d_next = load_desc(b.items, c_next);
+    }
     for (;;) {
         if (tid == 0) {
-            s_it = next;
-            if (next.item < total) load_item(next, a.src, b, total, atomicAdd(&b.counters[0], 1u));
+            s_item = c_next;
+            if (c_next < total) {
+                s_it = d_next;
+                c_next = c_after;
+                if (c_next < total) {
+                    d_next = load_desc(b.items, c_next);
+                    c_after = atomicAdd(&b.counters[0], 1u);
+                }
+            }
         }
         __syncthreads();
-        const ItemInfo it = s_it;
-        if (it.item >= total) break;
-        const uint32_t k = it.item - it.first_item;  // tile index within the segment
+        const ItemDesc it = s_it;
+        const uint32_t item = s_item;
+        if (item >= total) break;
+        const uint32_t k = it.k;  // tile index within the segment
         const uint64_t begin = (uint64_t)k * TILE;   // within the segment
         const uint32_t len = (uint32_t)min((uint64_t)TILE, it.len - begin);
         const T* in = reinterpret_cast<const T*>(it.in);
@@ -357,8 +395,8 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                 if (tid == 0) write(tot, totm);
             } else {
                 if (tid == 0) {
-                    if (mm) put_val(&b.partials[it.item], totm);
-                    else put_val(&b.partials[it.item], tot);
+                    if (mm) put_val(&b.partials[item], totm);
+                    else put_val(&b.partials[item], tot);
                     __threadfence();
                     s_last = atomicAdd(&b.tickets[it.seg], 1u) == it.seg_items - 1;
                 }
@@ -418,7 +456,7 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                 }
                 __syncthreads();
                 const A prefix =
-                    lookback_cta<A, BLOCK>(ts, it.item, agg, red, first, it.first_item);
+                    lookback_cta<A, BLOCK>(ts, item, agg, red, first, it.first_item);
                 const A tb = (A)a.init + ((prefix + woff) + tex);
                 uint4* row = reinterpret_cast<uint4*>(sm + tid * ITEMS);
 #pragma unroll
@@ -456,7 +494,7 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                 uint32_t kstart;
                 const uint32_t kept = tile_ranks<BLOCK>(__popc(f), wcnt, &kstart);
                 const uint64_t prefix =
-                    lookback_cta<uint64_t, BLOCK>(tsk, it.item, (uint64_t)kept, red64, first,
+                    lookback_cta<uint64_t, BLOCK>(tsk, item, (uint64_t)kept, red64, first,
                                                   it.first_item);
                 if constexpr (OP == SEG_SELECT) {
                     // pack the kept elements at the front of the staged tile, then store
@@ -515,7 +553,7 @@ constexpr int min_tile() {  // the smallest tile of any shape, in elements of T
 // segment buffer (zeroed when it is (re)allocated).
 bool seg_buffers(Workspace& ws, uint64_t S, uint64_t items, SegBuffers* out) {
     const size_t need = 256 + up256((S + 1) * 4) + up256(S * 4) + up256(items * 8) +
-                        up256(items * 4);
+                        up256(items * sizeof(ItemDesc));
     char* p = static_cast<char*>(ws.seg(need));
     out->status = static_cast<StatusEntry*>(ws.seg_status(items));
     if (!p || !out->status) return false;
@@ -528,7 +566,7 @@ bool seg_buffers(Workspace& ws, uint64_t S, uint64_t items, SegBuffers* out) {
     p += up256(S * 4);
     out->partials = reinterpret_cast<uint64_t*>(p);
     p += up256(items * 8);
-    out->item_seg = reinterpret_cast<uint32_t*>(p);
+    out->items = reinterpret_cast<ItemDesc*>(p);
     return true;
 }
 
@@ -602,10 +640,10 @@ bool enqueue_shape(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     auto plan = [&](SegEmpty empty, bool tickets) {
         k_seg_plan<256><<<1, 256, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE, b.item_start,
                                           b.counters, empty, tickets ? b.tickets : nullptr,
-                                          b.status, b.status_cap, err,
-                                          items_cap <= kInlineItems ? b.item_seg : nullptr);
-        if (items_cap > kInlineItems)
-            k_seg_map<256><<<seg_map_grid(c.S), 256, 0, s>>>(b.item_start, c.S, b.item_seg);
+                                          b.status, b.status_cap, err, nullptr);
+        const uint64_t dg = (items_cap + 255) / 256;
+        k_item_descs<<<(unsigned)(dg < 1184 ? dg : 1184), 256, 0, s>>>(c.src, c.S, b.item_start,
+                                                                        b.items);
     };
     switch (c.op) {
         case SEG_REDUCE:
