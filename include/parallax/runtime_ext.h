@@ -169,7 +169,7 @@ typedef struct parallax_serve_config {
     uint64_t inflight_bytes; /* admission budget: operand + temporary bytes of admitted,
                                 unfinished requests (0: half the arena capacity) */
     uint32_t schedulers;     /* host threads that form and launch batches, each owning an
-                                equal share of the lanes (0: 4, at most `lanes`) */
+                                equal share of the lanes (0: 2, at most `lanes`) */
     uint32_t reserved;       /* 0 */
 } parallax_serve_config;
 

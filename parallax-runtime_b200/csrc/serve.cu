@@ -88,12 +88,14 @@ void finish(Request* r, int status) {
 }
 
 // Blocks until the request has been finished; returns its status. Short requests finish
-// within microseconds of their launch, so the waiter first polls the completion flag for a
-// few microseconds (no sleep / wake-up latency), then sleeps on the condition variable.
+// within microseconds of their launch, so the waiter first polls the completion flag for up
+// to 20 us (no sleep / wake-up latency), then sleeps on the condition variable.
 int wait_request(Request* r, uint64_t* done_ns) {
-    constexpr int kPolls = 4000;
-    for (int i = 0; i < kPolls && !r->released.load(std::memory_order_acquire); ++i)
+    const uint64_t poll_until = now_ns() + 20000;
+    for (int i = 1; !r->released.load(std::memory_order_acquire); ++i) {
         __builtin_ia32_pause();
+        if ((i & 63) == 0 && now_ns() > poll_until) break;
+    }
     if (!r->released.load(std::memory_order_acquire)) {
         std::unique_lock<std::mutex> lk(r->m);
         r->cv.wait(lk, [&] { return r->done; });
@@ -140,7 +142,7 @@ class Server {
         if (cfg.max_batch == 0) cfg.max_batch = 1024;
         if (cfg.solo_elements == 0) cfg.solo_elements = 1ull << 18;
         if (cfg.inflight_bytes == 0) cfg.inflight_bytes = parallax_arena_capacity() / 2;
-        if (cfg.schedulers == 0) cfg.schedulers = 4;
+        if (cfg.schedulers == 0) cfg.schedulers = 2;
         if (cfg.schedulers > cfg.lanes) cfg.schedulers = cfg.lanes;
         lanes.resize(cfg.lanes);
         for (Lane& l : lanes) {
