@@ -51,6 +51,12 @@ void parallax_clear_error(void);
  * mod:<m>:<r> (x % m == r, integers) nonzero. The handle of a partition spec is also
  * the partition-scatter handle. Returns NULL on a malformed spec. */
 parallax_kernel_t parallax_builtin_kernel(const char* spec);
+/* 1 when `key` (a stdpar funnel key, e.g. "T parallax::detail::device_reduce(...) [with
+ * T = float; ...]" or one of its ":scan" / ":add" / ... suffixed forms) names a kernel this
+ * runtime provides built in, so a compiler need not register an image for it; 0 when the
+ * key needs a registered image. Answered from the key alone, with or without a device
+ * (parallax_kernel_lookup itself returns NULL when no device is available). */
+int parallax_kernel_resolves(const char* key);
 
 /* ---- arena residency ------------------------------------------------------------- */
 enum parallax_residency {

@@ -18,6 +18,7 @@ extern "C" {
 HID parallax_kernel_t parallax_kernel_lookup(const char*) { return nullptr; }
 HID void parallax_kernel_register(const char*, const unsigned int*, size_t) {}
 HID int parallax_arena_contains(const void*) { return 0; }
+HID int parallax_heap_contains(const void*) { return 0; }
 HID void* parallax_arena_alloc(size_t, size_t) { return nullptr; }
 HID void parallax_arena_free(void*) {}
 static void unreachable(const char* f) {

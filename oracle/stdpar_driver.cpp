@@ -1,12 +1,17 @@
 // Drives the reference's own stdpar funnels (include/parallax/stdpar.hpp, unmodified) on
 // seeded inputs and writes every result to a file. TEST INFRASTRUCTURE ONLY.
 //
-// oracle/Makefile builds it twice from the same source:
+// oracle/Makefile builds it three times from the same source:
 //   _ref/stdpar_driver_gpu   linked against libparallax-runtime.so: fixed funnels (reduce,
 //                            scans, sort, unique) resolve to the built-in sm_100a kernels;
 //                            the functor funnels resolve to the sm_100a images this program
 //                            registers at start-up, the way compiler-emitted registrars do
 //                            (include/parallax/runtime.h:96-103);
+//   _ref/stdpar_driver_heap  the same, also linked with the whole-heap capture shim
+//                            (lib/libparallax-heap.a): every std::vector lives in the heap
+//                            pool, so the funnels find their data in the arena and call the
+//                            runtime on it in place, and a transform may chase pointers
+//                            stored in heap records;
 //   _ref/stdpar_driver_host  linked against abi_stub.cpp, whose lookups all miss: every call
 //                            runs the reference's host fallback.
 // tests/test_gpu_stdpar.py runs both and compares them call by call.
@@ -39,6 +44,17 @@ struct Affine {  // captures: two floats
     void operator()(float& x) const {
         volatile float ax = a * x;  // rounded product, then a rounded sum (no contraction)
         x = ax + b;
+    }
+};
+struct Rec {  // a heap record holding a pointer into another heap array
+    float x;
+    unsigned pad;
+    const float* p;
+};
+struct GatherPlus {  // y = 0 * x + *p (the gather image with no captures: a = 0)
+    float operator()(const Rec& r) const {
+        volatile float ax = 0.0f * r.x;
+        return ax + *r.p;
     }
 };
 struct AffineDefault {  // no captures: x = 2x + 1
@@ -142,6 +158,7 @@ bool register_all(const std::string& dir) {
     const std::string inv = "void parallax::detail::device_invoke(T*, std::size_t, F) [with T = float; F = ";
     const std::string xf = "void parallax::detail::device_transform(const Tin*, Tout*, std::size_t, F) [with Tin = int; Tout = double; F = HalfD";
     const std::string cnt = "long int parallax::detail::device_count_if(const T*, std::size_t, Pred) [with T = float; Pred = GtHalf";
+    const std::string gat = "void parallax::detail::device_transform(const Tin*, Tout*, std::size_t, F) [with Tin = Rec; Tout = float; F = GatherPlus";
     bool ok = true;
     ok &= register_image(dir, cpy + SZ + ":flags", "flags_mod3_i32");
     ok &= register_image(dir, rem + SZ + ":flags", "flags_not_mod3_i32");
@@ -150,6 +167,7 @@ bool register_all(const std::string& dir) {
     ok &= register_image(dir, inv + "AffineDefault" + SZ, "affine_f32");
     ok &= register_image(dir, xf + SZ, "half_i32_to_f64");
     ok &= register_image(dir, cnt + SZ + ":pred", "pred_gt_half_f32");
+    ok &= register_image(dir, gat + SZ, "saxpy_gather_f32");
     return ok;
 }
 
@@ -256,6 +274,24 @@ void run(size_t n) {
         b = launches();
         long cnt = parallax::count_if(P, c.begin(), c.end(), GtHalf{});
         record_scalar("count_if_gt_half_f32" + sfx, b, (uint64_t)cnt);
+    }
+    {  // where the heap lives, and a transform that chases pointers stored in heap records
+        std::vector<float> tgt = f32_unit(28, n);
+        const uint64_t where = (uint64_t)parallax_heap_contains(tgt.data()) |
+                               (uint64_t)parallax_arena_contains(tgt.data()) << 1;
+        record_scalar("heap_capture" + sfx, launches(), where);
+        // Stored pointers mean something on the device only when the heap is captured (the
+        // host fallback follows them anyway); without capture the call is left out.
+        const bool host_build = parallax_launch_count == nullptr;
+        if (host_build || where == 3) {
+            std::vector<Rec> recs(n);
+            for (size_t i = 0; i < n; ++i)
+                recs[i] = Rec{(float)(u_at(29, i) >> 40) * 0x1p-24f, 0u, &tgt[u_at(30, i) % n]};
+            std::vector<float> y(n);
+            b = launches();
+            parallax::transform(P, recs.begin(), recs.end(), y.begin(), GatherPlus{});
+            record("transform_gather_f32" + sfx, b, 0, y.data(), n);
+        }
     }
 }
 

@@ -93,6 +93,7 @@ _SIGNATURES = {
     "parallax_error_string": (C.c_char_p, [C.c_int]),
     "parallax_clear_error": (None, []),
     "parallax_builtin_kernel": (vp, [C.c_char_p]),
+    "parallax_kernel_resolves": (C.c_int, [C.c_char_p]),
     "parallax_arena_set_residency": (C.c_int, [vp, C.c_int]),
     "parallax_arena_get_residency": (C.c_int, [vp]),
     "parallax_arena_sync_to_device": (C.c_int, [vp, sz]),

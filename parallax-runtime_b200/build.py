@@ -4,7 +4,8 @@ Compiles every CUDA/C++ source under csrc/ with nvcc for sm_100a and links one s
 library, lib/libparallax-runtime.so, that exports the parallax C ABI. Objects go to
 _build/ and are rebuilt when a source or any header is newer than the object. The
 serving-mix load generator (loadgen/loadgen.cpp, host C++ over the public ABI) is linked
-against it as lib/libparallax-loadgen.so.
+against it as lib/libparallax-loadgen.so, and the whole-heap capture shim
+(heap/heap_capture.cpp) is archived as lib/libparallax-heap.a.
 
     python parallax-runtime_b200/build.py [--force] [--jobs N]
 """
@@ -94,6 +95,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False,
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
     build_loadgen(force)
+    build_heap_capture(force)
     return LIB
 
 
@@ -116,6 +118,32 @@ def build_loadgen(force: bool = False) -> Path:
         raise RuntimeError(f"loadgen build failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LOADGEN)
     return LOADGEN
+
+
+HEAP_SRC = PKG / "heap" / "heap_capture.cpp"
+HEAP_LIB = LIB_DIR / "libparallax-heap.a"
+
+
+def build_heap_capture(force: bool = False) -> Path:
+    """The whole-heap capture shim: a static library a program links (before the C library)
+    so that its malloc / operator new allocate from the runtime's heap pool."""
+    newest = max(HEAP_SRC.stat().st_mtime, (ROOT / "include" / "parallax" / "heap_pool.h").stat().st_mtime)
+    if not force and HEAP_LIB.exists() and HEAP_LIB.stat().st_mtime >= newest:
+        return HEAP_LIB
+    obj = BUILD / "heap_capture.o"
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", "-I", str(ROOT / "include"), "-c",
+           str(HEAP_SRC), "-o", str(obj)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"heap capture build failed:\n{r.stdout}\n{r.stderr}")
+    tmp = HEAP_LIB.with_suffix(".a.tmp")
+    if tmp.exists():
+        tmp.unlink()
+    r = subprocess.run(["ar", "rcs", str(tmp), str(obj)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"ar failed:\n{r.stderr}")
+    os.replace(tmp, HEAP_LIB)
+    return HEAP_LIB
 
 
 def main() -> None:

@@ -39,6 +39,10 @@ bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int slot
             return false;
         }
         out->dev = arena_dev(p);
+        if (arena_zero_copy()) {  // whole-heap capture: used in place, nothing to copy
+            out->kind = OperandKind::ARENA_RESIDENT;
+            return arena_make_accessible();
+        }
         out->kind = b.residency == PARALLAX_DEVICE_RESIDENT ? OperandKind::ARENA_RESIDENT
                                                             : OperandKind::ARENA_COHERENT;
         if (out->kind == OperandKind::ARENA_COHERENT && upload && bytes)
@@ -115,14 +119,15 @@ constexpr size_t kCopyOverlapMin = size_t(64) << 20;
 // A pointer into a live arena block in coherent mode (the call copies it both ways).
 bool coherent_arena(const void* p) {
     ArenaBlock b;
-    return p && arena_contains(p) && arena_find(p, &b) && b.residency != PARALLAX_DEVICE_RESIDENT;
+    return p && arena_contains(p) && !arena_zero_copy() && arena_find(p, &b) &&
+           b.residency != PARALLAX_DEVICE_RESIDENT;
 }
 // Device memory a call uses in place: a device-resident arena block or a CUDA pointer.
 bool in_place_device(const void* p) {
     if (!p) return false;
     if (arena_contains(p)) {
         ArenaBlock b;
-        return arena_find(p, &b) && b.residency == PARALLAX_DEVICE_RESIDENT;
+        return arena_find(p, &b) && (arena_zero_copy() || b.residency == PARALLAX_DEVICE_RESIDENT);
     }
     cudaPointerAttributes attr;
     const bool dev = cudaPointerGetAttributes(&attr, p) == cudaSuccess &&

@@ -16,6 +16,19 @@
 //     (see abi.cu), never the whole arena;
 //   * allocation is first-fit over an offset-ordered free map with coalescing (the
 //     reference never coalesces, arena.cpp:354-355), 256-byte minimum alignment.
+// Pool-backed mode (whole-heap capture; reference arena.cpp:183-275, :336-386): when the
+// heap pool (heap_pool.cu) is live at the arena's first use - a program linked with the
+// capture shim lib/libparallax-heap.a, or one that called px_pool_init() - the arena adopts
+// the pool's reservation instead of mapping memory of its own, and works like the
+// reference's imported host memory: the pool is page-locked (cudaHostRegister) in 64 MiB
+// chunks up to its high-water mark before any kernel that may touch it runs, its device
+// address is its host address (dev_base == host_base, so stored heap pointers relocate to
+// themselves), and kernels read and write it in place over the host link. Nothing is
+// copied, so no copy can ever overwrite a host-side change, and every heap pointer is an
+// arena pointer. Arena blocks are pool blocks (px_pool_alloc); residency modes and the
+// explicit sync calls have nothing to do in this mode. Needs a device that can use host
+// pointers for registered memory (a range that cannot be registered is still usable on a
+// device with pageable-memory access); otherwise the arena keeps its own mapping.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <stdio.h>
@@ -27,6 +40,7 @@
 #include <mutex>
 #include <vector>
 
+#include "parallax/heap_pool.h"
 #include "runtime.hpp"
 
 namespace pxb {
@@ -59,6 +73,9 @@ struct Arena {
     std::mutex mu;
     bool tried = false;
     bool ok = false;
+    bool pool = false;     // pool-backed: zero-copy over the heap pool's reservation
+    bool pageable = false;   // the device reaches pageable host memory itself (HMM)
+    size_t pool_locked = 0;  // pool bytes page-locked so far (from the base)
     size_t capacity = 0;
     char* host_base = nullptr;
     CUdeviceptr dev_base = 0;
@@ -78,7 +95,9 @@ struct Arena {
         std::lock_guard<std::mutex> g(mu);
         for (size_t c = off / chunk; c * chunk < off + bytes && c < pinned.size(); ++c) {
             if (pinned[c]) continue;
-            if (cudaHostRegister(host_base + c * chunk, chunk, cudaHostRegisterDefault) !=
+            // the pool's reservation may end inside its last chunk
+            const size_t len = capacity - c * chunk < chunk ? capacity - c * chunk : chunk;
+            if (cudaHostRegister(host_base + c * chunk, len, cudaHostRegisterDefault) !=
                 cudaSuccess) {
                 cudaGetLastError();  // copies from this chunk stay pageable (slower, correct)
                 continue;
@@ -116,6 +135,24 @@ struct Arena {
             gran = 2ull << 20;
         chunk = align_up(chunk, gran);
         capacity = align_up(capacity, chunk);
+        int host_ptrs = 0;
+        cudaDeviceGetAttribute(&host_ptrs, cudaDevAttrCanUseHostPointerForRegisteredMem,
+                               device_info().device);
+        void* pb = heap_pool_base();
+        if (pb && host_ptrs) {  // whole-heap capture: adopt the pool, zero-copy
+            pool = true;
+            int pma = 0;
+            cudaDeviceGetAttribute(&pma, cudaDevAttrPageableMemoryAccess, device_info().device);
+            pageable = pma != 0;
+            capacity = heap_pool_reservation();
+            host_base = static_cast<char*>(pb);
+            dev_base = reinterpret_cast<CUdeviceptr>(pb);
+            ok = true;
+            if (getenv("PARALLAX_DEBUG"))
+                fprintf(stderr, "[parallax] arena: pool-backed, %zu MiB host_base=%p dev_base=0x%llx\n",
+                        capacity >> 20, (void*)host_base, (unsigned long long)dev_base);
+            return true;
+        }
         if (drv.reserve(&dev_base, capacity, chunk, 0, 0) != CUDA_SUCCESS) {
             set_error(PARALLAX_ERR_OUT_OF_MEMORY, "arena: cannot reserve %zu MiB of device VA",
                       capacity >> 20);
@@ -164,6 +201,14 @@ struct Arena {
         size_t a = align < kAlign ? kAlign : align;
         if (a & (a - 1)) a = align_up(a, kAlign);
         size_t need = align_up(size, kAlign);
+        if (pool) {
+            char* p = static_cast<char*>(px_pool_alloc(need, a));
+            if (!p) {
+                set_error(PARALLAX_ERR_OUT_OF_MEMORY, "arena: heap pool exhausted (%zu bytes)", need);
+                return nullptr;
+            }
+            return commit((size_t)(p - host_base), need);
+        }
         // first fit in offset order
         for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
             size_t off = align_up(it->first, a);
@@ -213,6 +258,10 @@ struct Arena {
         size_t size = it->second.size;
         live.erase(it);
         used -= size;
+        if (pool) {
+            px_pool_free(p);
+            return;
+        }
         // insert and coalesce with neighbours
         auto nx = free_blocks.lower_bound(off);
         if (nx != free_blocks.end() && off + size == nx->first) {
@@ -239,10 +288,44 @@ struct Arena {
         if (!contains(p)) return false;
         size_t off = static_cast<const char*>(p) - host_base;
         auto it = live.upper_bound(off);
-        if (it == live.begin()) return false;
-        --it;
-        if (off >= it->first + it->second.size) return false;
-        if (out) *out = it->second;
+        if (it != live.begin()) {
+            --it;
+            if (off < it->first + it->second.size) {
+                if (out) *out = it->second;
+                return true;
+            }
+        }
+        if (!pool) return false;
+        // a heap object of a captured program: one region up to the pool's high water
+        const size_t hw = heap_pool_high_water();
+        if (off >= hw) return false;
+        if (out) {
+            out->offset = 0;
+            out->size = hw;
+            out->residency = PARALLAX_COHERENT;
+        }
+        return true;
+    }
+
+    // Pool-backed mode: page-locks the pool up to its high-water mark (64 MiB steps, never
+    // undone), so kernels can use any pool address. False when registration fails.
+    bool lock_pool() {
+        std::lock_guard<std::mutex> g(mu);
+        const size_t hw = heap_pool_high_water();
+        constexpr size_t kStep = 64ull << 20;
+        while (pool_locked < hw) {
+            const size_t len = capacity - pool_locked < kStep ? capacity - pool_locked : kStep;
+            if (cudaHostRegister(host_base + pool_locked, len, cudaHostRegisterDefault) != cudaSuccess) {
+                cudaGetLastError();
+                // a device that reaches pageable memory itself still sees this range
+                if (!pageable) {
+                    set_error(PARALLAX_ERR_CUDA,
+                              "arena: cannot page-lock the heap pool at offset %zu", pool_locked);
+                    return false;
+                }
+            }
+            pool_locked += len;
+        }
         return true;
     }
 
@@ -305,8 +388,18 @@ bool arena_copy_async(void* dst, const void* src, size_t bytes, bool to_device,
     return true;
 }
 
+bool arena_zero_copy() {
+    Arena& a = arena();
+    return a.ok && a.pool;
+}
+bool arena_make_accessible() {
+    Arena& a = arena();
+    return !(a.ok && a.pool) || a.lock_pool();
+}
+
 bool arena_sync_coherent(Workspace& ws, bool to_device) {
     Arena& a = arena();
+    if (a.ok && a.pool) return a.lock_pool();  // zero-copy: nothing moves
     std::vector<std::pair<size_t, size_t>> ranges;  // [begin, end) offsets
     {
         std::lock_guard<std::mutex> g(a.mu);
@@ -348,7 +441,6 @@ PXB_EXPORT int parallax_arena_contains(const void* ptr) {
     }
     return ptr && a.contains(ptr) ? 1 : 0;
 }
-PXB_EXPORT int parallax_heap_contains(const void*) { return 0; }
 
 PXB_EXPORT void* parallax_umalloc(size_t size, unsigned) { return parallax_arena_alloc(size, 256); }
 PXB_EXPORT void parallax_ufree(void* ptr) { parallax_arena_free(ptr); }
@@ -394,6 +486,7 @@ static int arena_copy(const void* ptr, size_t bytes, bool to_device) {
     if (!ws) return PARALLAX_ERR_NO_DEVICE;
     ArenaBlock b;
     if (!arena().find(ptr, &b)) return PARALLAX_ERR_INVALID_ARGUMENT;
+    if (arena_zero_copy()) return PARALLAX_OK;  // one copy, seen by both sides
     size_t off = static_cast<const char*>(ptr) - arena().host_base;
     if (off + bytes > b.offset + b.size) return PARALLAX_ERR_INVALID_ARGUMENT;
     void* dev = arena_dev(ptr);

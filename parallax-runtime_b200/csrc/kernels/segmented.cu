@@ -895,6 +895,8 @@ void* device_operand(const void* p, const char* fn, const char* what) {
     }
     if (arena_contains(p)) {
         ArenaBlock blk;
+        if (arena_find(p, &blk) && arena_zero_copy())  // whole-heap capture: in place
+            return arena_make_accessible() ? arena_dev(p) : nullptr;
         if (!arena_find(p, &blk) || blk.residency != PARALLAX_DEVICE_RESIDENT) {
             set_error(PARALLAX_ERR_INVALID_ARGUMENT,
                       "%s: %s: arena blocks must be PARALLAX_DEVICE_RESIDENT", fn, what);

@@ -397,8 +397,18 @@ PXB_EXPORT void parallax_kernel_register(const char* key, const unsigned int* sp
     if (debug()) fprintf(stderr, "[parallax_kernel_register] %s (%zu words)\n", key, words);
 }
 
+PXB_EXPORT int parallax_kernel_resolves(const char* key) {
+    if (!key) return 0;
+    std::lock_guard<std::mutex> g(reg_mu());
+    return funnel_builtin(key) != nullptr ? 1 : 0;
+}
+
 PXB_EXPORT parallax_kernel_t parallax_kernel_lookup(const char* key) {
     if (!key) return nullptr;
+    // Without a device nothing can be launched: every lookup misses and the caller runs its
+    // host loop, as a reference lookup does when its kernel cannot be loaded
+    // (src/kernel/cache.cpp:90-104).
+    if (!ensure_device()) return nullptr;
     std::lock_guard<std::mutex> g(reg_mu());
     auto& reg = registry();
     auto it = reg.find(key);

@@ -153,6 +153,11 @@ bool graph_launch(Workspace& ws, const std::string& key, const std::function<boo
 // default 120000) and surfaces in-kernel wait timeouts. Returns a parallax_status.
 int sync_stream(Workspace& ws);
 
+// ---- heap pool (heap_pool.cu) --------------------------------------------------------
+void* heap_pool_base();          // nullptr until the pool is initialized
+size_t heap_pool_reservation();
+size_t heap_pool_high_water();
+
 // ---- arena ---------------------------------------------------------------------------
 struct ArenaBlock {
     size_t offset = 0;
@@ -171,6 +176,12 @@ uint64_t arena_mapped_bytes();  // bytes of the arena currently backed by device
 // may touch any block, so they get the reference's whole-arena coherence
 // (src/memory/arena.cpp:296-304) restricted to blocks in coherent mode.
 bool arena_sync_coherent(Workspace& ws, bool to_device);
+// Pool-backed (whole-heap capture) mode: arena memory is page-locked host memory that
+// kernels use in place (device address == host address); nothing is ever copied.
+bool arena_zero_copy();
+// In that mode, page-locks the pool up to its high-water mark before a kernel may touch
+// it; true (and nothing to do) otherwise.
+bool arena_make_accessible();
 // Host mirror <-> device copy of an arena range (split at page-lock chunk boundaries).
 bool arena_copy_async(void* dst, const void* src, size_t bytes, bool to_device,
                       cudaStream_t s);

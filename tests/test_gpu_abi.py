@@ -276,3 +276,27 @@ def test_coherent_operand_spanning_arena_chunks(lib, px, ox, arena):
     lib.parallax_scan(h, h, P(data), n, 4)
     px.check()
     assert np.array_equal(data, ox.scan(x))
+
+
+GCC_REDUCE_KEY = ("T parallax::detail::device_reduce(const T*, std::size_t, T) "
+                  "[with T = {t}; std::size_t = long unsigned int]")
+
+
+def test_funnel_lookups_return_one_handle(lib):
+    k = GCC_REDUCE_KEY.format(t="float").encode()
+    h = lib.parallax_kernel_lookup(k)
+    assert h and h == lib.parallax_kernel_lookup(k)
+
+
+def test_registered_spirv_for_fixed_funnel_still_resolves(lib):
+    # A SPIR-V image cannot run here; a fixed primitive funnel key resolves to the
+    # built-in sm_100a kernel, a functor funnel key misses (host fallback).
+    words = (C.c_uint * 5)(0x07230203, 0x00010500, 0, 1, 0)
+    key = GCC_REDUCE_KEY.format(t="double").encode() + b" "
+    lib.parallax_kernel_register(key, words, 5)
+    assert lib.parallax_kernel_lookup(key)
+    fkey = b"void parallax::detail::device_invoke(T*, std::size_t, F) [with T = double; F = g]"
+    lib.parallax_kernel_register(fkey, words, 5)
+    assert not lib.parallax_kernel_lookup(fkey)
+    lib.parallax_clear_error()
+

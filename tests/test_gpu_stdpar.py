@@ -12,9 +12,16 @@ checked byte-exact against the oracle), floating-point sums and prefixes against
 compensated oracle within 1e-5 (fp32) / 1e-12 (fp64) (the host fallback is a left fold),
 partition against the stable oracle (the host fallback, std::partition, is unstable).
 Every device-side call must have launched runtime kernels; the host run launches none.
+
+A third build, `stdpar_driver_heap`, also links the whole-heap capture shim
+(lib/libparallax-heap.a, reference src/memory/heap_capture.cpp): every std::vector of the
+program lives in the runtime's heap pool, the arena adopts the pool (zero-copy), the funnels
+find their data in the arena and call the runtime on it in place, and a transform chases
+pointers stored in heap records. Its results must match the host run the same way.
 """
 from __future__ import annotations
 
+import os
 import subprocess
 from pathlib import Path
 
@@ -46,19 +53,26 @@ def parse(path: Path) -> dict[str, tuple[int, int, bytes]]:
 
 @pytest.fixture(scope="module")
 def runs(tmp_path_factory):
-    exe = {k: REF / f"stdpar_driver_{k}" for k in ("gpu", "host")}
+    exe = {k: REF / f"stdpar_driver_{k}" for k in ("gpu", "heap", "host")}
     if not all(p.exists() for p in exe.values()):
         pytest.skip("stdpar drivers not built (oracle/Makefile needs the reference's headers)")
     d = tmp_path_factory.mktemp("stdpar")
     res = {}
     for k, p in exe.items():
         out = d / f"{k}.bin"
+        env = dict(os.environ, PARALLAX_HEAP_POOL="16384")
         r = subprocess.run([str(p), str(IMAGES), str(out)], capture_output=True, text=True,
-                           timeout=600)
+                           timeout=600, env=env)
         assert r.returncode == 0, f"{p.name} failed ({r.returncode}):\n{r.stdout}\n{r.stderr}"
         res[k] = parse(out)
-    assert res["gpu"].keys() == res["host"].keys()
+    # the pointer-chasing transform runs only where stored heap pointers reach the device
+    gather = {k for k in res["host"] if k.startswith("transform_gather")}
+    assert res["gpu"].keys() == res["host"].keys() - gather
+    assert res["heap"].keys() == res["host"].keys()
     return res
+
+
+BUILDS = ("gpu", "heap")
 
 
 def inputs(ox, n):
@@ -85,21 +99,23 @@ def scalar(rec, dtype):
 NO_LAUNCH_AT_1 = {"inclusive_scan_f32", "inclusive_scan_i64", "sort_u32", "sort_f32"}
 
 
+@pytest.mark.parametrize("build", BUILDS)
 @pytest.mark.parametrize("n", SIZES)
-def test_every_call_went_through_the_runtime(runs, n):
-    for name, (launches, _, _) in runs["gpu"].items():
+def test_every_call_went_through_the_runtime(runs, n, build):
+    for name, (launches, _, _) in runs[build].items():
         base, size = name.split("@")
         if int(size) != n:
             continue
         assert runs["host"][name][0] == 0
-        if n == 1 and base in NO_LAUNCH_AT_1:
+        if (n == 1 and base in NO_LAUNCH_AT_1) or base == "heap_capture":
             continue
         assert launches > 0, f"{name}: no runtime kernel launched (the funnel fell back)"
 
 
+@pytest.mark.parametrize("build", BUILDS)
 @pytest.mark.parametrize("n", SIZES)
-def test_reduce_and_scans(runs, ox, n):
-    g, h = runs["gpu"], runs["host"]
+def test_reduce_and_scans(runs, build, ox, n):
+    g, h = runs[build], runs["host"]
     f32, f64, i32, i64 = inputs(ox, n)
     s = f"@{n}"
     got = scalar(g["reduce_f32" + s], np.float32)
@@ -121,9 +137,10 @@ def test_reduce_and_scans(runs, ox, n):
     assert ox.max_rel_err(ex, want) <= F64_TOL
 
 
+@pytest.mark.parametrize("build", BUILDS)
 @pytest.mark.parametrize("n", SIZES)
-def test_sort_and_unique(runs, ox, n):
-    g, h = runs["gpu"], runs["host"]
+def test_sort_and_unique(runs, build, ox, n):
+    g, h = runs[build], runs["host"]
     s = f"@{n}"
     got = arr(g["sort_u32" + s], np.uint32)
     assert np.array_equal(got, arr(h["sort_u32" + s], np.uint32))
@@ -140,9 +157,10 @@ def test_sort_and_unique(runs, ox, n):
     assert np.array_equal(arr(g["unique_i32" + s], np.int32), arr(h["unique_i32" + s], np.int32))
 
 
+@pytest.mark.parametrize("build", BUILDS)
 @pytest.mark.parametrize("n", SIZES)
-def test_compaction_with_registered_predicates(runs, ox, n):
-    g, h = runs["gpu"], runs["host"]
+def test_compaction_with_registered_predicates(runs, build, ox, n):
+    g, h = runs[build], runs["host"]
     s = f"@{n}"
     for name in ("copy_if_mod3_i32", "remove_if_mod3_i32"):
         assert g[name + s][1] == h[name + s][1], name
@@ -157,12 +175,29 @@ def test_compaction_with_registered_predicates(runs, ox, n):
     assert np.array_equal(np.sort(hv), np.sort(x))
 
 
+@pytest.mark.parametrize("build", BUILDS)
 @pytest.mark.parametrize("n", SIZES)
-def test_element_wise_funnels_with_registered_images(runs, n):
-    g, h = runs["gpu"], runs["host"]
+def test_element_wise_funnels_with_registered_images(runs, build, n):
+    g, h = runs[build], runs["host"]
     s = f"@{n}"
     for name, dt in (("for_each_affine_f32", np.float32), ("for_each_default_f32", np.float32),
                      ("transform_half_i32", np.float64)):
         assert np.array_equal(arr(g[name + s], dt).view(np.uint8),
                               arr(h[name + s], dt).view(np.uint8)), name
     assert g["count_if_gt_half_f32" + s][1] == h["count_if_gt_half_f32" + s][1]
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_whole_heap_capture(runs, n):
+    """Under capture the program's vectors are heap-pool memory that the arena adopted
+    (parallax_heap_contains and parallax_arena_contains both 1); without it, neither. The
+    transform over heap records that store pointers into another heap array gives the host
+    fallback's bytes (relocation of stored heap pointers)."""
+    s = f"@{n}"
+    assert runs["heap"]["heap_capture" + s][1] == 3
+    assert runs["gpu"]["heap_capture" + s][1] == 0
+    assert runs["host"]["heap_capture" + s][1] == 0
+    g, h = runs["heap"]["transform_gather_f32" + s], runs["host"]["transform_gather_f32" + s]
+    assert g[0] > 0
+    assert g[2] == h[2]
+
