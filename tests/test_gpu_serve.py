@@ -178,6 +178,14 @@ def test_alone_equals_mix_equals_oracle(server, px, dev, ox):
     run_mixed(lib, px, mixed)
     s1 = px.ServeStats()
     assert lib.parallax_serve_get_stats(C.byref(s1)) == px.OK
+    check_outputs(ox, alone, mixed)
+    # every request went through a batch (coalesced or alone); whether requests coalesce
+    # depends on how many wait when a lane frees up: test_zz_queued_requests_coalesce
+    assert s1.batches - s0.batches <= len(mixed)
+
+
+def check_outputs(ox, alone, mixed):
+    """Each request's result is the same alone and in the mix, and matches the oracle."""
     for a, m in zip(alone, mixed):
         ga, gm = a.output(), m.output()
         want = oracle_of(ox, a)
@@ -191,10 +199,6 @@ def test_alone_equals_mix_equals_oracle(server, px, dev, ox):
         else:
             assert same(a, ga, want if a.kind != "reduce" else a.x.dtype.type(want),
                         exact_fp=True), f"{a.spec} n={a.x.size}: differs from the oracle"
-    # the mix was coalesced: fewer launches than requests
-    batches = s1.batches - s0.batches
-    assert s1.coalesced_requests > s0.coalesced_requests
-    assert batches < len(mixed)
 
 
 def test_admission_by_memory_budget(server, px, dev, ox):
@@ -282,3 +286,36 @@ def test_zz_wait_after_stop_returns_the_status(lib, px, ox, dev):
     assert lib.parallax_serve_wait(t.value, C.byref(done)) == px.OK
     assert done.value > 0
     assert np.frombuffer(bytes(out), np.int32, 1)[0] == ox.reduce_sum(x)
+
+
+def test_zz_queued_requests_coalesce(lib, px, dev, ox):
+    """Requests that queue while the only lane is busy (behind a 2^26-key sort) are taken
+    as coalesced segmented launches, and every result is still the one it has alone."""
+    lib.parallax_serve_stop()
+    cfg = px.ServeConfig(lanes=1, max_batch=64, solo_elements=SOLO, inflight_bytes=4 << 30,
+                         schedulers=1)
+    assert lib.parallax_serve_start(C.byref(cfg)) == px.OK
+    try:
+        alone = mix(px, dev, ox, seed0=700)
+        queued = mix(px, dev, ox, seed0=700)
+        run_alone(lib, px, alone)
+        big = dev.put(ox.gen("i64_full", 77, 1 << 26))
+        dev.torch.cuda.synchronize()
+        r = px.Request()
+        r.kernel = px.builtin("sort:i64")
+        r.input = big.data_ptr()
+        r.count = 1 << 26
+        s0 = px.ServeStats()
+        lib.parallax_serve_get_stats(C.byref(s0))
+        t_big = C.c_uint64()
+        assert lib.parallax_serve_submit(C.byref(r), C.byref(t_big)) == px.OK
+        run_mixed(lib, px, queued, threads=1)
+        assert lib.parallax_serve_wait(t_big.value, None) == px.OK
+        s1 = px.ServeStats()
+        assert lib.parallax_serve_get_stats(C.byref(s1)) == px.OK
+        check_outputs(ox, alone, queued)
+        assert s1.coalesced_requests > s0.coalesced_requests
+        assert s1.batches - s0.batches < len(queued) + 1
+    finally:
+        assert lib.parallax_serve_stop() == px.OK
+
