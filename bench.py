@@ -553,6 +553,9 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the segmented, map and serving workloads")
+    ap.add_argument("--workloads", default=None,
+                    help="comma-separated subset of segmented,map,sort_paths,serving to run "
+                         "(default: all of them with the whole step, none with --ops)")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--ops", default="",
                     help="comma-separated operation names to run (default: the whole step), "
@@ -696,20 +699,28 @@ def main() -> None:
                     "share_of_step": round(dom["ms"] / args.steps / step_ms, 3)}
 
     workloads = {}
-    if selected is None and not args.no_workloads:
-        lib.parallax_set_async(1)
+    if args.workloads is not None:
+        wanted = {w for w in args.workloads.split(",") if w}
+    elif selected is None and not args.no_workloads:
+        wanted = {"segmented", "map", "sort_paths", "serving"}
+    else:
+        wanted = set()
+    lib.parallax_set_async(1)
+    if "segmented" in wanted:
         workloads["segmented"] = run_segmented(px, lib, torch, stream, args.steps, args.warmup, peak)
+    if "map" in wanted:
         workloads["map"] = run_map(px, lib, torch, stream, args.steps, args.warmup, peak)
+    if "sort_paths" in wanted:
         workloads["sort_paths"] = run_sort_paths(px, lib, torch, stream, args.steps, args.warmup,
                                                  peak)
     lib.parallax_set_async(0)
     lib.parallax_set_stream(None)
-    if selected is None and not args.no_workloads and rank == 0:
+    if "serving" in wanted and rank == 0:
         workloads["serving"] = run_serving(px, lib, args.serve_seconds)
 
     e2e = None
     if not args.no_e2e and rank == 0:
-        e2e = run_e2e(px, lib, x, kept_want, args.e2e_steps)
+        e2e = run_e2e(px, lib, x, kept_want, args.e2e_steps, torch)
     cpu = None
     if not args.no_cpu and rank == 0:
         cpu = cpu_baseline(x, min(args.ref_log2, args.log2n), min(args.ref_log2 - 2, args.log2sort))
@@ -1027,7 +1038,43 @@ def run_serving(px, lib, seconds: float) -> dict:
     return out
 
 
-def run_e2e(px, lib, x: dict, kept_want: dict, steps: int) -> dict:
+def copy_bandwidth(torch, nbytes: int = 1 << 30, reps: int = 5) -> dict:
+    """Pinned host <-> device copy bandwidth (GB/s): each direction alone, and both at once
+    on two streams (the bound of a step whose uploads and downloads overlap)."""
+    h_up = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h_dn = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d_a = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d_b = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s_up, s_dn = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(fn):
+        best = None
+        for _ in range(reps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        return best
+
+    def up():
+        with torch.cuda.stream(s_up):
+            d_a.copy_(h_up, non_blocking=True)
+
+    def dn():
+        with torch.cuda.stream(s_dn):
+            h_dn.copy_(d_b, non_blocking=True)
+
+    t_up, t_dn = timed(up), timed(dn)
+    t_both = timed(lambda: (up(), dn()))
+    del d_a, d_b
+    return {"h2d_gbs": round(nbytes / t_up / 1e9, 1), "d2h_gbs": round(nbytes / t_dn / 1e9, 1),
+            "bidir_gbs": round(2 * nbytes / t_both / 1e9, 1),
+            "how": "1 GiB pinned torch tensors, best of 5, host wall clock around each copy"}
+
+
+def run_e2e(px, lib, x: dict, kept_want: dict, steps: int, torch=None) -> dict:
     """Synchronous ABI calls on pinned host arena blocks (coherent mode)."""
     max_bytes = max(v.nbytes for v in x.values())
     pin = lib.parallax_arena_alloc(max_bytes, 256)
@@ -1082,10 +1129,17 @@ def run_e2e(px, lib, x: dict, kept_want: dict, steps: int) -> dict:
             d2h += down
     lib.parallax_arena_free(pin)
     lib.parallax_arena_free(pout)
-    return {"value": round(total_bytes / total_s / 1e9, 2), "unit": "GB/s",
-            "h2d_bytes_per_step": int(h2d // steps), "d2h_bytes_per_step": int(d2h // steps),
-            "steps": steps, "ms_per_step": round(1e3 * total_s / steps, 2),
-            "path": "synchronous C-ABI calls on pinned host arena blocks (coherent mode)"}
+    out = {"value": round(total_bytes / total_s / 1e9, 2), "unit": "GB/s",
+           "h2d_bytes_per_step": int(h2d // steps), "d2h_bytes_per_step": int(d2h // steps),
+           "steps": steps, "ms_per_step": round(1e3 * total_s / steps, 2),
+           "path": "synchronous C-ABI calls on pinned host arena blocks (coherent mode)"}
+    if torch is not None:
+        # the PCIe bound of the step: its copies alone, one direction after the other
+        bw = copy_bandwidth(torch)
+        serial_ms = 1e3 * (h2d / steps / (bw["h2d_gbs"] * 1e9) + d2h / steps / (bw["d2h_gbs"] * 1e9))
+        out["copy_bound"] = dict(bw, ms_per_step_serial=round(serial_ms, 2),
+                                 frac_of_serial_bound=round(serial_ms / out["ms_per_step"], 3))
+    return out
 
 
 if __name__ == "__main__":

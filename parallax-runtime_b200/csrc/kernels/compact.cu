@@ -306,19 +306,21 @@ __device__ __forceinline__ void compact_tile(T* buf, uint64_t* bars, uint32_t pa
     __syncthreads();  // buffer and shared state free for the next tile
 }
 
-// One CTA per tile, in blockIdx order (unaligned input).
+// One CTA per tile, in blockIdx order, or in the order of an atomic claim counter when
+// `claim` is given (see tile_claim()).
 template <typename T, int MODE, bool BULK>
 __global__ void __launch_bounds__(kBlock, kCtasPerSm)
 k_compact(const T* in, T* out, uint64_t n, PredDev<T> pred, TileStatus<uint64_t> ts,
           const unsigned long long* __restrict__ num_true,
-          unsigned long long* __restrict__ count_out) {
+          unsigned long long* __restrict__ count_out, uint32_t* claim) {
     constexpr int SUB = Shape<T>::SUB;
     constexpr int TILE = Shape<T>::TILE;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T* buf = reinterpret_cast<T*>(smem_raw);
     __shared__ __align__(8) uint64_t bars[kSub];
     __shared__ CompactSmem sm;
-    const uint64_t tile = blockIdx.x;
+    __shared__ uint32_t s_claim;
+    const uint64_t tile = claim ? tile_claim(claim, s_claim) : blockIdx.x;
     const uint64_t base = tile * (uint64_t)TILE;
     const uint64_t rem = n - base;
     const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
@@ -327,6 +329,7 @@ k_compact(const T* in, T* out, uint64_t n, PredDev<T> pred, TileStatus<uint64_t>
     __syncthreads();
     compact_tile<T, MODE, BULK>(buf, bars, 0, sm, tile, base, cnt, prev, out, n, pred, ts,
                                 num_true, count_out, tile == gridDim.x - 1);
+    if (claim && threadIdx.x == 0) persistent_exit(claim);
 }
 
 // Persistent CTAs (two per SM), two tile buffers each: the next claimed tile's bulk copies
@@ -416,7 +419,7 @@ bool launch_mode(uint64_t tiles, cudaStream_t s, bool bulk, const T* in, T* out,
         if (!smem_opt_in<k_compact<T, MODE, true>>(Shape<T>::SMEM))
             return cuda_ok(cudaGetLastError(), "k_compact shared-memory opt-in");
         k_compact<T, MODE, true><<<(unsigned)tiles, kBlock, Shape<T>::SMEM, s>>>(
-            in, out, n, p, ts, nt, count_out);
+            in, out, n, p, ts, nt, count_out, PXB_TILE_CLAIM ? counters : nullptr);
         return true;
     }
     if (bulk) {
@@ -431,8 +434,8 @@ bool launch_mode(uint64_t tiles, cudaStream_t s, bool bulk, const T* in, T* out,
     }
     if (!smem_opt_in<k_compact<T, MODE, false>>(Shape<T>::SMEM))
         return cuda_ok(cudaGetLastError(), "k_compact shared-memory opt-in");
-    k_compact<T, MODE, false><<<(unsigned)tiles, kBlock, Shape<T>::SMEM, s>>>(in, out, n, p, ts,
-                                                                              nt, count_out);
+    k_compact<T, MODE, false><<<(unsigned)tiles, kBlock, Shape<T>::SMEM, s>>>(
+        in, out, n, p, ts, nt, count_out, PXB_TILE_CLAIM ? counters : nullptr);
     return true;
 }
 

@@ -191,10 +191,13 @@ __device__ __forceinline__ void scan_tile(T* buf, uint64_t* bars, uint32_t parit
 // `tile0` is the first tile of this launch: a scan launched in chunks (so its copies can
 // overlap its tiles) passes each chunk's first tile, and every chunk shares one look-back
 // epoch, so the first tile of a chunk looks back into the chunks before it.
+// With `claim`, a CTA takes its tile from an atomic counter instead of its blockIdx (see
+// tile_claim()).
 template <typename T, bool EXCL, bool BULK>
 __global__ void __launch_bounds__(kBlock, kCtasPerSm)
 k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan)
-       typename ScanTypes<T>::A init, TileStatus<typename ScanTypes<T>::A> ts, uint64_t tile0) {
+       typename ScanTypes<T>::A init, TileStatus<typename ScanTypes<T>::A> ts, uint64_t tile0,
+       uint32_t* claim) {
     using A = typename ScanTypes<T>::A;
     constexpr int SUB = ScanShape<T>::SUB;
     constexpr int TILE = ScanShape<T>::TILE;
@@ -204,8 +207,9 @@ k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan
     __shared__ A s_tot[32];
     __shared__ A s_red[kBlock / 32 + 1];
     __shared__ int s_first[kBlock / 32];
+    __shared__ uint32_t s_claim;
     const int tid = threadIdx.x;
-    const uint64_t tile = tile0 + blockIdx.x;
+    const uint64_t tile = tile0 + (claim ? tile_claim(claim, s_claim) : blockIdx.x);
     const uint64_t base = tile * (uint64_t)TILE;
     const uint64_t rem = n - base;
     const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
@@ -217,6 +221,7 @@ k_scan(const T* in, T* out, uint64_t n,  // in == out allowed (in-place ABI scan
     if constexpr (BULK) {
         if (tid == 0 && bulk) bulk_wait_read_all();
     }
+    if (claim && tid == 0) persistent_exit(claim);
 }
 
 // Persistent CTAs (two per SM) with two tile buffers each: the bulk copies of the next
@@ -299,11 +304,11 @@ k_scan_persistent(const T* in, T* out, uint64_t n, uint64_t num_tiles,
 template <typename T, bool EXCL, bool BULK>
 bool launch_tiles_single(const T* in, T* out, uint64_t n, typename ScanTypes<T>::A init,
                          TileStatus<typename ScanTypes<T>::A> ts, uint64_t count,
-                         cudaStream_t s, uint64_t tile0 = 0) {
+                         cudaStream_t s, uint64_t tile0 = 0, uint32_t* claim = nullptr) {
     if (!smem_opt_in<k_scan<T, EXCL, BULK>>(ScanShape<T>::SMEM))
         return cuda_ok(cudaGetLastError(), "k_scan shared-memory opt-in");
-    k_scan<T, EXCL, BULK><<<(unsigned)count, kBlock, ScanShape<T>::SMEM, s>>>(in, out, n, init,
-                                                                            ts, tile0);
+    k_scan<T, EXCL, BULK><<<(unsigned)count, kBlock, ScanShape<T>::SMEM, s>>>(
+        in, out, n, init, ts, tile0, PXB_TILE_CLAIM ? claim : nullptr);
     return true;
 }
 
@@ -354,13 +359,13 @@ bool scan_typed(Workspace& ws, bool exclusive, const void* d_in, void* d_out, ui
     static const bool persistent = getenv("PARALLAX_PERSISTENT_TILES") != nullptr;
     bool ok;
     if (exclusive) {
-        ok = !bulk ? launch_tiles_single<T, true, false>(in, out, n, init, ts, tiles, s)
+        ok = !bulk ? launch_tiles_single<T, true, false>(in, out, n, init, ts, tiles, s, 0, counters)
            : persistent ? launch_tiles_persistent<T, true>(in, out, n, init, ts, tiles, counters, s)
-                        : launch_tiles_single<T, true, true>(in, out, n, init, ts, tiles, s);
+                        : launch_tiles_single<T, true, true>(in, out, n, init, ts, tiles, s, 0, counters);
     } else {
-        ok = !bulk ? launch_tiles_single<T, false, false>(in, out, n, init, ts, tiles, s)
+        ok = !bulk ? launch_tiles_single<T, false, false>(in, out, n, init, ts, tiles, s, 0, counters)
            : persistent ? launch_tiles_persistent<T, false>(in, out, n, init, ts, tiles, counters, s)
-                        : launch_tiles_single<T, false, true>(in, out, n, init, ts, tiles, s);
+                        : launch_tiles_single<T, false, true>(in, out, n, init, ts, tiles, s, 0, counters);
     }
     if (!ok) return false;
     count_launch();
@@ -428,9 +433,10 @@ bool scan_copies_typed(Workspace& ws, bool exclusive, const void* h_in, const vo
                 !cuda_ok(cudaStreamWaitEvent(s, ws.ev_copy[1], 0), "copy wait"))
                 return fail();
         }
+        uint32_t* counters = reinterpret_cast<uint32_t*>(scratch + ScratchOff::counters);
         const bool ok =
-            exclusive ? launch_tiles_single<T, true, true>(in, out, n, init, ts, t1 - t0, s, t0)
-                      : launch_tiles_single<T, false, true>(in, out, n, init, ts, t1 - t0, s, t0);
+            exclusive ? launch_tiles_single<T, true, true>(in, out, n, init, ts, t1 - t0, s, t0, counters)
+                      : launch_tiles_single<T, false, true>(in, out, n, init, ts, t1 - t0, s, t0, counters);
         if (!ok) return fail();
         if (h_out) {
             if (!cuda_ok(cudaEventRecord(ws.ev_copy[2], s), "copy event") ||

@@ -13,9 +13,10 @@
 // lengths into a tile work list (item_start[s] = first work item of segment s; a segment of
 // L elements has ceil(L / tile) items) and writes the results of empty segments; the
 // persistent kernel's CTAs then claim work items from an atomic counter in order and
-// process one tile each. While a CTA works on a tile, the claim and the segment
-// description of its next item are already on their way (prefetched by thread 0), so the
-// dependent loads that locate a tile overlap the work of the previous one.
+// process one tile each. A work item's descriptor (segment, tile index, addresses) is
+// precomputed, and thread 0 claims and describes the next item while the current tile's
+// results are being stored (a reduce tile: while it is being read), so the claim's round
+// trip and the descriptor load overlap the work of the previous tile.
 //
 // A tile is staged in shared memory with 16-byte vector loads (striped: consecutive
 // threads read consecutive vectors), at the segment's own 16-byte phase: element e of the
@@ -315,28 +316,29 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
     tsk.epoch = b.counters[2];
     tsk.err = err;
 
-    // Thread 0's two-stage pipeline: the item for the next tile is claimed two tiles ahead
-    // and its descriptor loaded one tile ahead, so no iteration waits on its own loads.
-    // Claims are made in order, so the lowest unfinished item is always the one its CTA is
-    // working on, and every look-back wait ends.
-    uint32_t c_next = 0, c_after = 0;
+    // Thread 0 claims the next item and loads its descriptor while the current tile is still
+    // in progress, so the claim's round trip and the dependent descriptor load overlap work.
+    // A look-back tile claims its successor only once its own inclusive prefix is published
+    // (before its stores): a claimed item that waits behind a tile still in its look-back
+    // would hold up every later tile's look-back for a whole tile. Reduce tiles never wait,
+    // and claim at their start. Claims are made in order and a CTA works on its claims in
+    // order, so the lowest unfinished item is always being worked on: every look-back ends.
+    uint32_t c_next = 0;
     ItemDesc d_next;
     if (tid == 0) {
         c_next = atomicAdd(&b.counters[0], 1u);
-        c_after = atomicAdd(&b.counters[0], 1u);
         if (c_next < total) d_next = load_desc(b.items, c_next);
     }
+    auto claim_next = [&]() {
+        if (tid == 0) c_next = atomicAdd(&b.counters[0], 1u);
+    };
+    auto describe_next = [&]() {
+        if (tid == 0 && c_next < total) d_next = load_desc(b.items, c_next);
+    };
     for (;;) {
         if (tid == 0) {
             s_item = c_next;
-            if (c_next < total) {
-                s_it = d_next;
-                c_next = c_after;
-                if (c_next < total) {
-                    d_next = load_desc(b.items, c_next);
-                    c_after = atomicAdd(&b.counters[0], 1u);
-                }
-            }
+            if (c_next < total) s_it = d_next;
         }
         __syncthreads();
         const ItemDesc it = s_it;
@@ -352,6 +354,8 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
         const bool vec_ok = reinterpret_cast<uintptr_t>(in) % sizeof(T) == 0;
 
         if constexpr (OP == SEG_REDUCE) {
+            claim_next();
+            describe_next();
             // straight from global memory: each thread folds VPT vectors; sums and counts
             // accumulate in A, max / min in T
             const bool mm = a.red == RED_MAX || a.red == RED_MIN;
@@ -457,6 +461,7 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                 __syncthreads();
                 const A prefix =
                     lookback_cta<A, BLOCK>(ts, item, agg, red, first, it.first_item);
+                claim_next();
                 const A tb = (A)a.init + ((prefix + woff) + tex);
                 uint4* row = reinterpret_cast<uint4*>(sm + tid * ITEMS);
 #pragma unroll
@@ -476,6 +481,7 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                     unstage<T, BLOCK, VPT>(sm, out, begin, len, mis);
                 else
                     for (uint32_t e = tid; e < len; e += BLOCK) out[begin + e] = sm[e + mis];
+                describe_next();
                 __syncthreads();
             } else {  // SEG_SELECT / SEG_PARTITION
                 uint32_t f = 0;
@@ -496,6 +502,7 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                 const uint64_t prefix =
                     lookback_cta<uint64_t, BLOCK>(tsk, item, (uint64_t)kept, red64, first,
                                                   it.first_item);
+                claim_next();
                 if constexpr (OP == SEG_SELECT) {
                     // pack the kept elements at the front of the staged tile, then store
                     uint32_t r = kstart;
@@ -534,6 +541,7 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                         else *err = 3;
                     }
                 }
+                describe_next();
                 __syncthreads();
             }
         }

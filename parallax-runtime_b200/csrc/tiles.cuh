@@ -119,6 +119,24 @@ __device__ __forceinline__ void bulk_wait_read_all() {
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// One-tile-per-CTA kernels take their tile from an atomic counter (PXB_TILE_CLAIM=1) or
+// use blockIdx (0). With a claim counter, a tile's predecessors were all claimed, i.e.
+// running, before it, whatever order the hardware dispatches the grid's blocks in; with
+// blockIdx the look-back relies on in-order dispatch, and a wait that nonetheless never
+// ends gives up after its poll limit with PARALLAX_ERR_DEVICE_SPIN instead of hanging.
+#ifndef PXB_TILE_CLAIM
+#define PXB_TILE_CLAIM 0
+#endif
+
+// Claims the next tile from counters[0]; every thread of the CTA gets it. The CTA must
+// call persistent_exit(counters) once at its end, which resets the counters for the next
+// launch.
+__device__ __forceinline__ uint32_t tile_claim(uint32_t* counters, uint32_t& s_slot) {
+    if (threadIdx.x == 0) s_slot = atomicAdd(&counters[0], 1u);
+    __syncthreads();
+    return s_slot;
+}
+
 // Claim / exit counters of a persistent launch: counters[0] hands out tiles,
 // counters[1] counts exited CTAs; the last CTA to exit zeroes both for the next launch.
 __device__ __forceinline__ void persistent_exit(uint32_t* counters) {
