@@ -556,6 +556,9 @@ def main() -> None:
     ap.add_argument("--workloads", default=None,
                     help="comma-separated subset of segmented,map,sort_paths,serving to run "
                          "(default: all of them with the whole step, none with --ops)")
+    ap.add_argument("--seg-ops", default="",
+                    help="comma-separated segmented operations to run (default: all), e.g. "
+                         "segmented_copy_if_f32 for a small profiling case")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--ops", default="",
                     help="comma-separated operation names to run (default: the whole step), "
@@ -707,7 +710,8 @@ def main() -> None:
         wanted = set()
     lib.parallax_set_async(1)
     if "segmented" in wanted:
-        workloads["segmented"] = run_segmented(px, lib, torch, stream, args.steps, args.warmup, peak)
+        workloads["segmented"] = run_segmented(px, lib, torch, stream, args.steps, args.warmup, peak,
+                                               {o for o in args.seg_ops.split(",") if o} or None)
     if "map" in wanted:
         workloads["map"] = run_map(px, lib, torch, stream, args.steps, args.warmup, peak)
     if "sort_paths" in wanted:
@@ -800,9 +804,11 @@ def timed_calls(torch, stream, fn, steps: int, warmup: int, restore=None) -> flo
     return statistics.fmean(times)
 
 
-def run_segmented(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dict:
+def run_segmented(px, lib, torch, stream, steps: int, warmup: int, peak: float,
+                  only: set | None = None) -> dict:
     """Batched segmented primitives: 4096 segments, lognormal sizes (median 4096, sigma 2,
-    clipped to [1, 2^22], seed 11); each call is one replayed CUDA graph."""
+    clipped to [1, 2^22], seed 11); each call is one replayed CUDA graph. `only`: the
+    operation names to run (all when None)."""
     off = lognormal_offsets(11, 4096, 4096, 2.0, 1, 1 << 22)
     total = int(off[-1])
     S = off.size - 1
@@ -841,6 +847,8 @@ def run_segmented(px, lib, torch, stream, steps: int, warmup: int, peak: float) 
     ops.append(("segmented_sort_kv_u32", 2 * total * 8, lambda: work.copy_(d_recs, non_blocking=True),
                 lambda: lib.parallax_segmented_sort(px.builtin("sort_kv:u32"), P(work), total,
                                                     P(d_off), S)))
+    if only:
+        ops = [op for op in ops if op[0] in only]
     per_op, tot_bytes, tot_ms = {}, 0, 0.0
     for name, nbytes, restore, fn in ops:
         ms = timed_calls(torch, stream, fn, steps, warmup, restore)
@@ -851,7 +859,7 @@ def run_segmented(px, lib, torch, stream, steps: int, warmup: int, peak: float) 
         tot_ms += ms
     # parity spot check of the sorted records (stable by key within each segment)
     got = work.cpu().numpy().view(np.uint64)
-    for s_ in (0, S // 2, S - 1):
+    for s_ in ((0, S // 2, S - 1) if "segmented_sort_kv_u32" in per_op else ()):
         a, b = int(off[s_]), int(off[s_ + 1])
         seg = recs[a:b]
         want = seg[np.argsort(seg >> np.uint64(32), kind="stable")]
@@ -1013,6 +1021,11 @@ def run_serving(px, lib, seconds: float) -> dict:
         # one call at a time: how a runtime that is not thread-safe (the reference's,
         # src/kernel/kernel_launcher.hpp:172-176) has to be driven by 16 client threads
         out["per_call_serialized_saturation"] = one(2, 0.0)
+        # what the device sustains for the mix: the same calls enqueued asynchronously on
+        # the 16 threads' streams, one synchronization per 64 calls (no host round trip per
+        # request); neither the per-call nor the served path can exceed it with these kernels
+        out["device_bound_saturation"] = {k: v for k, v in one(3, 0.0).items()
+                                          if k in ("req_s", "GB_s", "completed", "offered_req_s")}
         # where coalescing pays: the same mix restricted to small requests (2^10..2^16),
         # whose cost is launch and synchronisation rather than HBM traffic
         out["small_requests"] = {"per_call_saturation": one(0, 0.0, 16)}
@@ -1027,6 +1040,8 @@ def run_serving(px, lib, seconds: float) -> dict:
                               "max_batch": st.max_batch, "memory_waits": st.memory_waits}
         out["throughput_ratio_saturation"] = round(
             out["served_saturation"]["req_s"] / out["per_call_saturation"]["req_s"], 3)
+        out["served_fraction_of_device_bound"] = round(
+            out["served_saturation"]["req_s"] / out["device_bound_saturation"]["req_s"], 3)
         out["throughput_ratio_vs_serialized"] = round(
             out["served_saturation"]["req_s"] / out["per_call_serialized_saturation"]["req_s"], 3)
     finally:

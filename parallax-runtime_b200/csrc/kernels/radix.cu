@@ -75,6 +75,9 @@ __device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
 __device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+// Which 32-bit half of a ranking-table word holds the lane mask of digit d (1 = high).
+__device__ __forceinline__ uint32_t mask_half(uint32_t d) { return (d >> 4) & 1u; }
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -180,8 +183,10 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     // offsets of stream s of this warp in the tile, per digit (filled in step 3a): wh + s * kBins
     uint32_t* const wh = s_wh + warp * kSubs * kBins;
     // the ranking's tables borrow the key buffer, which is free until step 4a: one 64-bit
-    // word per (stream, digit), high half the stream's running count of the digit, low half
-    // the lane mask of the current item's peers, so one load reads both
+    // word per (stream, digit) holding the stream's running count of the digit and the lane
+    // mask of the current item's peers, so one load reads both. The mask is the low half for
+    // digits with bit 4 clear and the high half otherwise: digit d's word spans banks 2d and
+    // 2d + 1 (mod 32), so the atomic ORs of a warp spread over all 32 banks, not 16.
     static_assert((size_t)TILE * sizeof(K) >= (size_t)TABLES * kBins * 8, "rank tables fit");
     uint64_t* const wm = reinterpret_cast<uint64_t*>(s_keys) + warp * kSubs * kBins;
 #pragma unroll
@@ -228,23 +233,25 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     const uint32_t le = lt | (1u << lane);
 #pragma unroll
     for (int j = 0; j < STREAM_ITEMS; ++j) {  // item j of every stream
-        uint32_t d[kSubs], peers[kSubs], c[kSubs];
+        uint32_t d[kSubs], peers[kSubs], c[kSubs], ms[kSubs];
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
-            d[t] = digit_of(k[t * STREAM_ITEMS + j], shift) + t * kBins;
-            atomicOr(reinterpret_cast<uint32_t*>(&wm[d[t]]), 1u << lane);  // low half
+            const uint32_t dg = digit_of(k[t * STREAM_ITEMS + j], shift);
+            d[t] = dg + t * kBins;
+            ms[t] = mask_half(dg);
+            atomicOr(reinterpret_cast<uint32_t*>(&wm[d[t]]) + ms[t], 1u << lane);
         }
         __syncwarp();
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
             const uint64_t v = wm[d[t]];
-            peers[t] = (uint32_t)v;
-            c[t] = (uint32_t)(v >> 32) + __popc(peers[t] & lt);
+            peers[t] = (uint32_t)(v >> (32 * ms[t]));
+            c[t] = (uint32_t)(v >> (32 - 32 * ms[t])) + __popc(peers[t] & lt);
         }
         __syncwarp();
 #pragma unroll
-        for (int t = 0; t < kSubs; ++t)
-            if ((peers[t] & ~le) == 0) wm[d[t]] = (uint64_t)(c[t] + 1) << 32;  // the highest peer
+        for (int t = 0; t < kSubs; ++t)  // the highest peer: count + peers, mask cleared
+            if ((peers[t] & ~le) == 0) wm[d[t]] = (uint64_t)(c[t] + 1) << (32 - 32 * ms[t]);
         __syncwarp();
 #pragma unroll
         for (int t = 0; t < kSubs; ++t) {
@@ -262,7 +269,7 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
         const uint64_t* const all = reinterpret_cast<const uint64_t*>(s_keys);
 #pragma unroll 8
         for (int w = 0; w < TABLES; ++w) {
-            const uint32_t c = (uint32_t)(all[w * kBins + tid] >> 32);
+            const uint32_t c = (uint32_t)(all[w * kBins + tid] >> (32 - 32 * mask_half(tid)));
             s_wh[w * kBins + tid] = cnt;
             cnt += c;
         }

@@ -300,7 +300,6 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
     __shared__ T redT[WARPS + 1];
     __shared__ int first[WARPS];
     __shared__ uint32_t wcnt[WARPS];
-    __shared__ uint32_t wcnt2[WARPS];
     __shared__ ItemDesc s_it;
     __shared__ uint32_t s_item;
     __shared__ T s_prev;
@@ -356,34 +355,49 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
         if constexpr (OP == SEG_REDUCE) {
             claim_next();
             describe_next();
-            // straight from global memory: each thread folds VPT vectors; sums and counts
+            // straight from global memory: each thread first issues all of its VPT vector
+            // loads (streaming, no L1 allocation), then folds them; sums and counts
             // accumulate in A, max / min in T
             const bool mm = a.red == RED_MAX || a.red == RED_MIN;
             A acc = A(0);
             T accm = red_identity<T>(a.red);
             const T* base = in + begin - mis;
+            uint4 v[VPT];
 #pragma unroll
             for (int q = 0; q < VPT; ++q) {
                 const int j = q * BLOCK + tid;
                 const int e0 = j * V - (int)mis;
-                T x[V];
-                const bool full = vec_ok && e0 >= 0 && e0 + V <= (int)len;
-                if (full) {
-                    const uint4 v = *reinterpret_cast<const uint4*>(base + j * V);
-                    memcpy(x, &v, 16);
-                }
+                v[q] = vec_ok && e0 >= 0 && e0 + V <= (int)len
+                           ? ldg_stream16(base + j * V)
+                           : make_uint4(0u, 0u, 0u, 0u);
+            }
+            auto fold = [&](auto red_c) {
+                constexpr int R = decltype(red_c)::value;
 #pragma unroll
-                for (int e = 0; e < V; ++e) {
-                    const int i = e0 + e;
-                    const bool in_tile = i >= 0 && i < (int)len;
-                    if (!full && in_tile) x[e] = in[begin + i];
-                    if (full || in_tile) {
-                        if (a.red == RED_SUM) acc = acc + (A)x[e];
-                        else if (a.red == RED_COUNT) acc = acc + (A)(a.pred(x[e]) ? 1 : 0);
-                        else if (a.red == RED_MAX) accm = OpMax()(accm, x[e]);
-                        else accm = OpMin()(accm, x[e]);
+                for (int q = 0; q < VPT; ++q) {
+                    const int e0 = (q * BLOCK + tid) * V - (int)mis;
+                    const bool full = vec_ok && e0 >= 0 && e0 + V <= (int)len;
+                    T x[V];
+                    memcpy(x, &v[q], 16);
+#pragma unroll
+                    for (int e = 0; e < V; ++e) {
+                        const int i = e0 + e;
+                        const bool in_tile = i >= 0 && i < (int)len;
+                        if (!full && in_tile) x[e] = in[begin + i];  // the ragged ends
+                        if (full || in_tile) {
+                            if constexpr (R == RED_SUM) acc = acc + (A)x[e];
+                            else if constexpr (R == RED_COUNT) acc = acc + (A)(a.pred(x[e]) ? 1 : 0);
+                            else if constexpr (R == RED_MAX) accm = OpMax()(accm, x[e]);
+                            else accm = OpMin()(accm, x[e]);
+                        }
                     }
                 }
+            };
+            switch (a.red) {
+                case RED_SUM: fold(std::integral_constant<int, RED_SUM>()); break;
+                case RED_COUNT: fold(std::integral_constant<int, RED_COUNT>()); break;
+                case RED_MAX: fold(std::integral_constant<int, RED_MAX>()); break;
+                default: fold(std::integral_constant<int, RED_MIN>()); break;
             }
             const bool count = a.red == RED_COUNT;
             A tot = A(0);
@@ -503,41 +517,61 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                     lookback_cta<uint64_t, BLOCK>(tsk, item, (uint64_t)kept, red64, first,
                                                   it.first_item);
                 claim_next();
+                // Output warp by warp: warp w's rows are the staged slots [w * 32 * ITEMS,
+                // + 32 * ITEMS), whose kept elements form one contiguous output run (and, for
+                // partition, whose rejected ones form another), so each warp packs its own
+                // slots in place and stores its runs with no CTA-wide barrier.
+                T* const wsm = sm + warp * 32 * ITEMS;
+                {  // the row again, from shared memory (fewer registers live across the look-back)
+                    const uint4* row = reinterpret_cast<const uint4*>(sm + tid * ITEMS);
+#pragma unroll
+                    for (int v = 0; v < VPT; ++v) {
+                        const uint4 q = row[v];
+                        memcpy(&x[v * V], &q, 16);
+                    }
+                }
+                __syncwarp();  // every row of the warp is in registers before it is overwritten
+                const uint32_t wex = shfl_idx(kstart, 0);                      // kept before the warp
+                const uint32_t wk = shfl_idx(kstart + (uint32_t)__popc(f), 31) - wex;
+                uint32_t rk = kstart - wex;
                 if constexpr (OP == SEG_SELECT) {
-                    // pack the kept elements at the front of the staged tile, then store
-                    uint32_t r = kstart;
 #pragma unroll
                     for (int j = 0; j < ITEMS; ++j)
-                        if (f >> j & 1u) sm[r++] = x[j];  // rows were read before the barriers
-                    __syncthreads();
-                    for (uint32_t i = tid; i < kept; i += BLOCK) {
-                        if (prefix + i < it.len) out[prefix + i] = sm[i];
+                        if (f >> j & 1u) wsm[rk++] = x[j];
+                    __syncwarp();
+                    for (uint32_t i = lane; i < wk; i += 32) {
+                        if (prefix + wex + i < it.len) out[prefix + wex + i] = wsm[i];
                         else *err = 3;
                     }
                     if (tid == 0 && k == it.seg_items - 1)
                         *reinterpret_cast<uint64_t*>(it.aux) = prefix + kept;
                 } else {
-                    // rejected elements of this row follow the kept run of the tile
+                    // rejected elements of the warp follow its kept run in its slots
                     uint32_t valid = 0;
 #pragma unroll
                     for (int j = 0; j < ITEMS; ++j) valid += (r0 + j >= 0 && r0 + j < (int)len);
-                    uint32_t rstart;
-                    tile_ranks<BLOCK>(valid - __popc(f), wcnt2, &rstart);
-                    uint32_t rk = kstart, rr = kept + rstart;
+                    const uint32_t rej = valid - __popc(f);
+                    const uint32_t rincl = warp_inclusive_scan(rej, OpSum());
+                    const uint32_t wr = shfl_idx(rincl, 31);
+                    uint32_t rr = wk + rincl - rej;
 #pragma unroll
                     for (int j = 0; j < ITEMS; ++j) {
                         const int i = r0 + j;
                         if (i < 0 || i >= (int)len) continue;
-                        if (f >> j & 1u) sm[rk++] = x[j];
-                        else sm[rr++] = x[j];
+                        if (f >> j & 1u) wsm[rk++] = x[j];
+                        else wsm[rr++] = x[j];
                     }
-                    __syncthreads();
-                    // the segment's kept total, written by the count pass
+                    __syncwarp();
+                    // the segment's kept total, written by the count pass; the tile's rejected
+                    // elements start after the segment's kept run and the earlier tiles'
+                    // rejected ones, the warp's after the tile's earlier warps'
                     const uint64_t seg_true = *reinterpret_cast<const uint64_t*>(it.aux);
-                    const uint64_t rej_base = seg_true + (begin - prefix);
-                    for (uint32_t i = tid; i < len; i += BLOCK) {
-                        const uint64_t dst = i < kept ? prefix + i : rej_base + (i - kept);
-                        if (dst < it.len) out[dst] = sm[i];
+                    const int first_elem = warp * 32 * ITEMS - (int)mis;  // of the warp's slots
+                    const uint32_t before = first_elem <= 0 ? 0u : min((uint32_t)first_elem, len);
+                    const uint64_t rej_base = seg_true + (begin - prefix) + (before - wex);
+                    for (uint32_t i = lane; i < wk + wr; i += 32) {
+                        const uint64_t dst = i < wk ? prefix + wex + i : rej_base + (i - wk);
+                        if (dst < it.len) out[dst] = wsm[i];
                         else *err = 3;
                     }
                 }
@@ -774,6 +808,9 @@ int tuned_shape(Workspace& ws, const SegCall& c) {
         if (cudaEventSynchronize(e1) != cudaSuccess) break;
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
+        if (getenv("PARALLAX_DEBUG"))
+            fprintf(stderr, "[parallax] segmented op %d dtype %d bucket %d: %d threads x %d vectors %.3f ms\n",
+                    opkey, (int)c.t, bucket_of(c), kShapes[cand].block, kShapes[cand].vpt, ms);
         if (ms < best_ms) {
             best_ms = ms;
             best = cand;

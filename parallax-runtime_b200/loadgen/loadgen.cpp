@@ -44,7 +44,11 @@ typedef struct px_loadgen_config {
     uint32_t threads;        /* client threads (16) */
     uint32_t mode;           /* 0 per-call, 1 served, 2 per-call serialized by one lock
                                 (one call at a time, as a runtime that is not thread-safe
-                                must be driven) */
+                                must be driven), 3 device bound: every thread enqueues its
+                                calls asynchronously on its own stream and synchronizes once
+                                per 64 calls, so the rate is what the device sustains for the
+                                mix with no host round trip per request (latencies are not
+                                meaningful in this mode) */
     double rate;             /* offered requests/s over all threads; <= 0: back-to-back */
     double seconds;          /* issuing window */
     uint64_t seed;
@@ -153,13 +157,15 @@ void free_buf(Item& it) {
 // ---- per-call path: one synchronous ABI call ---------------------------------------------
 std::mutex g_call_mu;  // mode 2: one call at a time
 
-int run_call(Item& it) {
+// `dev_result`: where a reduce writes its value in async mode (a device-resident block).
+int run_call(Item& it, void* dev_result = nullptr) {
     const int t = it.t;
     const size_t s = kSize[t];
     parallax_clear_error();
     switch (it.op) {
         case OP_REDUCE:
-            parallax_reduce(g_pool.reduce[t], const_cast<void*>(input_of(it)), it.n, s, &it.result);
+            parallax_reduce(g_pool.reduce[t], const_cast<void*>(input_of(it)), it.n, s,
+                            dev_result ? dev_result : &it.result);
             break;
         case OP_SCAN: {
             const uint64_t zero = 0;
@@ -174,6 +180,7 @@ int run_call(Item& it) {
             parallax_kernel_t h = g_pool.copy_if[t];
             it.result = parallax_copy_if(h, h, h, h, const_cast<void*>(input_of(it)), it.buf, it.n, s,
                                          t < 2);
+            if (dev_result) it.result = 0;  // async: the count is not read back
             break;
         }
     }
@@ -277,6 +284,45 @@ void client(const px_loadgen_config& c, int tid, StartLine* line, ThreadOut* out
         }
     };
     advance();
+    if (c.mode == 3) {
+        void* dres = parallax_arena_alloc(256, 256);
+        if (!dres || parallax_arena_set_residency(dres, PARALLAX_DEVICE_RESIDENT) != PARALLAX_OK) {
+            Item bad;
+            bad.status = PARALLAX_ERR_OUT_OF_MEMORY;
+            out->items.push_back(bad);
+            return;
+        }
+        parallax_set_async(1);
+        std::vector<Item> chunk;
+        auto drain = [&] {
+            const int st = parallax_synchronize();
+            const uint64_t t = now_ns();
+            for (Item& it : chunk) {
+                it.done = t;
+                if (it.status == PARALLAX_OK) it.status = st;
+                free_buf(it);
+                out->items.push_back(it);
+            }
+            chunk.clear();
+        };
+        sleep_until(t0);
+        for (;;) {
+            Item it = make_item(r, c);
+            it.arrival = now_ns();
+            if (it.arrival >= t_end) break;
+            if (!alloc_buf(it)) {  // arena full: let this thread's calls finish first
+                drain();
+                while (!alloc_buf(it)) std::this_thread::yield();
+            }
+            it.status = run_call(it, dres);
+            chunk.push_back(it);
+            if (chunk.size() == 64) drain();
+        }
+        drain();
+        parallax_set_async(0);
+        parallax_arena_free(dres);
+        return;
+    }
     if (c.mode == 0 || c.mode == 2) {
         sleep_until(t0);
         for (;;) {
