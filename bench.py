@@ -1012,6 +1012,9 @@ def run_serving(px, lib, seconds: float) -> dict:
         out = {"per_call_saturation": one(0, 0.0)}
         assert lib.parallax_serve_start(None) == px.OK
         out["served_saturation"] = one(1, 0.0)
+        # the same client concurrency as per-call (one outstanding request per client), so the
+        # latencies compare at equal load; the point above keeps 8 per client outstanding
+        out["served_saturation_depth1"] = one(1, 0.0, inflight=1)
         rate = round(0.7 * out["per_call_saturation"]["req_s"], 1)
         out["served_at_rate"] = one(1, rate)
         st = px.ServeStats()
@@ -1040,6 +1043,8 @@ def run_serving(px, lib, seconds: float) -> dict:
                               "max_batch": st.max_batch, "memory_waits": st.memory_waits}
         out["throughput_ratio_saturation"] = round(
             out["served_saturation"]["req_s"] / out["per_call_saturation"]["req_s"], 3)
+        out["throughput_ratio_saturation_depth1"] = round(
+            out["served_saturation_depth1"]["req_s"] / out["per_call_saturation"]["req_s"], 3)
         out["served_fraction_of_device_bound"] = round(
             out["served_saturation"]["req_s"] / out["device_bound_saturation"]["req_s"], 3)
         out["throughput_ratio_vs_serialized"] = round(
