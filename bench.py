@@ -554,7 +554,7 @@ def main() -> None:
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the segmented, map and serving workloads")
     ap.add_argument("--workloads", default=None,
-                    help="comma-separated subset of segmented,map,sort_paths,serving to run "
+                    help="comma-separated subset of segmented,map,funnels,sort_paths,serving to run "
                          "(default: all of them with the whole step, none with --ops)")
     ap.add_argument("--seg-ops", default="",
                     help="comma-separated segmented operations to run (default: all), e.g. "
@@ -705,7 +705,7 @@ def main() -> None:
     if args.workloads is not None:
         wanted = {w for w in args.workloads.split(",") if w}
     elif selected is None and not args.no_workloads:
-        wanted = {"segmented", "map", "sort_paths", "serving"}
+        wanted = {"segmented", "map", "funnels", "sort_paths", "serving"}
     else:
         wanted = set()
     lib.parallax_set_async(1)
@@ -714,6 +714,8 @@ def main() -> None:
                                                {o for o in args.seg_ops.split(",") if o} or None)
     if "map" in wanted:
         workloads["map"] = run_map(px, lib, torch, stream, args.steps, args.warmup, peak)
+    if "funnels" in wanted:
+        workloads["funnels"] = run_funnels(px, lib, torch, stream, args.steps, args.warmup, peak)
     if "sort_paths" in wanted:
         workloads["sort_paths"] = run_sort_paths(px, lib, torch, stream, args.steps, args.warmup,
                                                  peak)
@@ -871,6 +873,80 @@ def run_segmented(px, lib, torch, stream, steps: int, warmup: int, peak: float,
             "elements": total, "GB_s": round(tot_bytes / tot_ms / 1e6, 1),
             "frac_of_peak": round(tot_bytes / tot_ms / 1e6 / peak, 3), "ms": round(tot_ms, 3),
             "per_op": per_op}
+
+
+def run_funnels(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dict:
+    """The transform_reduce funnel's two ABI calls (stdpar.hpp:251-259: transform2 of an
+    int32 -> fp64 transform, x * 0.5, then the '+' reduce of its output) over 2^28
+    device-resident int32 U[-1000,1000] (seed 3). The transform is a registered image that
+    also exports its element function as LTO-IR (tests/images/xform_half_i32_to_f64_lto.cu,
+    standing in for compiler output), so the runtime fuses the pair into one pass; the same
+    image under a plain transform key, followed by the built-in reduce, is the two-pass path
+    the reference runs. Both sums are checked exactly (multiples of 0.5, exact in fp64)."""
+    img = ROOT / "tests" / "images" / "_build" / "xform_half_i32_to_f64_lto.fatbin"
+    if not img.exists():
+        return {"skipped": f"{img.name} not built (tests/images/build_images.py)"}
+    data = img.read_bytes()
+    data += b"\0" * (-len(data) % 4)
+    words = (C.c_uint32 * (len(data) // 4)).from_buffer_copy(data)
+    sz = "std::size_t = long unsigned int"
+    tr = ("U parallax::detail::device_transform_reduce(const T*, std::size_t, F) "
+          f"[with T = int; U = double; F = HalfBench; {sz}]")
+    tf = ("void parallax::detail::device_transform(const Tin*, Tout*, std::size_t, F) "
+          f"[with Tin = int; Tout = double; F = HalfBench; {sz}]")
+    for k in (tr + ":xform", tf):
+        lib.parallax_kernel_register(k.encode(), C.cast(words, C.c_void_p), len(words))
+    kx, kr = lib.parallax_kernel_lookup((tr + ":xform").encode()), lib.parallax_kernel_lookup((tr + ":reduce").encode())
+    kt, kr2 = lib.parallax_kernel_lookup(tf.encode()), px.builtin("reduce:sum:f64")
+    if not (kx and kr and kt and kr2):
+        return {"skipped": "funnel keys did not resolve"}
+    n = 1 << 28
+    x = gen("i32_pm1000", 3, n)
+    want = float(x.astype(np.int64).sum()) * 0.5
+    blocks = []
+
+    def block(nbytes, src=None):
+        p = lib.parallax_arena_alloc(nbytes, 256)
+        if not p:
+            raise RuntimeError("arena allocation failed")
+        blocks.append(p)
+        if src is not None:
+            np.ctypeslib.as_array((C.c_ubyte * nbytes).from_address(p))[:] = src.view(np.uint8)
+        lib.parallax_arena_set_residency(C.c_void_p(p), px.DEVICE_RESIDENT)
+        if src is not None:
+            lib.parallax_arena_sync_to_device(C.c_void_p(p), nbytes)
+        return p
+
+    lib.parallax_set_async(0)  # the funnel's calls are synchronous
+    try:
+        pin, pout = block(n * 4, x), block(n * 8)
+        res = np.zeros(1, np.float64)
+
+        def pair(kxf, krd):
+            def fn():
+                lib.parallax_kernel_launch_transform2(kxf, C.c_void_p(pin), C.c_void_p(pout), n, 4, 8)
+                lib.parallax_reduce(krd, C.c_void_p(pout), n, 8, res.ctypes.data)
+            return fn
+
+        out = {"workload": ("transform_reduce funnel: 2^28 int32 U[-1000,1000] (seed 3) -> fp64 "
+                            "x * 0.5 -> '+', device-resident; GB/s on the n*4 basis (one read of "
+                            "the input)")}
+        for name, fn in (("fused", pair(kx, kr)), ("two_pass", pair(kt, kr2))):
+            before = lib.parallax_launch_count()
+            ms = timed_calls(torch, stream, fn, steps, warmup)
+            px.check(f"funnel {name}")
+            if res[0] != want:
+                raise RuntimeError(f"funnel {name}: sum {res[0]} != {want}")
+            launches = (lib.parallax_launch_count() - before) / (steps + warmup)
+            out[name] = {"ms": round(ms, 4), "GB_s": round(n * 4 / ms / 1e6, 1),
+                         "frac_of_peak": round(n * 4 / ms / 1e6 / peak, 3),
+                         "launches_per_call": launches}
+        out["speedup"] = round(out["two_pass"]["ms"] / out["fused"]["ms"], 2)
+        return out
+    finally:
+        for p in blocks:
+            lib.parallax_arena_free(C.c_void_p(p))
+        lib.parallax_set_async(1)
 
 
 def run_map(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dict:

@@ -14,6 +14,21 @@
  * 148 * 16 blocks; the kernel must cover args.count elements with a grid-stride loop.
  * Stored host pointers into the arena are relocated in the kernel with
  *     device_address = args.dev_base + (host_pointer - args.host_base).
+ *
+ * Fusable transforms. A transform image registered under the key of a transform_reduce
+ * (":xform") or count_if (":pred") funnel may also export its per-element function,
+ *
+ *     extern "C" __device__ void parallax_elem(const void* in, void* out);
+ *
+ * (reads one input element at `in`, writes the transformed element at `out`), as LTO-IR,
+ * i.e. compiled relocatable with an LTO target beside the machine code:
+ *
+ *     nvcc -rdc=true -fatbin -gencode arch=compute_100a,code=[sm_100a,lto_100a] ...
+ *
+ * The runtime then links that function into its own reduce tile (nvJitLink, link-time
+ * optimisation) and runs the funnel's transform2 + reduce pair as one pass over the input:
+ * the transform2 call is held back until the reduce of its output, and any other call on
+ * the same thread runs it first. An image without parallax_elem runs as two passes.
  */
 #ifndef PARALLAX_KERNEL_ABI_H
 #define PARALLAX_KERNEL_ABI_H

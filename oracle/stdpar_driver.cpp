@@ -28,6 +28,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -159,6 +160,7 @@ bool register_all(const std::string& dir) {
     const std::string xf = "void parallax::detail::device_transform(const Tin*, Tout*, std::size_t, F) [with Tin = int; Tout = double; F = HalfD";
     const std::string cnt = "long int parallax::detail::device_count_if(const T*, std::size_t, Pred) [with T = float; Pred = GtHalf";
     const std::string gat = "void parallax::detail::device_transform(const Tin*, Tout*, std::size_t, F) [with Tin = Rec; Tout = float; F = GatherPlus";
+    const std::string trd = "U parallax::detail::device_transform_reduce(const T*, std::size_t, F) [with T = int; U = double; F = HalfD";
     bool ok = true;
     ok &= register_image(dir, cpy + SZ + ":flags", "flags_mod3_i32");
     ok &= register_image(dir, rem + SZ + ":flags", "flags_not_mod3_i32");
@@ -166,7 +168,10 @@ bool register_all(const std::string& dir) {
     ok &= register_image(dir, inv + "Affine" + SZ, "affine_f32");
     ok &= register_image(dir, inv + "AffineDefault" + SZ, "affine_f32");
     ok &= register_image(dir, xf + SZ, "half_i32_to_f64");
-    ok &= register_image(dir, cnt + SZ + ":pred", "pred_gt_half_f32");
+    // transforms that also export their element function (LTO-IR): the runtime fuses each
+    // funnel's transform + reduce into one pass
+    ok &= register_image(dir, cnt + SZ + ":pred", "pred_gt_half_f32_lto");
+    ok &= register_image(dir, trd + SZ + ":xform", "xform_half_i32_to_f64_lto");
     ok &= register_image(dir, gat + SZ, "saxpy_gather_f32");
     return ok;
 }
@@ -274,6 +279,13 @@ void run(size_t n) {
         b = launches();
         long cnt = parallax::count_if(P, c.begin(), c.end(), GtHalf{});
         record_scalar("count_if_gt_half_f32" + sfx, b, (uint64_t)cnt);
+        auto t = i32_pm1000(24, n);
+        b = launches();
+        const double tr = parallax::transform_reduce(P, t.begin(), t.end(), 0.0, std::plus<>{},
+                                                     HalfD{});
+        uint64_t tr_bits;
+        memcpy(&tr_bits, &tr, sizeof tr_bits);
+        record_scalar("transform_reduce_half_i32" + sfx, b, tr_bits);
     }
     {  // where the heap lives, and a transform that chases pointers stored in heap records
         std::vector<float> tgt = f32_unit(28, n);

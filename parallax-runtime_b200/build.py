@@ -1,7 +1,9 @@
 """Build recipe for libparallax-runtime.so (sm_100a).
 
 Compiles every CUDA/C++ source under csrc/ with nvcc for sm_100a and links one shared
-library, lib/libparallax-runtime.so, that exports the parallax C ABI. Objects go to
+library, lib/libparallax-runtime.so, that exports the parallax C ABI. Modules under
+csrc/lto/ are compiled to LTO-IR and embedded in the library as data instead: the runtime
+links them with registered images at run time (nvJitLink). Objects go to
 _build/ and are rebuilt when a source or any header is newer than the object. The
 serving-mix load generator (loadgen/loadgen.cpp, host C++ over the public ABI) is linked
 against it as lib/libparallax-loadgen.so, and the whole-heap capture shim
@@ -42,8 +44,45 @@ def nvcc() -> str:
     return cand
 
 
+LTO_DIR = CSRC / "lto"
+
+
 def sources() -> list[Path]:
-    return sorted(CSRC.rglob("*.cu"))
+    # csrc/lto/ holds modules linked at run time (embedded as LTO-IR), not library code
+    return sorted(s for s in CSRC.rglob("*.cu") if LTO_DIR not in s.parents)
+
+
+def build_lto_embed(force: bool, newest_header: float) -> Path:
+    """Compiles every module under csrc/lto/ to an LTO-IR fatbin for sm_100a and writes an
+    object that embeds the fatbins as byte arrays (pxb_lto_<stem>, pxb_lto_<stem>_size),
+    which the runtime hands to nvJitLink together with a registered image."""
+    obj = BUILD / "lto_embed.o"
+    srcs = sorted(LTO_DIR.glob("*.cu"))
+    newest = max([newest_header, *(s.stat().st_mtime for s in srcs)])
+    if not force and obj.exists() and obj.stat().st_mtime >= newest:
+        return obj
+    lines = ["#include <stddef.h>", "/* generated by build.py: LTO-IR fatbins of csrc/lto */"]
+    for src in srcs:
+        fat = BUILD / f"lto_{src.stem}.fatbin"
+        cmd = [nvcc(), "-std=c++17", "-O3", "-rdc=true", "-fatbin",
+               "-gencode", "arch=compute_100a,code=lto_100a", "-I", str(ROOT / "include"),
+               "-o", str(fat), str(src)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stdout}\n{r.stderr}")
+        data = fat.read_bytes()
+        body = ",".join(str(b) for b in data)
+        lines.append(f"__attribute__((visibility(\"hidden\"), aligned(16))) const unsigned char "
+                     f"pxb_lto_{src.stem}[{len(data)}] = {{{body}}};")
+        lines.append(f"__attribute__((visibility(\"hidden\"))) const size_t "
+                     f"pxb_lto_{src.stem}_size = {len(data)};")
+    gen = BUILD / "lto_embed.c"
+    gen.write_text("\n".join(lines) + "\n")
+    cmd = ["gcc", "-O0", "-fPIC", "-c", str(gen), "-o", str(obj)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"lto embed compile failed:\n{r.stdout}\n{r.stderr}")
+    return obj
 
 
 def headers() -> list[Path]:
@@ -82,6 +121,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False,
     with cf.ThreadPoolExecutor(jobs) as ex:
         results = list(ex.map(lambda s: compile_one(s, newest_header, force or ptxas_verbose, extra), srcs))
     objs = [o for o, _ in results]
+    objs.append(build_lto_embed(force, newest_header))
     if verbose or ptxas_verbose:
         for o, log in results:
             if log:

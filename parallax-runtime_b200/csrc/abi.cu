@@ -88,9 +88,13 @@ using namespace pxb;
 
 namespace {
 
-// Common prologue: handle + workspace + element-size check.
+void settle_deferred(Workspace& ws);
+
+// Common prologue: handle + workspace + element-size check. A transform held back on this
+// thread (Workspace::deferred) runs first.
 Workspace* begin(Handle* h, const char* fn, size_t elem_size, std::initializer_list<Kind> kinds) {
     set_ok();
+    if (Workspace* cur = current_workspace()) settle_deferred(*cur);
     if (!h) {
         set_error(PARALLAX_ERR_INVALID_HANDLE, "%s: invalid kernel handle", fn);
         return nullptr;
@@ -208,12 +212,33 @@ void map_inplace(const char* fn, parallax_kernel_t kernel, void* buffer, size_t 
     finish(*ws);
 }
 
+// Keys of the funnels whose transform feeds a '+' reduce of its output and nothing else
+// (stdpar.hpp:245-293): device_transform_reduce<T, U, F> ":xform" and device_count_if<T,
+// Pred> ":pred". The funnel frees the staging buffer right after the reduce and never reads
+// it, so the two calls may run as one fused pass.
+bool fusable_funnel_key(const std::string& k) {
+    auto ends_with = [&](const char* suf) {
+        const size_t n = strlen(suf);
+        return k.size() >= n && k.compare(k.size() - n, n, suf) == 0;
+    };
+    return (k.find("device_transform_reduce") != std::string::npos && ends_with(":xform")) ||
+           (k.find("device_count_if") != std::string::npos && ends_with(":pred"));
+}
+
 void map_transform(const char* fn, parallax_kernel_t kernel, void* in, void* out, size_t count,
-                   size_t in_es, size_t out_es, void* captures, size_t capture_size) {
+                   size_t in_es, size_t out_es, void* captures, size_t capture_size,
+                   bool may_defer = true) {
     Handle* h = as_handle(kernel);
     Workspace* ws = begin(h, fn, 0, {Kind::MAP, Kind::USER});
     if (!ws || count == 0) return;
     if (out_es == 0) out_es = in_es;
+    if (may_defer && h->kind == Kind::USER && !ws->async && capture_size == 0 &&
+        fusable_funnel_key(h->name) && xform_fusable(h)) {
+        // held back: the funnel's reduce of `out` runs both as one pass (parallax_reduce);
+        // any other call on this thread runs the transform first
+        ws->deferred = {h, in, out, count, in_es, out_es};
+        return;
+    }
     const bool chase = reads_through_pointers(h);
     if (chase && !arena_sync_coherent(*ws, true)) return;
     Operand oi, oo;
@@ -232,7 +257,38 @@ void map_transform(const char* fn, parallax_kernel_t kernel, void* in, void* out
     finish(*ws);
 }
 
+void settle_deferred(Workspace& ws) {
+    if (!ws.deferred.h) return;
+    const Workspace::Deferred d = ws.deferred;
+    ws.deferred = Workspace::Deferred();
+    map_transform("parallax_kernel_launch_transform2", reinterpret_cast<parallax_kernel_t>(d.h),
+                  d.in, d.out, d.n, d.in_es, d.out_es, nullptr, 0, false);
+}
+
+// The funnel's reduce of a held-back transform's output: one pass over the transform's
+// input, with the operand handling of the transform it replaces (a registered image may
+// read through stored arena pointers: every coherent block is uploaded before and
+// downloaded after, as for the transform alone).
+void fused_transform_reduce(Workspace& ws, const Workspace::Deferred& d, Handle* red,
+                            void* result) {
+    Handle* xf = d.h;
+    if (!arena_sync_coherent(ws, true)) return;
+    Operand oi;
+    if (!resolve_operand(ws, d.in, d.n * d.in_es, !arena_contains(d.in), 0, &oi)) return;
+    if (!launch_xform_reduce(ws, xf, red->dtype, oi.dev, d.n, d.in_es, ws.d_slot->result))
+        return;
+    if (!arena_sync_coherent(ws, false)) return;
+    if (sync_stream(ws) != PARALLAX_OK) return;
+    memcpy(result, ws.h_slot->result, dtype_size(red->dtype));
+}
+
 }  // namespace
+
+namespace pxb {
+void settle_deferred_here() {
+    if (Workspace* cur = current_workspace()) settle_deferred(*cur);
+}
+}  // namespace pxb
 
 // ---- element-wise launches ------------------------------------------------------------------
 
@@ -284,6 +340,17 @@ PXB_EXPORT void parallax_kernel_launch_with_captures(parallax_kernel_t kernel, v
 PXB_EXPORT void parallax_reduce(parallax_kernel_t kernel, void* data, size_t count,
                                 size_t elem_size, void* result) {
     Handle* h = as_handle(kernel);
+    if (Workspace* cur = current_workspace(); cur && cur->deferred.h) {
+        const Workspace::Deferred d = cur->deferred;
+        if (h && h->kind == Kind::REDUCE && h->op == RedOp::SUM && result && data == d.out &&
+            count == d.n && elem_size == d.out_es && dtype_size(h->dtype) == d.out_es &&
+            !cur->async) {
+            cur->deferred = Workspace::Deferred();
+            set_ok();
+            fused_transform_reduce(*cur, d, h, result);
+            return;
+        }
+    }
     Workspace* ws = begin(h, "parallax_reduce", elem_size, {Kind::REDUCE});
     if (!ws) return;
     if (!result) {
@@ -393,7 +460,7 @@ PXB_EXPORT void parallax_sort(parallax_kernel_t kernel, void* data, size_t count
     size_t bytes = count * dtype_size(h->dtype);
     Operand op;
     if (!resolve_operand(*ws, data, bytes, true, 0, &op)) return;
-    if (!launch_sort(*ws, h->dtype, op.dev, count)) return;
+    if (!launch_sort(*ws, h->dtype, op.dev, count, h->kind == Kind::SORT_KV)) return;
     if (!writeback_operand(*ws, op, bytes)) return;
     finish(*ws);
 }

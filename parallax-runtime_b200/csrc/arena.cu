@@ -432,7 +432,10 @@ PXB_EXPORT void* parallax_arena_alloc(size_t size, size_t align) {
         fprintf(stderr, "[parallax_arena_alloc] %zu bytes -> %p\n", size, p);
     return p;
 }
-PXB_EXPORT void parallax_arena_free(void* ptr) { arena().deallocate(ptr); }
+PXB_EXPORT void parallax_arena_free(void* ptr) {
+    settle_deferred_here();  // a held-back transform may read or write this block
+    arena().deallocate(ptr);
+}
 PXB_EXPORT int parallax_arena_contains(const void* ptr) {
     Arena& a = arena();
     if (!a.ok) {
@@ -446,6 +449,7 @@ PXB_EXPORT void* parallax_umalloc(size_t size, unsigned) { return parallax_arena
 PXB_EXPORT void parallax_ufree(void* ptr) { parallax_arena_free(ptr); }
 
 PXB_EXPORT int parallax_arena_set_residency(void* ptr, int mode) {
+    settle_deferred_here();
     if (mode != PARALLAX_COHERENT && mode != PARALLAX_DEVICE_RESIDENT)
         return PARALLAX_ERR_INVALID_ARGUMENT;
     return arena().set_residency(ptr, mode) ? PARALLAX_OK : PARALLAX_ERR_INVALID_ARGUMENT;
@@ -482,6 +486,7 @@ PXB_EXPORT size_t parallax_arena_mapped(void) {
 }
 
 static int arena_copy(const void* ptr, size_t bytes, bool to_device) {
+    settle_deferred_here();
     Workspace* ws = workspace();
     if (!ws) return PARALLAX_ERR_NO_DEVICE;
     ArenaBlock b;

@@ -92,6 +92,8 @@ static std::mutex g_ws_mu;
 static std::vector<Workspace*>* g_ws_list = nullptr;
 static thread_local Workspace* tls_ws = nullptr;
 
+Workspace* current_workspace() { return tls_ws; }
+
 Workspace* workspace() {
     if (tls_ws) return tls_ws;
     tls_ws = new_workspace();
@@ -207,6 +209,25 @@ void* Workspace::radix(size_t bytes) {
     radix_epoch = 1;
     ++generation;
     return d_radix;
+}
+
+void* Workspace::seg_radix(size_t bytes) {
+    if (bytes <= seg_radix_cap) return d_seg_radix;
+    cudaStream_t s = stream();
+    if (d_seg_radix) {
+        if (!cuda_ok(cudaStreamSynchronize(s), "segmented radix buffer sync")) return nullptr;
+        cudaFree(d_seg_radix);
+        d_seg_radix = nullptr;
+        seg_radix_cap = 0;
+    }
+    size_t cap = 1 << 20;
+    while (cap < bytes) cap <<= 1;
+    if (!cuda_ok(cudaMalloc(&d_seg_radix, cap), "cudaMalloc(segmented radix buffer)")) return nullptr;
+    if (!cuda_ok(cudaMemsetAsync(d_seg_radix, 0, cap, s), "cudaMemset(segmented radix buffer)"))
+        return nullptr;
+    seg_radix_cap = cap;
+    ++generation;
+    return d_seg_radix;
 }
 
 bool Workspace::copy_streams() {
@@ -455,18 +476,21 @@ PXB_EXPORT const char* parallax_error_string(int status) {
 }
 
 PXB_EXPORT int parallax_set_stream(void* cuda_stream) {
+    settle_deferred_here();
     Workspace* ws = workspace();
     if (!ws) return PARALLAX_ERR_NO_DEVICE;
     ws->user_stream = static_cast<cudaStream_t>(cuda_stream);
     return PARALLAX_OK;
 }
 PXB_EXPORT int parallax_set_async(int async) {
+    settle_deferred_here();
     Workspace* ws = workspace();
     if (!ws) return PARALLAX_ERR_NO_DEVICE;
     ws->async = async != 0;
     return PARALLAX_OK;
 }
 PXB_EXPORT int parallax_synchronize(void) {
+    settle_deferred_here();
     Workspace* ws = workspace();
     if (!ws) return PARALLAX_ERR_NO_DEVICE;
     int st = sync_stream(*ws);

@@ -30,6 +30,7 @@
 #include <string.h>
 
 #include "../runtime.hpp"
+#include "../segplan.cuh"
 #include "../sortkey.cuh"
 #include "../tiles.cuh"
 
@@ -154,14 +155,29 @@ __device__ __forceinline__ T digit_exclusive_scan(T v, T* part) {
     return before + inc - v;
 }
 
+// Segmented mode of a digit pass (many segments, each sorted on its own, in one launch): the
+// claimed tile is work item `tile` of the planner's list (segplan.cuh), i.e. tile k of one
+// segment; offsets are segment-local, the look-back stops at the segment's first tile, and
+// that tile starts every digit's chain from the segment's own histogram.
+struct SegRadix {
+    SegSrc src;                   // segments: data at in_addr, temporary at aux_addr
+    const uint32_t* item_start;   // S + 1: first work item of every segment
+    const uint32_t* item_seg;     // work item -> segment
+    const uint32_t* seg_hist;     // [S][npos][256] digit counts of every segment
+    const uint32_t* epoch_base;   // this call's first pass epoch (device side)
+    uint64_t S;
+    uint32_t npos, pos;           // digit positions counted, this pass's position among them
+    uint32_t parity;              // 0: data -> temporary, 1: temporary -> data
+};
+
 // ---- one digit pass --------------------------------------------------------------------------
 // XF_IN transforms keys as they are read (the first pass reads the caller's values),
 // XF_OUT restores them as they are written (the last pass writes the caller's values).
-template <typename K, int XF_IN, int XF_OUT>
+template <typename K, int XF_IN, int XF_OUT, bool SEG = false>
 __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
-    k_radix_pass(const K* __restrict__ in, K* __restrict__ out, uint64_t n, int shift,
-                 const unsigned long long* __restrict__ hist, uint64_t* status, uint32_t epoch,
-                 uint64_t tiles, uint32_t* counters, volatile int32_t* err) {
+    k_radix_pass(const K* __restrict__ in_, K* __restrict__ out_, uint64_t n_, int shift,
+                 const unsigned long long* __restrict__ hist, uint64_t* status, uint32_t epoch_,
+                 uint64_t tiles, uint32_t* counters, volatile int32_t* err, SegRadix sr) {
     constexpr int BLOCK = RadixShape<K>::BLOCK, ITEMS = RadixShape<K>::ITEMS;
     constexpr int TILE = BLOCK * ITEMS, WARPS = BLOCK / 32;
     constexpr int TABLES = WARPS * kSubs, STREAM_ITEMS = ITEMS / kSubs;
@@ -193,14 +209,31 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     for (int i = lane; i < kSubs * kBins; i += 32) wm[i] = 0ull;
     __syncthreads();
     const uint64_t tile = s_tile;
-    if (tile >= tiles) {  // claim counter out of step: touch nothing
+    // plain: tile `tile` of the array; segmented: work item `tile` is tile tk of segment seg
+    const K* in = in_;
+    K* out = out_;
+    uint64_t n = n_, tk = tile, seg = 0;  // tk: tile index within the array / segment
+    uint32_t epoch = epoch_;
+    if constexpr (SEG) {
+        if (tile >= sr.item_start[sr.S]) {  // the grid is an upper bound of the work items
+            if (tid == 0) persistent_exit(counters);
+            return;
+        }
+        seg = sr.item_seg[tile];
+        tk = tile - sr.item_start[seg];
+        n = sr.src.len(seg);
+        const uint64_t a = sr.src.in_addr(seg), b = sr.src.aux_addr(seg);
+        in = reinterpret_cast<const K*>(sr.parity ? b : a);
+        out = reinterpret_cast<K*>(sr.parity ? a : b);
+        epoch = *sr.epoch_base + sr.pos;
+    } else if (tile >= tiles) {  // claim counter out of step: touch nothing
         if (tid == 0) {
             *err = kErrRadixRange;
             persistent_exit(counters);
         }
         return;
     }
-    const uint64_t base = tile * TILE;
+    const uint64_t base = tk * TILE;
     const uint64_t rem = n - base;
     const uint32_t valid = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
 
@@ -273,15 +306,20 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
             s_wh[w * kBins + tid] = cnt;
             cnt += c;
         }
-        if (tile != 0)
+        if (tk != 0)
             st_relaxed_u64(&status[tile * kBins + tid],
                            ((uint64_t)epoch << kEpochShift) | kStAgg | cnt);
     }
     const uint32_t loc = digit_exclusive_scan<uint32_t, BLOCK>(tid < kBins ? cnt : 0u, s_part32);
-    uint64_t start = 0;  // tile 0: the digit's first output position
-    if (tile == 0)
-        start = digit_exclusive_scan<uint64_t, BLOCK>(tid < kBins ? (uint64_t)hist[tid] : 0ull,
-                                                      s_part64);
+    uint64_t start = 0;  // first tile: the digit's first output position
+    if (tk == 0) {
+        uint64_t h = 0;
+        if (tid < kBins) {
+            if constexpr (SEG) h = sr.seg_hist[(seg * sr.npos + sr.pos) * kBins + tid];
+            else h = hist[tid];
+        }
+        start = digit_exclusive_scan<uint64_t, BLOCK>(h, s_part64);
+    }
     if (tid < kBins) {
 #pragma unroll 8
         for (int w = 0; w < TABLES; ++w) s_wh[w * kBins + tid] += loc;
@@ -301,7 +339,7 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
     // are then consumed in order until an inclusive count ends the walk.
     if (tid < kBins) {
         uint64_t excl = start;
-        if (tile != 0) {
+        if (tk != 0) {  // (segmented: the walk ends at the segment's first tile, always INC)
             bool done = false;
             for (int64_t j = (int64_t)tile - 1; !done && j >= 0; j -= kLookWindow) {
                 uint64_t w[kLookWindow];
@@ -361,12 +399,166 @@ bool launch_pass(const K* in, K* out, uint64_t n, int shift, const unsigned long
     if (!smem_opt_in<k_radix_pass<K, XF_IN, XF_OUT>>(smem))
         return cuda_ok(cudaGetLastError(), "k_radix_pass shared-memory opt-in");
     k_radix_pass<K, XF_IN, XF_OUT><<<(unsigned)tiles, RadixShape<K>::BLOCK, smem, s>>>(
-        in, out, n, shift, hist, status, epoch, tiles, counters, err);
+        in, out, n, shift, hist, status, epoch, tiles, counters, err, SegRadix{});
     return true;
 }
 
+// ---- segmented radix sort -------------------------------------------------------------------
+// Digit counts of every segment for digit positions p0 .. P-1, one CTA per work item (tile):
+// shared-memory counts of the tile, then one global atomic add per nonzero (position,
+// digit). seg_hist must be zero on entry.
+constexpr int kSegHistBlock = 512;
+
 template <typename K, int XF>
-bool radix_sort_keys(Workspace& ws, void* d_data, uint64_t n) {
+__global__ void __launch_bounds__(kSegHistBlock)
+    k_seg_radix_hist(SegRadix sr, int p0, uint32_t* __restrict__ seg_hist) {
+    constexpr int P = sizeof(K);
+    constexpr int TILE = RadixShape<K>::BLOCK * RadixShape<K>::ITEMS;
+    __shared__ uint32_t h[P][kBins];
+    const uint32_t item = blockIdx.x;
+    if (item >= sr.item_start[sr.S]) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < P * kBins; i += kSegHistBlock) (&h[0][0])[i] = 0u;
+    __syncthreads();
+    const uint64_t seg = sr.item_seg[item];
+    const uint64_t k = item - sr.item_start[seg];
+    const uint64_t len = sr.src.len(seg);
+    const K* in = reinterpret_cast<const K*>(sr.src.in_addr(seg)) + k * TILE;
+    const uint64_t rem = len - k * TILE;
+    const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+    for (uint32_t i = tid; i < cnt; i += kSegHistBlock) {
+        const K key = to_key<K, XF>(__ldcs(in + i));
+        for (int p = p0; p < P; ++p) atomicAdd(&h[p][digit_of(key, 8 * p)], 1u);
+    }
+    __syncthreads();
+    const int npos = P - p0;
+    for (int i = tid; i < npos * kBins; i += kSegHistBlock) {
+        const uint32_t v = h[p0 + i / kBins][i % kBins];
+        if (v) atomicAdd(&seg_hist[(seg * npos + i / kBins) * kBins + i % kBins], v);
+    }
+}
+
+// Advances the device-side epoch of the segmented radix words by `npass` (so every replay
+// of a captured call uses new epochs) and records this call's first epoch in counters[3].
+// When the 22-bit epoch would wrap, the look-back words are cleared first.
+__global__ void __launch_bounds__(256)
+    k_seg_radix_epoch(uint32_t* counters, uint32_t npass, uint64_t* status, uint64_t words) {
+    __shared__ uint32_t s_base;
+    __shared__ bool s_wrap;
+    if (threadIdx.x == 0) {
+        uint32_t e = counters[2];
+        if (e == 0) e = 1;  // a zeroed buffer: words of epoch 0 never match
+        s_wrap = e + npass >= (1u << (64 - kEpochShift));
+        s_base = s_wrap ? 1u : e;
+    }
+    __syncthreads();
+    if (s_wrap)
+        for (uint64_t i = threadIdx.x; i < words; i += 256) status[i] = 0ull;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        counters[2] = s_base + npass;
+        counters[3] = s_base;
+    }
+}
+
+template <typename K, int XF_IN, int XF_OUT>
+bool launch_seg_pass(const SegRadix& sr, int shift, uint64_t* status, uint32_t* counters,
+                     volatile int32_t* err, uint64_t items_cap, cudaStream_t s) {
+    constexpr size_t smem = radix_smem<K>();
+    if (!smem_opt_in<k_radix_pass<K, XF_IN, XF_OUT, true>>(smem))
+        return cuda_ok(cudaGetLastError(), "k_radix_pass shared-memory opt-in");
+    k_radix_pass<K, XF_IN, XF_OUT, true><<<(unsigned)items_cap, RadixShape<K>::BLOCK, smem, s>>>(
+        nullptr, nullptr, 0, shift, nullptr, status, 0, items_cap, counters, err, sr);
+    return true;
+}
+
+// S segments (CSR offsets or descriptors, segplan.cuh), each sorted in place by digit
+// positions p0 .. P-1 (p0 = 4 on 8-byte records: stably by the high 32 bits). Launches: the
+// planner (+ item map), a histogram clear, the segment histograms, the epoch step and one
+// launch per digit pass; all capturable in a CUDA graph (device-side epochs).
+template <typename K, int XF>
+bool seg_radix_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, int p0,
+                         bool graph) {
+    constexpr int P = sizeof(K);
+    constexpr int TILE = RadixShape<K>::BLOCK * RadixShape<K>::ITEMS;
+    const uint64_t items_cap = S + count / TILE + 1;
+    const uint32_t npos = (uint32_t)(P - p0);
+    if (items_cap >= 0x7fffffffull || (npos % 2) != 0) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "segmented sort: too many tiles");
+        return false;
+    }
+    auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+    const bool csr_tmp = src.offsets != nullptr;
+    const size_t tmp_bytes = csr_tmp ? up(count * sizeof(K)) : 0;
+    const size_t hist_bytes = up(S * npos * kBins * sizeof(uint32_t));
+    char* t = static_cast<char*>(ws.temp(tmp_bytes + hist_bytes));
+    char* sb = static_cast<char*>(ws.seg(256 + up((S + 1) * 4) + up(items_cap * 4)));
+    StatusEntry* st = static_cast<StatusEntry*>(ws.seg_status(1));
+    const uint64_t words = items_cap * kBins;
+    char* rb = static_cast<char*>(ws.seg_radix(256 + words * 8));
+    if (!t || !sb || !st || !rb) return false;
+    if (csr_tmp) src.aux = reinterpret_cast<uint64_t>(t);
+    src.aux_stride = 0;
+    src.elem = sizeof(K);
+    uint32_t* plan_counters = reinterpret_cast<uint32_t*>(sb);
+    uint32_t* item_start = reinterpret_cast<uint32_t*>(sb + 256);
+    uint32_t* item_seg = reinterpret_cast<uint32_t*>(sb + 256 + up((S + 1) * 4));
+    uint32_t* seg_hist = reinterpret_cast<uint32_t*>(t + tmp_bytes);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(rb);
+    uint64_t* status = reinterpret_cast<uint64_t*>(rb + 256);
+    volatile int32_t* err = &ws.d_slot->spin_error;
+    cudaStream_t s = ws.stream();
+
+    SegRadix sr{};
+    sr.src = src;
+    sr.item_start = item_start;
+    sr.item_seg = item_seg;
+    sr.seg_hist = seg_hist;
+    sr.epoch_base = counters + 3;
+    sr.S = S;
+    sr.npos = npos;
+    ProfScope prof(ws, "segmented_radix_sort", 2 * count * sizeof(K));
+    count_launch(4 + npos);
+    auto enqueue = [&]() -> bool {
+        k_seg_plan<256><<<1, 256, 0, s>>>(src, S, count, (uint32_t)TILE, item_start, plan_counters,
+                                          SegEmpty::NONE, nullptr, st, ws.seg_status_cap, err,
+                                          items_cap <= kInlineItems ? item_seg : nullptr);
+        if (items_cap > kInlineItems)
+            k_seg_map<256><<<seg_map_grid(S), 256, 0, s>>>(item_start, S, item_seg);
+        if (!cuda_ok(cudaMemsetAsync(seg_hist, 0, hist_bytes, s), "segment histogram clear"))
+            return false;
+        k_seg_radix_hist<K, XF><<<(unsigned)items_cap, kSegHistBlock, 0, s>>>(sr, p0, seg_hist);
+        k_seg_radix_epoch<<<1, 256, 0, s>>>(counters, npos, status, words);
+        for (int p = p0; p < P; ++p) {
+            SegRadix q = sr;
+            q.pos = (uint32_t)(p - p0);
+            q.parity = (uint32_t)((p - p0) & 1);
+            bool ok;
+            if (p == p0 && p == P - 1)
+                ok = launch_seg_pass<K, XF, XF>(q, 8 * p, status, counters, err, items_cap, s);
+            else if (p == p0)
+                ok = launch_seg_pass<K, XF, 0>(q, 8 * p, status, counters, err, items_cap, s);
+            else if (p == P - 1)
+                ok = launch_seg_pass<K, 0, XF>(q, 8 * p, status, counters, err, items_cap, s);
+            else
+                ok = launch_seg_pass<K, 0, 0>(q, 8 * p, status, counters, err, items_cap, s);
+            if (!ok) return false;
+        }
+        return cuda_ok(cudaGetLastError(), "segmented radix sort launch");
+    };
+    if (!graph) return enqueue();
+    char key[256];
+    snprintf(key, sizeof key, "segradix/%d/%d/%d/%p/%p/%llu/%llu", (int)sizeof(K), XF, p0,
+             (const void*)src.in, (const void*)src.offsets, (unsigned long long)S,
+             (unsigned long long)count);
+    return graph_launch(ws, key, enqueue);
+}
+
+// Digit passes p0 .. P-1: p0 = 0 sorts by the whole key; p0 = 4 on 8-byte records sorts
+// them stably by their high 32 bits alone (LSD passes are stable), the (key << 32 | value)
+// records of a sort_kv handle.
+template <typename K, int XF>
+bool radix_sort_keys(Workspace& ws, void* d_data, uint64_t n, int p0 = 0) {
     constexpr int P = sizeof(K);
     constexpr int TILE = RadixShape<K>::BLOCK * RadixShape<K>::ITEMS;
     const uint64_t tiles = (n + TILE - 1) / TILE;
@@ -406,14 +598,14 @@ bool radix_sort_keys(Workspace& ws, void* d_data, uint64_t n) {
     }
     count_launch();
     static_assert(P % 2 == 0, "an even number of passes ends in the caller's array");
-    for (int p = 0; p < P; ++p) {
-        const K* src = (p % 2 == 0) ? data : tmp;
-        K* dst = (p % 2 == 0) ? tmp : data;
+    for (int p = p0; p < P; ++p) {  // P - p0 is even, so the last pass ends in `data`
+        const K* src = ((p - p0) % 2 == 0) ? data : tmp;
+        K* dst = ((p - p0) % 2 == 0) ? tmp : data;
         const unsigned long long* hp = hist + (size_t)p * kBins;
         bool ok;
         {
             ProfScope prof(ws, "k_radix_pass", 2 * n * sizeof(K));
-            if (p == 0)
+            if (p == p0)
                 ok = launch_pass<K, XF, 0>(src, dst, n, 8 * p, hp, status, ep0 + p, counters, err,
                                            tiles, s);
             else if (p == P - 1)
@@ -431,7 +623,41 @@ bool radix_sort_keys(Workspace& ws, void* d_data, uint64_t n) {
 
 }  // namespace
 
-bool launch_radix_sort(Workspace& ws, DType t, void* d_data, size_t n) {
+bool launch_segmented_radix_sort(Workspace& ws, DType t, const SegSrc& src, uint64_t count,
+                                 uint64_t S, bool by_key, bool graph) {
+    if (by_key) {
+        if (t != DType::U64) {
+            set_error(PARALLAX_ERR_INVALID_ARGUMENT, "segmented sort: by-key sorts 8-byte records");
+            return false;
+        }
+        return seg_radix_sort_keys<uint64_t, 0>(ws, src, count, S, 4, graph);
+    }
+    switch (t) {
+        case DType::U32: return seg_radix_sort_keys<uint32_t, 0>(ws, src, count, S, 0, graph);
+        case DType::I32: return seg_radix_sort_keys<uint32_t, 1>(ws, src, count, S, 0, graph);
+        case DType::F32: return seg_radix_sort_keys<uint32_t, 2>(ws, src, count, S, 0, graph);
+        case DType::U64: return seg_radix_sort_keys<uint64_t, 0>(ws, src, count, S, 0, graph);
+        case DType::I64: return seg_radix_sort_keys<uint64_t, 1>(ws, src, count, S, 0, graph);
+        case DType::F64: return seg_radix_sort_keys<uint64_t, 2>(ws, src, count, S, 0, graph);
+        default: break;
+    }
+    set_error(PARALLAX_ERR_INVALID_ARGUMENT, "segmented sort: unsupported element type");
+    return false;
+}
+
+uint64_t segmented_radix_tile(DType t) {
+    return dtype_size(t) == 4 ? (uint64_t)RadixShape<uint32_t>::BLOCK * RadixShape<uint32_t>::ITEMS
+                              : (uint64_t)RadixShape<uint64_t>::BLOCK * RadixShape<uint64_t>::ITEMS;
+}
+
+bool launch_radix_sort(Workspace& ws, DType t, void* d_data, size_t n, bool by_key) {
+    if (by_key) {
+        if (t != DType::U64) {
+            set_error(PARALLAX_ERR_INVALID_ARGUMENT, "sort: by-key sorts 8-byte records");
+            return false;
+        }
+        return radix_sort_keys<uint64_t, 0>(ws, d_data, n, 4);
+    }
     switch (t) {
         case DType::U32: return radix_sort_keys<uint32_t, 0>(ws, d_data, n);
         case DType::I32: return radix_sort_keys<uint32_t, 1>(ws, d_data, n);

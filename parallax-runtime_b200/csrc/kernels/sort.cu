@@ -600,8 +600,16 @@ bool seg_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, uint64
     return graph_launch(ws, key, enqueue);
 }
 
+// by_key (sort_kv records, stable by key) always takes the segmented radix sort; plain keys
+// take it when the mean segment spans at least one radix tile, the merge sort otherwise.
 bool seg_sort_dispatch(Workspace& ws, DType t, const SegSrc& src, uint64_t count, uint64_t S,
-                       uint64_t max_len, bool graph) {
+                       uint64_t max_len, bool graph, bool by_key) {
+    bool radix = by_key || count / S >= segmented_radix_tile(t);
+    if (const char* e = getenv("PARALLAX_SORT")) {
+        if (!strcmp(e, "merge") && !by_key) radix = false;
+        else if (!strcmp(e, "radix")) radix = true;
+    }
+    if (radix) return launch_segmented_radix_sort(ws, t, src, count, S, by_key, graph);
     switch (t) {
         case DType::U32: return seg_sort_keys<uint32_t, 0>(ws, src, count, S, max_len, graph);
         case DType::I32: return seg_sort_keys<uint32_t, 1>(ws, src, count, S, max_len, graph);
@@ -625,8 +633,10 @@ constexpr size_t kRadixMin8 = size_t(1) << 19;
 
 size_t sort_radix_min(DType t) { return dtype_size(t) == 4 ? kRadixMin4 : kRadixMin8; }
 
-bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
+bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n, bool by_key) {
     if (n <= 1) return true;
+    // stable by key at every size: only the radix passes over the key bytes give that
+    if (by_key) return launch_radix_sort(ws, t, d_data, n, true);
     const size_t es = dtype_size(t);
     bool radix = n >= sort_radix_min(t);
     if (const char* e = getenv("PARALLAX_SORT")) {
@@ -648,10 +658,10 @@ bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n) {
 }
 
 bool launch_segmented_sort_descs(Workspace& ws, DType t, const SegDesc* d_descs, uint64_t S,
-                                 uint64_t total, uint64_t max_len) {
+                                 uint64_t total, uint64_t max_len, bool by_key) {
     if (S == 0 || total == 0) return true;
     const SegSrc src{nullptr, d_descs, 0, 0, 0, 0, (uint32_t)dtype_size(t)};
-    return seg_sort_dispatch(ws, t, src, total, S, max_len, false);
+    return seg_sort_dispatch(ws, t, src, total, S, max_len, false, by_key);
 }
 
 }  // namespace pxb
@@ -676,7 +686,8 @@ PXB_EXPORT int parallax_segmented_sort(parallax_kernel_t kernel, void* data, siz
     const SegSrc src{static_cast<const uint64_t*>(o), nullptr, reinterpret_cast<uint64_t>(d), 0, 0,
                      0, (uint32_t)dtype_size(t)};
     // CSR: every segment lies within the array, so `count` bounds the longest one
-    const bool ok = seg_sort_dispatch(*ws, t, src, count, num_segments, count, true);
+    const bool ok = seg_sort_dispatch(*ws, t, src, count, num_segments, count, true,
+                                      h->kind == Kind::SORT_KV);
     if (!ok) return last_error() ? last_error() : PARALLAX_ERR_CUDA;
     return ws->async ? PARALLAX_OK : sync_stream(*ws);
 }

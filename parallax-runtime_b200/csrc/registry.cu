@@ -349,9 +349,23 @@ Handle* load_image(const unsigned int* image, size_t words, const std::string& n
     Handle* h = new Handle();
     h->kind = Kind::USER;
     h->name = name;
-    if (!cuda_ok(cudaLibraryLoadData(&h->library, image, nullptr, nullptr, 0, nullptr, nullptr, 0),
-                 "cudaLibraryLoadData") ||
-        !cuda_ok(cudaLibraryGetKernel(&h->kernel, h->library, "parallax_entry"),
+    // kept: a transform image may be linked again later, with the fused reduce tile
+    const unsigned char* bytes = reinterpret_cast<const unsigned char*>(image);
+    h->image.assign(bytes, bytes + words * sizeof(unsigned int));
+    if (cudaLibraryLoadData(&h->library, image, nullptr, nullptr, 0, nullptr, nullptr, 0) !=
+        cudaSuccess) {
+        // relocatable machine code or LTO-IR only: link the image alone, then load that
+        cudaGetLastError();
+        h->library = nullptr;
+        if (!link_images({{h->image.data(), h->image.size()}}, &h->linked, name.c_str()) ||
+            !cuda_ok(cudaLibraryLoadData(&h->library, h->linked.data(), nullptr, nullptr, 0,
+                                         nullptr, nullptr, 0),
+                     "cudaLibraryLoadData")) {
+            delete h;
+            return nullptr;
+        }
+    }
+    if (!cuda_ok(cudaLibraryGetKernel(&h->kernel, h->library, "parallax_entry"),
                  "cudaLibraryGetKernel(parallax_entry)")) {
         delete h;
         return nullptr;

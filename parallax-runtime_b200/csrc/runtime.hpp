@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 #include <utility>
 
 #include "common.cuh"
@@ -47,6 +48,7 @@ uint64_t launch_count();
 // launch's algorithmic bytes (the minimum HBM traffic of the work it does), so achieved
 // bandwidth per kernel comes from live events. Disabled: one predictable branch.
 struct Workspace;
+struct Handle;
 class ProfScope {
   public:
     ProfScope(Workspace& ws, const char* kernel, uint64_t alg_bytes);
@@ -104,6 +106,8 @@ struct Workspace {
     void* d_radix = nullptr;              // radix sort: tile claim counters, digit histograms,
     size_t radix_cap = 0;                 // per-(tile, digit) look-back words
     uint32_t radix_epoch = 1;             // next epoch of those words, see next_radix_epochs()
+    void* d_seg_radix = nullptr;          // segmented radix sort: counters (device-side epoch)
+    size_t seg_radix_cap = 0;             // and per-(work item, digit) look-back words
     // Copy streams of calls whose host operand copies overlap their kernels (uploads and
     // downloads on separate copy engines) and the events that order them; see copy_streams().
     cudaStream_t copy_up = nullptr;
@@ -113,6 +117,15 @@ struct Workspace {
     // buffer addresses are re-captured.
     uint64_t generation = 0;
     std::map<std::string, std::pair<uint64_t, cudaGraphExec_t>> graphs;
+    // A transform2 of a transform_reduce / count_if funnel whose image can be fused with
+    // the reduce that follows it: held back until the next call on this thread, which
+    // either is that reduce (one fused pass) or runs it first (see abi.cu).
+    struct Deferred {
+        Handle* h = nullptr;
+        void* in = nullptr;
+        void* out = nullptr;
+        size_t n = 0, in_es = 0, out_es = 0;
+    } deferred;
 
     cudaStream_t stream() const { return user_stream ? user_stream : own_stream; }
     // Device scratch with a fixed layout (zeroed whenever it is reallocated):
@@ -128,6 +141,10 @@ struct Workspace {
     void* seg_status(uint64_t entries);
     // Radix sort buffer (zeroed on (re)allocation): only radix-sort words ever live there.
     void* radix(size_t bytes);
+    // Segmented radix sort buffer (zeroed on (re)allocation): its look-back words carry a
+    // device-side epoch (replayed graphs advance it), so they never share the radix buffer,
+    // whose words carry host-side epochs.
+    void* seg_radix(size_t bytes);
     // `count` consecutive 22-bit epochs (one per radix pass) for the radix sort's look-back
     // words; returns the first. Called before a sort enqueues anything: on wrap-around it
     // enqueues a clear of the buffer, so no stale word can alias a reused epoch.
@@ -140,6 +157,7 @@ struct Workspace {
     uint32_t next_epoch();
 };
 Workspace* workspace();  // the calling thread's; nullptr when the device is unavailable
+Workspace* current_workspace();  // the calling thread's if it has one, else nullptr
 Workspace* new_workspace();  // an independent one (own stream and buffers), never freed
 
 // Replays the CUDA graph cached under `key` on the workspace stream, capturing it first
@@ -246,9 +264,30 @@ struct Handle {
     cudaLibrary_t library = nullptr;
     cudaKernel_t kernel = nullptr;
     std::string name;
+    std::vector<unsigned char> image;   // the registered image (linked again for fusion)
+    std::vector<char> linked;           // cubin nvJitLink made of it, when loaded that way
+    // Fused transform + reduce (fused.cu): 0 not tried, 1 linked, 2 not possible
+    int fused_state = 0;
+    cudaLibrary_t fused_library = nullptr;
+    cudaKernel_t fused[6] = {};         // per reduced type: f32 f64 i32 i64 u32 u64
 };
 Handle* as_handle(parallax_kernel_t k);
 Handle* builtin_handle(const char* spec);
+
+// ---- run-time linking of registered images (fused.cu) ---------------------------------------
+// Links fatbin / cubin / LTO-IR inputs for sm_100a with nvJitLink (link-time optimisation on)
+// into one cubin; false when the link fails (with an error set unless `quiet`).
+bool link_images(const std::vector<std::pair<const void*, size_t>>& inputs,
+                 std::vector<char>* cubin, const char* what, bool quiet = false);
+// True when `h` (a registered transform image) exports parallax_elem as LTO-IR, i.e. it
+// links with the fused transform + reduce tile; links it on first use.
+bool xform_fusable(Handle* h);
+// One pass: reduce of xf(in[i]) over n input elements of in_es bytes into one element of
+// dtype u at d_out (the runtime's reduce accumulation). xform_fusable(xf) must hold.
+bool launch_xform_reduce(Workspace& ws, Handle* xf, DType u, const void* d_in, size_t n,
+                         size_t in_es, void* d_out);
+// Runs a transform held back on the calling thread (Workspace::deferred), if any.
+void settle_deferred_here();
 
 // ---- launchers (all asynchronous on `s`) -------------------------------------------------
 // Reduce: writes one element (type of dtype; sum of f32 is rounded from fp64) to d_out.
@@ -273,11 +312,12 @@ bool launch_count_flags(Workspace& ws, const uint8_t* d_flags, size_t n, uint64_
 // Elements a flags array written for launch_compact with PredKind::FLAGS must be padded to
 // (the compaction reads whole rows of flags; bytes past n are ignored).
 size_t compact_flags_padding(size_t n);
-bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n);
+// by_key: 8-byte (key << 32 | value) records sorted stably by key (sort_kv handles).
+bool launch_sort(Workspace& ws, DType t, void* d_data, size_t n, bool by_key = false);
 // Smallest array launch_sort gives to the radix sort (by default; PARALLAX_SORT overrides).
 size_t sort_radix_min(DType t);
 // One-sweep LSD radix sort (kernels/radix.cu); launch_sort picks it for large arrays.
-bool launch_radix_sort(Workspace& ws, DType t, void* d_data, size_t n);
+bool launch_radix_sort(Workspace& ws, DType t, void* d_data, size_t n, bool by_key = false);
 bool launch_map(Workspace& ws, MapOp op, const void* d_in, void* d_out, size_t n,
                 const void* captures, size_t capture_size);
 bool launch_find(Workspace& ws, DType t, const Pred& p, const void* d_in, size_t n,
@@ -301,7 +341,7 @@ bool launch_segmented_descs(Workspace& ws, SegKind op, DType t, const Pred& p, b
 // Sorts every descriptor's segment in place (aux = an n-element device temporary);
 // `max_len` bounds the segment lengths. `t` is U64 for sort_kv records.
 bool launch_segmented_sort_descs(Workspace& ws, DType t, const SegDesc* d_descs, uint64_t S,
-                                 uint64_t total, uint64_t max_len);
+                                 uint64_t total, uint64_t max_len, bool by_key = false);
 
 // Device address of an operand of the segmented entry points, which take device memory or
 // PARALLAX_DEVICE_RESIDENT arena blocks only. nullptr (error recorded) otherwise.

@@ -160,4 +160,16 @@ k_seg_plan(SegSrc src, uint64_t S, uint64_t count, uint32_t tile,
     }
 }
 
+struct Workspace;
+
+// Segmented radix sort (kernels/radix.cu): each of the S segments of `src` sorted in place,
+// one histogram launch and one launch per digit pass for all of them; by_key: 8-byte
+// (key << 32 | value) records sorted stably by key (four passes). CSR segments need
+// src.aux unset (the temporary comes from the workspace), descriptors carry their own.
+// `graph`: captured once per argument set as a CUDA graph and replayed.
+bool launch_segmented_radix_sort(Workspace& ws, DType t, const SegSrc& src, uint64_t count,
+                                 uint64_t S, bool by_key, bool graph);
+// Keys per tile (work item) of the segmented radix sort.
+uint64_t segmented_radix_tile(DType t);
+
 }  // namespace pxb

@@ -52,6 +52,7 @@ uint64_t now_ns() {
 struct Request {
     ReqOp op = ReqOp::REDUCE;
     DType t = DType::INVALID;  // U64 for sort_kv records
+    bool by_key = false;       // sort_kv: records sorted stably by their high 32 bits
     RedOp red = RedOp::SUM;
     CompactMode mode = CompactMode::SELECT;
     Pred pred;                 // negate folded in (remove_if)
@@ -106,7 +107,7 @@ int wait_request(Request* r, uint64_t* done_ns) {
 }
 
 bool same_kind(const Request& a, const Request& b) {
-    return a.op == b.op && a.t == b.t && a.red == b.red && a.mode == b.mode &&
+    return a.op == b.op && a.t == b.t && a.by_key == b.by_key && a.red == b.red && a.mode == b.mode &&
            a.exclusive == b.exclusive && a.init_bits == b.init_bits &&
            a.pred.kind == b.pred.kind && a.pred.negate == b.pred.negate &&
            a.pred.i == b.pred.i && a.pred.u == b.pred.u &&
@@ -257,7 +258,8 @@ class Server {
                 case ReqOp::SCAN:
                     return launch_scan(ws, h.t, h.exclusive, h.d_in, h.d_out ? h.d_out : (void*)h.d_in,
                                        h.n, h.exclusive ? &h.init_bits : nullptr);
-                case ReqOp::SORT: return launch_sort(ws, h.t, const_cast<void*>(h.d_in), h.n);
+                case ReqOp::SORT:
+                    return launch_sort(ws, h.t, const_cast<void*>(h.d_in), h.n, h.by_key);
                 case ReqOp::COMPACT:
                     return launch_compact(ws, h.t, h.mode, h.pred, h.d_in, h.d_out, h.n, l.d_res);
             }
@@ -290,7 +292,7 @@ class Server {
                 return launch_segmented_descs(ws, SegKind::COPY_IF, h.t, h.pred, false, 0, l.d_desc,
                                               S, total, RedOp::SUM, h.mode);
             case ReqOp::SORT:
-                return launch_segmented_sort_descs(ws, h.t, l.d_desc, S, total, max_len);
+                return launch_segmented_sort_descs(ws, h.t, l.d_desc, S, total, max_len, h.by_key);
         }
         return false;
     }
@@ -413,6 +415,7 @@ int make_request(const parallax_request* q, Request* r) {
         case Kind::SORT:
         case Kind::SORT_KV:
             r->op = ReqOp::SORT;
+            r->by_key = h->kind == Kind::SORT_KV;
             r->coalescible = true;
             break;
         case Kind::COMPACT_FLAGS:
@@ -474,6 +477,7 @@ PXB_EXPORT int parallax_serve_stop(void) {
 }
 
 PXB_EXPORT int parallax_serve_submit(const parallax_request* req, uint64_t* ticket) {
+    settle_deferred_here();  // a transform held back on this thread may produce the operand
     set_ok();
     if (!ticket) {
         set_error(PARALLAX_ERR_INVALID_ARGUMENT, "parallax_serve_submit: ticket is null");

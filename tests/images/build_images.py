@@ -3,6 +3,9 @@
 Each image is one translation unit exporting parallax_entry (include/parallax/kernel_abi.h),
 compiled the way a compiler targeting this runtime would embed its kernels:
     nvcc -fatbin -gencode arch=compute_100a,code=sm_100a -I include -o _build/<name>.fatbin <name>.cu
+Images whose name ends in _lto also export their element function (parallax_elem) and are
+compiled relocatable with LTO-IR beside the machine code, so the runtime can fuse them:
+    nvcc -fatbin -rdc=true -gencode arch=compute_100a,code=[sm_100a,lto_100a] ...
 Rebuilt when the source, image_common.cuh or kernel_abi.h is newer than the fatbin.
 
     python tests/images/build_images.py
@@ -31,7 +34,9 @@ def build() -> list[Path]:
     for src in sorted(HERE.glob("*.cu")):
         out = fatbin(src.stem)
         if (not out.exists() or out.stat().st_mtime < max(src.stat().st_mtime, newest_dep)):
-            cmd = [nvcc, "-fatbin", "-gencode", "arch=compute_100a,code=sm_100a", "-O3",
+            code = "[sm_100a,lto_100a]" if src.stem.endswith("_lto") else "sm_100a"
+            cmd = [nvcc, "-fatbin", "-gencode", f"arch=compute_100a,code={code}", "-O3",
+                   *(["-rdc=true"] if src.stem.endswith("_lto") else []),
                    "-I", str(ROOT / "include"), "-o", str(out), str(src)]
             r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:

@@ -248,13 +248,23 @@ def test_sort_unaligned_data(lib, px, ox, dev, t, shift, n):
     assert np.array_equal(got, ox.sort(x))
 
 
-def test_sort_kv_is_stable_by_key(lib, px, ox, dev):
-    n = 100000
+@pytest.mark.parametrize("n", [2, 1000, 100000, (1 << 20) + 3])
+def test_sort_kv_is_stable_by_key(lib, px, ox, dev, n):
     keys = (ox.gen("u32_full", 8, n) % 1000).astype(np.uint64)
     rec = (keys << np.uint64(32)) | np.arange(n, dtype=np.uint64)
     got = sort_dev(lib, px, dev, "sort_kv:u32", rec)
     order = np.argsort(keys, kind="stable")
     assert np.array_equal(got & np.uint64(0xFFFFFFFF), order.astype(np.uint64))
+
+
+@pytest.mark.parametrize("n", [3, 4097, 300001])
+def test_sort_kv_keeps_input_order_of_equal_keys_with_random_values(lib, px, ox, dev, n):
+    """Stable by key means equal keys keep their input order, not their value order."""
+    keys = (ox.gen("u32_full", 9, n) % 50).astype(np.uint64)
+    vals = ox.gen("u32_full", 10, n).astype(np.uint64)
+    rec = (keys << np.uint64(32)) | vals
+    got = sort_dev(lib, px, dev, "sort_kv:u32", rec)
+    assert np.array_equal(got, rec[np.argsort(keys, kind="stable")])
 
 
 @pytest.mark.parametrize("t", list(DTYPES))

@@ -250,9 +250,15 @@ def test_segmented_unaligned_arrays(lib, px, ox, dev, shift):
     assert np.array_equal(dev.get(r, np.int32, off.size - 1), ox.seg_sum(x, off))
 
 
+@pytest.mark.parametrize("path", ["auto", "radix", "merge"])
 @pytest.mark.parametrize("t", list(DTYPES))
 @pytest.mark.parametrize("layout", list(LAYOUTS))
-def test_segmented_sort(lib, px, ox, dev, t, layout):
+def test_segmented_sort(lib, px, ox, dev, t, layout, path, monkeypatch):
+    """Both segmented sort paths (one-sweep radix over segment-local tiles, and tile sort +
+    per-segment merge passes; `auto` picks radix when the mean segment spans a radix tile)
+    return the oracle's bytes on every layout."""
+    if path != "auto":
+        monkeypatch.setenv("PARALLAX_SORT", path)
     off = LAYOUTS[layout]
     x = make(ox, t, int(off[-1]))
     d, o = dev.put(x), dev.put(off)
@@ -263,12 +269,18 @@ def test_segmented_sort(lib, px, ox, dev, t, layout):
     assert np.array_equal(got.view(np.uint8), ox.seg_sort(x, off).view(np.uint8))
 
 
-def test_segmented_sort_kv_stable(lib, px, ox, dev):
-    """sort_kv:u32 records (key << 32 | value) sort stably by key inside each segment."""
-    off = LAYOUTS["lognormal"]
+@pytest.mark.parametrize("values", ["index", "random"])
+@pytest.mark.parametrize("layout", ["lognormal", "tile_edges", "big_and_small", "ones"])
+def test_segmented_sort_kv_stable(lib, px, ox, dev, values, layout):
+    """sort_kv:u32 records (key << 32 | value) sort stably by key inside each segment: equal
+    keys keep their input order whatever their values (random values would be reordered by
+    a sort of the whole 64-bit records)."""
+    off = LAYOUTS[layout]
     n = int(off[-1])
     keys = (ox.gen("u32_full", 5, n) % 97).astype(np.uint64)
-    recs = (keys << np.uint64(32)) | np.arange(n, dtype=np.uint64)
+    vals = (np.arange(n, dtype=np.uint64) if values == "index"
+            else ox.gen("u32_full", 6, n).astype(np.uint64))
+    recs = (keys << np.uint64(32)) | vals
     d, o = dev.put(recs), dev.put(off)
     lib.parallax_segmented_sort(px.builtin("sort_kv:u32"), d.data_ptr(), n, o.data_ptr(),
                                 off.size - 1)

@@ -18,6 +18,9 @@ A third build, `stdpar_driver_heap`, also links the whole-heap capture shim
 program lives in the runtime's heap pool, the arena adopts the pool (zero-copy), the funnels
 find their data in the arena and call the runtime on it in place, and a transform chases
 pointers stored in heap records. Its results must match the host run the same way.
+
+The count_if and transform_reduce transforms are registered as images that also export
+their element function (LTO-IR), so each of those funnels must run as one fused launch.
 """
 from __future__ import annotations
 
@@ -185,6 +188,12 @@ def test_element_wise_funnels_with_registered_images(runs, build, n):
         assert np.array_equal(arr(g[name + s], dt).view(np.uint8),
                               arr(h[name + s], dt).view(np.uint8)), name
     assert g["count_if_gt_half_f32" + s][1] == h["count_if_gt_half_f32" + s][1]
+    # sums of x * 0.5 over int32 are exact in fp64: the fused pass gives the host's bits
+    assert g["transform_reduce_half_i32" + s][1] == h["transform_reduce_half_i32" + s][1]
+    # both transforms export their element function: each funnel ran as ONE fused pass
+    # (transform + reduce in one kernel) instead of a transform kernel and a reduce kernel
+    for name in ("count_if_gt_half_f32", "transform_reduce_half_i32"):
+        assert g[name + s][0] == 1, f"{name}: {g[name + s][0]} launches, not one fused pass"
 
 
 @pytest.mark.parametrize("n", SIZES)

@@ -11,6 +11,9 @@ for that output. Each test registers an image under the key GCC gives the stdpar
   copy_if with a registered :flags  device_copy_if / remove_if / partition (stdpar.hpp:300-371;
                                     reference kernel_launcher.cpp:1701-1791)
   :pred transform + ':reduce'       device_count_if     (stdpar.hpp:271-293)
+  :xform transform + ':reduce'      device_transform_reduce (stdpar.hpp:241-267)
+Transforms whose image also exports its element function as LTO-IR (images/*_lto.cu) run
+fused with the reduce that follows them: one launch instead of two.
 Results are compared with host computations (bit-exact) and the oracle.
 """
 from __future__ import annotations
@@ -39,6 +42,7 @@ COPY_IF = "std::size_t parallax::detail::device_copy_if(const T*, T*, std::size_
 REMOVE_IF = "std::size_t parallax::detail::device_remove_if(T*, std::size_t, Pred)"
 PARTITION = "std::size_t parallax::detail::device_partition(T*, std::size_t, Pred)"
 COUNT_IF = "long int parallax::detail::device_count_if(const T*, std::size_t, Pred)"
+TRANSFORM_REDUCE = "U parallax::detail::device_transform_reduce(const T*, std::size_t, F)"
 
 _keep = []  # registered images must outlive the process (the registry borrows them)
 
@@ -279,3 +283,101 @@ def test_registered_flags_refuse_other_element_sizes(lib, px, dev):
     assert lib.parallax_copy_if(*hs, d.data_ptr(), o.data_ptr(), 64, 2, 0) == 0
     assert lib.parallax_last_error() == px.ERR_UNSUPPORTED
     lib.parallax_clear_error()
+
+
+# ---- fused transform + reduce (images that export parallax_elem as LTO-IR) ---------------------
+
+def funnel_call(lib, px, kx, kr, inp, out, n, in_es, out_es, res):
+    """The funnel's two calls (stdpar.hpp:251-259); returns the kernels they launched."""
+    before = lib.parallax_launch_count()
+    lib.parallax_kernel_launch_transform2(kx, P(inp), P(out), n, in_es, out_es)
+    px.check("funnel transform")
+    lib.parallax_reduce(kr, P(out), n, out_es, P(res))
+    px.check("funnel reduce")
+    return lib.parallax_launch_count() - before
+
+
+@pytest.mark.parametrize("n", [1, 255, 2049, 1_000_003])
+def test_transform_reduce_funnel_runs_as_one_fused_pass(lib, px, arena, n):
+    sig_with = "T = int; U = double; F = HalfL"
+    kx = register(lib, key(TRANSFORM_REDUCE, sig_with, "xform"), "xform_half_i32_to_f64_lto")
+    kr = lookup(lib, key(TRANSFORM_REDUCE, sig_with, "reduce"))
+    assert kr
+    x = np.random.default_rng(31).integers(-2**31, 2**31, n, dtype=np.int64).astype(np.int32)
+    inp, out = arena.array(x), arena.empty(n, np.float64)
+    res = np.zeros(1, np.float64)
+    assert funnel_call(lib, px, kx, kr, inp, out, n, 4, 8, res) == 1
+    # multiples of 0.5 below 2^52: the fp64 sum is exact in any order
+    assert res[0] == float(x.astype(np.int64).sum()) * 0.5
+
+
+@pytest.mark.parametrize("n", [1, 4097, 777_777])
+def test_count_if_funnel_runs_as_one_fused_pass(lib, px, arena, n):
+    sig_with = "T = float; Pred = GtHalfL"
+    kp = register(lib, key(COUNT_IF, sig_with, "pred"), "pred_gt_half_f32_lto")
+    kr = lookup(lib, key(COUNT_IF, sig_with, "reduce"))
+    x = rng_f32(n, 12)
+    inp, flags = arena.array(x), arena.empty(n, np.int32)
+    res = np.zeros(1, np.int32)
+    assert funnel_call(lib, px, kp, kr, inp, flags, n, 4, 4, res) == 1
+    assert res[0] == np.count_nonzero(x > np.float32(0.5))
+
+
+def test_fused_integer_sum_equals_two_pass_sum(lib, px, arena, dev):
+    """x * x over int64 (wrapping), summed with wrap-around: the fused pass and the two-pass
+    path (the same image under a transform key that is not fused, then the built-in reduce)
+    give the same bits, and both equal the host's modular sum."""
+    n = 3_000_001
+    x = np.random.default_rng(32).integers(-2**62, 2**62, n, dtype=np.int64)
+    sig_with = "T = long int; U = long int; F = SqL"
+    kx = register(lib, key(TRANSFORM_REDUCE, sig_with, "xform"), "xform_sq_i64_lto")
+    kr = lookup(lib, key(TRANSFORM_REDUCE, sig_with, "reduce"))
+    inp, out = arena.array(x), arena.empty(n, np.int64)
+    fused = np.zeros(1, np.int64)
+    assert funnel_call(lib, px, kx, kr, inp, out, n, 8, 8, fused) == 1
+    kt = register(lib, key(TRANSFORM, "Tin = long int; Tout = long int; F = SqL"), "xform_sq_i64_lto")
+    two = np.zeros(1, np.int64)
+    assert funnel_call(lib, px, kt, px.builtin("reduce:sum:i64"), inp, out, n, 8, 8, two) == 2
+    xu = x.view(np.uint64)
+    with np.errstate(over="ignore"):
+        want = np.array([(xu * xu).sum(dtype=np.uint64)], np.uint64).view(np.int64)[0]
+    assert fused[0] == two[0] == want
+    assert np.array_equal(out.view(np.uint64), xu * xu)  # the two-pass transform's output
+
+
+def test_held_back_transform_runs_before_any_other_call(lib, px, arena):
+    """A funnel transform is held back only until the next call on the thread: a different
+    call (here a max reduce of its output, then a free of its input) sees the transform's
+    output exactly as if it had run at once."""
+    sig_with = "T = int; U = double; F = HalfM"
+    kx = register(lib, key(TRANSFORM_REDUCE, sig_with, "xform"), "xform_half_i32_to_f64_lto")
+    x = np.random.default_rng(33).integers(-10**6, 10**6, 100_003, dtype=np.int64).astype(np.int32)
+    inp, out = arena.array(x), arena.empty(x.size, np.float64)
+    lib.parallax_kernel_launch_transform2(kx, P(inp), P(out), x.size, 4, 8)
+    px.check("held-back transform")
+    res = np.zeros(1, np.float64)
+    lib.parallax_reduce(px.builtin("reduce:max:f64"), P(out), x.size, 8, P(res))
+    px.check("max of the transform's output")
+    assert res[0] == x.max() * 0.5
+    assert np.array_equal(out, x.astype(np.float64) * 0.5)
+    # held back again, then the input block is freed: the transform runs before the free
+    out[:] = 0
+    lib.parallax_kernel_launch_transform2(kx, P(inp), P(out), x.size, 4, 8)
+    lib.parallax_arena_free(C.c_void_p(P(inp)))
+    arena.blocks.remove(P(inp))
+    px.check("free after a held-back transform")
+    assert np.array_equal(out, x.astype(np.float64) * 0.5)
+
+
+def test_transform_without_element_function_runs_two_passes(lib, px, arena):
+    """The same funnel with an image that exports no parallax_elem (plain sm_100a) runs its
+    transform and its reduce as two launches and gives the same sum."""
+    sig_with = "T = int; U = double; F = HalfP"
+    kx = register(lib, key(TRANSFORM_REDUCE, sig_with, "xform"), "half_i32_to_f64")
+    kr = lookup(lib, key(TRANSFORM_REDUCE, sig_with, "reduce"))
+    x = np.random.default_rng(34).integers(-2**31, 2**31, 500_001, dtype=np.int64).astype(np.int32)
+    inp, out = arena.array(x), arena.empty(x.size, np.float64)
+    res = np.zeros(1, np.float64)
+    assert funnel_call(lib, px, kx, kr, inp, out, x.size, 4, 8, res) == 2
+    assert res[0] == float(x.astype(np.int64).sum()) * 0.5
+    assert np.array_equal(out, x.astype(np.float64) * 0.5)
