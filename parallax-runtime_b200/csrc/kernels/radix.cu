@@ -46,7 +46,14 @@ constexpr int kEpochShift = 42;
 constexpr int kLookWindow = 4;  // predecessor words a look-back step loads at once
 
 template <typename K> struct RadixShape;
-template <> struct RadixShape<uint32_t> { static constexpr int BLOCK = 512, ITEMS = 16; };
+// Keys per thread of the 4-byte pass and CTAs per SM; build-time knobs (-D) for sweeps.
+#ifndef PXB_RADIX_ITEMS32
+#define PXB_RADIX_ITEMS32 16
+#endif
+#ifndef PXB_RADIX_CTAS
+#define PXB_RADIX_CTAS 3
+#endif
+template <> struct RadixShape<uint32_t> { static constexpr int BLOCK = 512, ITEMS = PXB_RADIX_ITEMS32; };
 template <> struct RadixShape<uint64_t> { static constexpr int BLOCK = 512, ITEMS = 8; };
 
 // Each warp may rank its keys as kSubs independent streams (consecutive parts of its keys),
@@ -54,7 +61,7 @@ template <> struct RadixShape<uint64_t> { static constexpr int BLOCK = 512, ITEM
 // 2^26-key pass: one stream at three CTAs per SM (0.338 ms, some registers spilled to fit)
 // beats two streams at two CTAs per SM (0.362 ms) and at three (0.378 ms).
 constexpr int kSubs = 1;
-constexpr int kPassCtasPerSm = 3;
+constexpr int kPassCtasPerSm = PXB_RADIX_CTAS;
 
 template <typename K>
 constexpr size_t radix_smem() {
@@ -222,6 +229,10 @@ __global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
         seg = sr.item_seg[tile];
         tk = tile - sr.item_start[seg];
         n = sr.src.len(seg);
+        if (n < 2) {  // sorted already; such a segment may come without a temporary
+            if (tid == 0) persistent_exit(counters);
+            return;
+        }
         const uint64_t a = sr.src.in_addr(seg), b = sr.src.aux_addr(seg);
         in = reinterpret_cast<const K*>(sr.parity ? b : a);
         out = reinterpret_cast<K*>(sr.parity ? a : b);
@@ -423,6 +434,7 @@ __global__ void __launch_bounds__(kSegHistBlock)
     const uint64_t seg = sr.item_seg[item];
     const uint64_t k = item - sr.item_start[seg];
     const uint64_t len = sr.src.len(seg);
+    if (len < 2) return;  // not sorted (see k_radix_pass)
     const K* in = reinterpret_cast<const K*>(sr.src.in_addr(seg)) + k * TILE;
     const uint64_t rem = len - k * TILE;
     const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
