@@ -60,12 +60,15 @@ int parallax_kernel_resolves(const char* key);
 
 /* ---- arena residency ------------------------------------------------------------- */
 enum parallax_residency {
-    /* Default. Every ABI call uploads the arena ranges it reads from the pinned host
-     * mirror and downloads the ranges it writes, so host code sees the reference's
-     * synchronous unified-memory behaviour. */
+    /* Default. The pinned host mirror is authoritative between calls: every ABI call
+     * uploads the arena ranges it reads and downloads the ranges it writes, so host code
+     * sees the reference's synchronous unified-memory behaviour. Operands of at most
+     * 64 KiB are not copied at all: the kernel reads and writes the host mirror itself
+     * (zero-copy). The device copy of a coherent block is therefore not kept current. */
     PARALLAX_COHERENT = 0,
     /* The device copy is authoritative; ABI calls move nothing. Host code moves data
-     * explicitly with parallax_arena_sync_to_device / _to_host. */
+     * explicitly with parallax_arena_sync_to_device / _to_host (also when a block that
+     * was used coherently becomes device-resident). */
     PARALLAX_DEVICE_RESIDENT = 1,
 };
 /* Applies to the whole arena block that contains ptr. Returns a parallax_status. */

@@ -16,8 +16,13 @@
 
 namespace pxb {
 
+// Coherent arena operands up to this size are used in place in the page-locked host mirror
+// (zero-copy: the kernel's loads and stores cross PCIe) instead of being copied to the device
+// and back, which for small operands costs more than the transfer itself.
+constexpr size_t kMappedMax = size_t(64) << 10;
+
 bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int slot,
-                     Operand* out) {
+                     Operand* out, bool mappable) {
     out->user = p;
     out->bytes = bytes;
     if (!p) {
@@ -45,6 +50,13 @@ bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int slot
         }
         out->kind = b.residency == PARALLAX_DEVICE_RESIDENT ? OperandKind::ARENA_RESIDENT
                                                             : OperandKind::ARENA_COHERENT;
+        if (out->kind == OperandKind::ARENA_COHERENT && mappable && !ws.async &&
+            bytes <= kMappedMax && arena_host_mapped(p, bytes)) {
+            // small: the kernel works on the host mirror itself, no copy either way
+            out->kind = OperandKind::ARENA_MAPPED;
+            out->dev = p;
+            return true;
+        }
         if (out->kind == OperandKind::ARENA_COHERENT && upload && bytes)
             return arena_copy_async(out->dev, p, bytes, true, s);
         return true;
@@ -198,7 +210,9 @@ void map_inplace(const char* fn, parallax_kernel_t kernel, void* buffer, size_t 
     if (chase && !arena_sync_coherent(*ws, true)) return;
     Operand op;
     size_t bytes = count * elem_size;
-    if (!resolve_operand(*ws, buffer, bytes, !(chase && arena_contains(buffer)), 0, &op)) return;
+    // (a kernel that chases stored pointers syncs the whole arena: operands stay staged)
+    if (!resolve_operand(*ws, buffer, bytes, !(chase && arena_contains(buffer)), 0, &op, !chase))
+        return;
     bool ok = h->kind == Kind::USER
         ? launch_user(*ws, h, op.dev, op.dev, count, elem_size, elem_size, captures, capture_size)
         : launch_map(*ws, h->map, op.dev, op.dev, count, captures, capture_size);
@@ -242,8 +256,9 @@ void map_transform(const char* fn, parallax_kernel_t kernel, void* in, void* out
     const bool chase = reads_through_pointers(h);
     if (chase && !arena_sync_coherent(*ws, true)) return;
     Operand oi, oo;
-    if (!resolve_operand(*ws, in, count * in_es, !(chase && arena_contains(in)), 0, &oi)) return;
-    if (!resolve_operand(*ws, out, count * out_es, false, 1, &oo)) return;
+    if (!resolve_operand(*ws, in, count * in_es, !(chase && arena_contains(in)), 0, &oi, !chase))
+        return;
+    if (!resolve_operand(*ws, out, count * out_es, false, 1, &oo, !chase)) return;
     bool ok = h->kind == Kind::USER
         ? launch_user(*ws, h, oi.dev, oo.dev, count, in_es, out_es, captures, capture_size)
         : launch_map(*ws, h->map, oi.dev, oo.dev, count, captures, capture_size);
@@ -274,7 +289,7 @@ void fused_transform_reduce(Workspace& ws, const Workspace::Deferred& d, Handle*
     Handle* xf = d.h;
     if (!arena_sync_coherent(ws, true)) return;
     Operand oi;
-    if (!resolve_operand(ws, d.in, d.n * d.in_es, !arena_contains(d.in), 0, &oi)) return;
+    if (!resolve_operand(ws, d.in, d.n * d.in_es, !arena_contains(d.in), 0, &oi, false)) return;
     if (!launch_xform_reduce(ws, xf, red->dtype, oi.dev, d.n, d.in_es, ws.d_slot->result))
         return;
     if (!arena_sync_coherent(ws, false)) return;
@@ -524,8 +539,9 @@ PXB_EXPORT size_t parallax_copy_if(parallax_kernel_t flags_kernel, parallax_kern
     const bool chase = user;  // the image may read through stored arena pointers
     if (chase && !arena_sync_coherent(*ws, true)) return 0;
     Operand oi, oo;
-    if (!resolve_operand(*ws, input, bytes, !(chase && arena_contains(input)), 0, &oi)) return 0;
-    if (!resolve_operand(*ws, output, bytes, false, 1, &oo)) return 0;
+    if (!resolve_operand(*ws, input, bytes, !(chase && arena_contains(input)), 0, &oi, !chase))
+        return 0;
+    if (!resolve_operand(*ws, output, bytes, false, 1, &oo, !chase)) return 0;
     if (user) {
         uint8_t* d_flags = static_cast<uint8_t*>(ws->temp(compact_flags_padding(count)));
         if (!d_flags) return 0;

@@ -88,6 +88,16 @@ struct Arena {
     DriverFns drv;
     std::vector<CUmemGenericAllocationHandle> handles;
     std::vector<uint8_t> pinned;  // per chunk: host mirror page-locked yet
+    bool host_ptr_ok = false;     // kernels may use registered host addresses as they are
+
+    // pin_range, then whether every chunk of the range is page-locked
+    bool pinned_range(size_t off, size_t bytes) {
+        pin_range(off, bytes);
+        std::lock_guard<std::mutex> g(mu);
+        for (size_t c = off / chunk; c * chunk < off + bytes; ++c)
+            if (c >= pinned.size() || !pinned[c]) return false;
+        return true;
+    }
 
     // Page-locks the host mirror of every chunk that [off, off + bytes) touches, on first
     // use: blocks that only ever live on the device never pin host memory.
@@ -138,6 +148,7 @@ struct Arena {
         int host_ptrs = 0;
         cudaDeviceGetAttribute(&host_ptrs, cudaDevAttrCanUseHostPointerForRegisteredMem,
                                device_info().device);
+        host_ptr_ok = host_ptrs != 0;
         void* pb = heap_pool_base();
         if (pb && host_ptrs) {  // whole-heap capture: adopt the pool, zero-copy
             pool = true;
@@ -391,6 +402,12 @@ bool arena_copy_async(void* dst, const void* src, size_t bytes, bool to_device,
 bool arena_zero_copy() {
     Arena& a = arena();
     return a.ok && a.pool;
+}
+bool arena_host_mapped(const void* p, size_t bytes) {
+    Arena& a = arena();
+    if (!a.ok || a.pool || !a.host_ptr_ok || !bytes) return false;
+    const size_t off = static_cast<size_t>(static_cast<const char*>(p) - a.host_base);
+    return a.pinned_range(off, bytes);
 }
 bool arena_make_accessible() {
     Arena& a = arena();

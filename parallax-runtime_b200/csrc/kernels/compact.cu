@@ -463,9 +463,9 @@ bool compact_typed(Workspace& ws, CompactMode mode, const Pred& pr, const void* 
         if (!ok) return false;
     }
     auto ts = tile_status_at<uint64_t>(scratch, ws.next_epoch(), &ws.d_slot->spin_error);
-    // bulk copies only from HBM; page-locked host memory (whole-heap capture) takes plain loads
-    const bool bulk = reinterpret_cast<uintptr_t>(d_in) % 16 == 0 &&
-                      !(arena_zero_copy() && arena_contains(d_in));
+    // bulk copies only from HBM; the page-locked host mirror (small coherent operands,
+    // whole-heap capture) takes plain loads
+    const bool bulk = reinterpret_cast<uintptr_t>(d_in) % 16 == 0 && !arena_contains(d_in);
     const T* in = static_cast<const T*>(d_in);
     T* out = static_cast<T*>(d_out);
     auto* cnt_out = reinterpret_cast<unsigned long long*>(d_count);

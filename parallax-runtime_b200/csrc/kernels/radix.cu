@@ -46,22 +46,31 @@ constexpr int kEpochShift = 42;
 constexpr int kLookWindow = 4;  // predecessor words a look-back step loads at once
 
 template <typename K> struct RadixShape;
-// Keys per thread of the 4-byte pass and CTAs per SM; build-time knobs (-D) for sweeps.
+// Keys per thread and CTAs per SM of each key size; build-time knobs (-D) for sweeps.
+// Measured on 2^26 uint32 keys (digit pass): 16 keys at 3 CTAs/SM 0.327 ms, 16 at 2 0.350,
+// 20 at 2 0.329, 24 at 2 0.315 ms (fewer, larger tiles: fewer look-backs; 64 registers,
+// no spills).
 #ifndef PXB_RADIX_ITEMS32
-#define PXB_RADIX_ITEMS32 16
+#define PXB_RADIX_ITEMS32 24
 #endif
-#ifndef PXB_RADIX_CTAS
-#define PXB_RADIX_CTAS 3
+#ifndef PXB_RADIX_CTAS32
+#define PXB_RADIX_CTAS32 2
 #endif
-template <> struct RadixShape<uint32_t> { static constexpr int BLOCK = 512, ITEMS = PXB_RADIX_ITEMS32; };
-template <> struct RadixShape<uint64_t> { static constexpr int BLOCK = 512, ITEMS = 8; };
+#ifndef PXB_RADIX_CTAS64
+#define PXB_RADIX_CTAS64 3
+#endif
+template <> struct RadixShape<uint32_t> {
+    static constexpr int BLOCK = 512, ITEMS = PXB_RADIX_ITEMS32, CTAS = PXB_RADIX_CTAS32;
+};
+template <> struct RadixShape<uint64_t> {
+    static constexpr int BLOCK = 512, ITEMS = 8, CTAS = PXB_RADIX_CTAS64;
+};
 
 // Each warp may rank its keys as kSubs independent streams (consecutive parts of its keys),
 // each with its own count and mask tables, so the dependency chains overlap. Measured on a
 // 2^26-key pass: one stream at three CTAs per SM (0.338 ms, some registers spilled to fit)
 // beats two streams at two CTAs per SM (0.362 ms) and at three (0.378 ms).
 constexpr int kSubs = 1;
-constexpr int kPassCtasPerSm = PXB_RADIX_CTAS;
 
 template <typename K>
 constexpr size_t radix_smem() {
@@ -181,7 +190,7 @@ struct SegRadix {
 // XF_IN transforms keys as they are read (the first pass reads the caller's values),
 // XF_OUT restores them as they are written (the last pass writes the caller's values).
 template <typename K, int XF_IN, int XF_OUT, bool SEG = false>
-__global__ void __launch_bounds__(RadixShape<K>::BLOCK, kPassCtasPerSm)
+__global__ void __launch_bounds__(RadixShape<K>::BLOCK, RadixShape<K>::CTAS)
     k_radix_pass(const K* __restrict__ in_, K* __restrict__ out_, uint64_t n_, int shift,
                  const unsigned long long* __restrict__ hist, uint64_t* status, uint32_t epoch_,
                  uint64_t tiles, uint32_t* counters, volatile int32_t* err, SegRadix sr) {

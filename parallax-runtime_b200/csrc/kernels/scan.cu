@@ -346,11 +346,11 @@ bool scan_typed(Workspace& ws, bool exclusive, const void* d_in, void* d_out, ui
         memcpy(&v, init_host, sizeof(T));
         init = (A)v;
     }
-    // bulk copies only between HBM and shared memory; operands in page-locked host memory
-    // (whole-heap capture) take the plain-load path
+    // bulk copies only between HBM and shared memory; operands in the page-locked host
+    // mirror (small coherent operands, whole-heap capture) take the plain-load path
     const bool bulk = (reinterpret_cast<uintptr_t>(d_in) % 16 == 0) &&
                       (reinterpret_cast<uintptr_t>(d_out) % 16 == 0) &&
-                      !(arena_zero_copy() && (arena_contains(d_in) || arena_contains(d_out)));
+                      !arena_contains(d_in) && !arena_contains(d_out);
     const T* in = static_cast<const T*>(d_in);
     T* out = static_cast<T*>(d_out);
     cudaStream_t s = ws.stream();

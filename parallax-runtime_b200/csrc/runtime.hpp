@@ -197,6 +197,9 @@ bool arena_sync_coherent(Workspace& ws, bool to_device);
 // Pool-backed (whole-heap capture) mode: arena memory is page-locked host memory that
 // kernels use in place (device address == host address); nothing is ever copied.
 bool arena_zero_copy();
+// Page-locks the host mirror under [p, p + bytes) if needed; true when a kernel can then
+// access it through the host address itself (registered memory, host pointers usable).
+bool arena_host_mapped(const void* p, size_t bytes);
 // In that mode, page-locks the pool up to its high-water mark before a kernel may touch
 // it; true (and nothing to do) otherwise.
 bool arena_make_accessible();
@@ -212,7 +215,9 @@ bool arena_copy_async(void* dst, const void* src, size_t bytes, bool to_device,
 //   HOST            any other host pointer; staged through device memory, results are
 //                   copied back (the reference never copies results back to such
 //                   pointers: src/memory/unified_buffer.cpp:126-136)
-enum class OperandKind { ARENA_COHERENT, ARENA_RESIDENT, DEVICE, HOST };
+// ARENA_MAPPED: a small coherent arena operand that the kernel reads and writes in the
+// page-locked host mirror itself (zero-copy), instead of a staged device copy.
+enum class OperandKind { ARENA_COHERENT, ARENA_RESIDENT, ARENA_MAPPED, DEVICE, HOST };
 struct Operand {
     void* user = nullptr;
     void* dev = nullptr;
@@ -222,7 +227,8 @@ struct Operand {
 // Resolves `p` and, when `upload`, enqueues the host-to-device copy. `stage_slot`
 // selects the workspace staging buffer used for HOST operands.
 bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int stage_slot,
-                     Operand* out);
+                     Operand* out,
+                     bool mappable = true);
 // Enqueues the device-to-host copy of the first `bytes` of a written operand.
 bool writeback_operand(Workspace& ws, const Operand& op, size_t bytes);
 
