@@ -554,7 +554,7 @@ def main() -> None:
     ap.add_argument("--no-workloads", action="store_true",
                     help="skip the segmented, map and serving workloads")
     ap.add_argument("--workloads", default=None,
-                    help="comma-separated subset of segmented,map,funnels,sort_paths,serving to run "
+                    help="comma-separated subset of segmented,map,funnels,sort_paths,small_calls,serving to run "
                          "(default: all of them with the whole step, none with --ops)")
     ap.add_argument("--seg-ops", default="",
                     help="comma-separated segmented operations to run (default: all), e.g. "
@@ -705,7 +705,7 @@ def main() -> None:
     if args.workloads is not None:
         wanted = {w for w in args.workloads.split(",") if w}
     elif selected is None and not args.no_workloads:
-        wanted = {"segmented", "map", "funnels", "sort_paths", "serving"}
+        wanted = {"segmented", "map", "funnels", "sort_paths", "small_calls", "serving"}
     else:
         wanted = set()
     lib.parallax_set_async(1)
@@ -721,6 +721,8 @@ def main() -> None:
                                                  peak)
     lib.parallax_set_async(0)
     lib.parallax_set_stream(None)
+    if "small_calls" in wanted:
+        workloads["small_calls"] = run_small_calls(px, lib)
     if "serving" in wanted and rank == 0:
         workloads["serving"] = run_serving(px, lib, args.serve_seconds)
 
@@ -947,6 +949,42 @@ def run_funnels(px, lib, torch, stream, steps: int, warmup: int, peak: float) ->
         for p in blocks:
             lib.parallax_arena_free(C.c_void_p(p))
         lib.parallax_set_async(1)
+
+
+def run_small_calls(px, lib, calls: int = 2000) -> dict:
+    """Host wall-clock time per synchronous ABI call on small operands (fp32 reduce and
+    exclusive scan of 2^10, 2^16 and 2^20 elements), on coherent arena blocks (operands of at
+    most 64 KiB run zero-copy on the host mirror, larger ones are copied both ways) and on
+    device-resident blocks. The latency of one call, not a throughput."""
+    out = {}
+    lib.parallax_set_async(0)
+    hr, hs = px.builtin("reduce:sum:f32"), px.builtin("scan:f32")
+    res = np.zeros(1, np.float32)
+    zero = np.zeros(1, np.float32)
+    for n in (1 << 10, 1 << 16, 1 << 20):
+        for mode in ("coherent", "device_resident"):
+            p = lib.parallax_arena_alloc(n * 4, 256)
+            q = lib.parallax_arena_alloc(n * 4, 256)
+            np.ctypeslib.as_array((C.c_float * n).from_address(p))[:] = 1.0
+            if mode == "device_resident":
+                for b in (p, q):
+                    lib.parallax_arena_set_residency(C.c_void_p(b), px.DEVICE_RESIDENT)
+                lib.parallax_arena_sync_to_device(C.c_void_p(p), n * 4)
+            calls_of = {
+                "reduce": lambda: lib.parallax_reduce(hr, C.c_void_p(p), n, 4, res.ctypes.data),
+                "exclusive_scan": lambda: lib.parallax_exclusive_scan(
+                    hs, hs, hs, C.c_void_p(p), C.c_void_p(q), n, 4, zero.ctypes.data)}
+            for name, fn in calls_of.items():
+                for _ in range(50):
+                    fn()
+                px.check(f"small {name}")
+                t0 = time.perf_counter()
+                for _ in range(calls):
+                    fn()
+                out[f"{name}_{mode}_{n}_us"] = round((time.perf_counter() - t0) / calls * 1e6, 2)
+            lib.parallax_arena_free(C.c_void_p(p))
+            lib.parallax_arena_free(C.c_void_p(q))
+    return out
 
 
 def run_map(px, lib, torch, stream, steps: int, warmup: int, peak: float) -> dict:

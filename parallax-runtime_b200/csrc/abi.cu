@@ -19,7 +19,7 @@ namespace pxb {
 // Coherent arena operands up to this size are used in place in the page-locked host mirror
 // (zero-copy: the kernel's loads and stores cross PCIe) instead of being copied to the device
 // and back, which for small operands costs more than the transfer itself.
-constexpr size_t kMappedMax = size_t(64) << 10;
+constexpr size_t kMappedMax = size_t(256) << 10;
 
 bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int slot,
                      Operand* out, bool mappable) {
