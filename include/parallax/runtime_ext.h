@@ -154,7 +154,7 @@ int parallax_segmented_sort(parallax_kernel_t kernel, void* data, size_t count,
  * That caps count at 24576 tiles: 704,643,072 elements of a 4-byte type, 352,321,536 of
  * an 8-byte type; larger counts return PARALLAX_ERR_INVALID_ARGUMENT and touch nothing.
  * The first call on a device looks up that array's device address (once per device, with
- * the device current); make that first call before any stream capture. All calls share
+ * the device current). All calls share
  * the array: calls that overlap on the GPU (other streams, other threads) race and must
  * be serialized by the caller. */
 int parallax_scan_noalloc(parallax_kernel_t scan_kernel, const void* input, void* output,
