@@ -62,9 +62,10 @@ int parallax_kernel_resolves(const char* key);
 enum parallax_residency {
     /* Default. The pinned host mirror is authoritative between calls: every ABI call
      * uploads the arena ranges it reads and downloads the ranges it writes, so host code
-     * sees the reference's synchronous unified-memory behaviour. Operands of at most
-     * 256 KiB are not copied at all: the kernel reads and writes the host mirror itself
-     * (zero-copy). The device copy of a coherent block is therefore not kept current. */
+     * sees the reference's synchronous unified-memory behaviour. Small operands (at most
+     * 64 KiB written, 256 KiB only read) are not copied at all: the kernel reads and writes
+     * the host mirror itself (zero-copy). The device copy of a coherent block is therefore
+     * not kept current. */
     PARALLAX_COHERENT = 0,
     /* The device copy is authoritative; ABI calls move nothing. Host code moves data
      * explicitly with parallax_arena_sync_to_device / _to_host (also when a block that

@@ -16,13 +16,16 @@
 
 namespace pxb {
 
-// Coherent arena operands up to this size are used in place in the page-locked host mirror
-// (zero-copy: the kernel's loads and stores cross PCIe) instead of being copied to the device
-// and back, which for small operands costs more than the transfer itself.
-constexpr size_t kMappedMax = size_t(256) << 10;
+// Coherent arena operands up to these sizes are used in place in the page-locked host
+// mirror (zero-copy: the kernel's loads and stores cross PCIe) instead of being copied to the
+// device and back, which for small operands costs more than the transfer itself. Measured per
+// synchronous call: a 256 KiB fp32 reduce 23.8 us zero-copy against 28.7 us staged, a 256 KiB
+// exclusive scan (read and written) 43.6 against 41.0 us, at 4 KiB 19.1 against 30.2 us.
+constexpr size_t kMappedMax = size_t(64) << 10;       // operands a call writes
+constexpr size_t kMappedMaxRead = size_t(256) << 10;  // operands a call only reads
 
 bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int slot,
-                     Operand* out, bool mappable) {
+                     Operand* out, bool mappable, size_t mapped_max) {
     out->user = p;
     out->bytes = bytes;
     if (!p) {
@@ -51,7 +54,7 @@ bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int slot
         out->kind = b.residency == PARALLAX_DEVICE_RESIDENT ? OperandKind::ARENA_RESIDENT
                                                             : OperandKind::ARENA_COHERENT;
         if (out->kind == OperandKind::ARENA_COHERENT && mappable && !ws.async &&
-            bytes <= kMappedMax && arena_host_mapped(p, bytes)) {
+            bytes <= (mapped_max ? mapped_max : kMappedMax) && arena_host_mapped(p, bytes)) {
             // small: the kernel works on the host mirror itself, no copy either way
             out->kind = OperandKind::ARENA_MAPPED;
             out->dev = p;
@@ -379,7 +382,7 @@ PXB_EXPORT void parallax_reduce(parallax_kernel_t kernel, void* data, size_t cou
         return;
     }
     Operand op;
-    if (!resolve_operand(*ws, data, count * es, true, 0, &op)) return;
+    if (!resolve_operand(*ws, data, count * es, true, 0, &op, true, kMappedMaxRead)) return;
     void* d_out = result;
     if (ws->async) {
         cudaPointerAttributes attr;
@@ -575,7 +578,9 @@ PXB_EXPORT size_t parallax_argminmax(parallax_kernel_t kernel, void* data, size_
     if (!ws) return count;
     if (count <= 1) return 0;  // reference kernel_launcher.cpp:994-995
     Operand op;
-    if (!resolve_operand(*ws, data, count * dtype_size(h->dtype), true, 0, &op)) return count;
+    if (!resolve_operand(*ws, data, count * dtype_size(h->dtype), true, 0, &op, true,
+                         kMappedMaxRead))
+        return count;
     uint64_t* d_idx = reinterpret_cast<uint64_t*>(ws->d_slot->result);
     if (!launch_argminmax(*ws, h->dtype, want_max != 0, want_last != 0, op.dev, count, d_idx))
         return count;
@@ -605,7 +610,9 @@ PXB_EXPORT size_t parallax_find(parallax_kernel_t kernel, void* data, size_t cou
         p.kind = PredKind::EQ;
     }
     Operand op;
-    if (!resolve_operand(*ws, data, count * dtype_size(h->dtype), true, 0, &op)) return count;
+    if (!resolve_operand(*ws, data, count * dtype_size(h->dtype), true, 0, &op, true,
+                         kMappedMaxRead))
+        return count;
     uint64_t* d_idx = reinterpret_cast<uint64_t*>(ws->d_slot->result);
     if (!launch_find(*ws, h->dtype, p, op.dev, count, d_idx)) return count;
     if (ws->async) return std::numeric_limits<size_t>::max();
@@ -621,8 +628,8 @@ PXB_EXPORT size_t parallax_mismatch(parallax_kernel_t kernel, void* a, void* b, 
     if (count == 0) return 0;
     size_t bytes = count * dtype_size(h->dtype);
     Operand oa, ob;
-    if (!resolve_operand(*ws, a, bytes, true, 0, &oa)) return count;
-    if (!resolve_operand(*ws, b, bytes, true, 1, &ob)) return count;
+    if (!resolve_operand(*ws, a, bytes, true, 0, &oa, true, kMappedMaxRead)) return count;
+    if (!resolve_operand(*ws, b, bytes, true, 1, &ob, true, kMappedMaxRead)) return count;
     uint64_t* d_idx = reinterpret_cast<uint64_t*>(ws->d_slot->result);
     if (!launch_mismatch(*ws, h->dtype, oa.dev, ob.dev, count, d_idx)) return count;
     if (ws->async) return std::numeric_limits<size_t>::max();

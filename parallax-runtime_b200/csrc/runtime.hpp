@@ -228,7 +228,7 @@ struct Operand {
 // selects the workspace staging buffer used for HOST operands.
 bool resolve_operand(Workspace& ws, void* p, size_t bytes, bool upload, int stage_slot,
                      Operand* out,
-                     bool mappable = true);
+                     bool mappable = true, size_t mapped_max = 0);
 // Enqueues the device-to-host copy of the first `bytes` of a written operand.
 bool writeback_operand(Workspace& ws, const Operand& op, size_t bytes);
 
