@@ -1147,14 +1147,23 @@ def run_serving(px, lib, seconds: float) -> dict:
         # whose cost is launch and synchronisation rather than HBM traffic
         out["small_requests"] = {"per_call_saturation": one(0, 0.0, 16)}
         assert lib.parallax_serve_start(None) == px.OK
+        s0 = px.ServeStats()
+        lib.parallax_serve_get_stats(C.byref(s0))
         out["small_requests"]["served_saturation"] = one(1, 0.0, 16, inflight=32)
+        s1 = px.ServeStats()
+        lib.parallax_serve_get_stats(C.byref(s1))
+        out["small_requests"]["serve_stats"] = {
+            f: getattr(s1, f) - getattr(s0, f) for f in
+            ("requests", "batches", "coalesced_requests", "launch_ns", "complete_ns")}
+        out["small_requests"]["serve_stats"]["max_batch"] = s1.max_batch
         lib.parallax_serve_stop()
         out["small_requests"]["throughput_ratio"] = round(
             out["small_requests"]["served_saturation"]["req_s"] /
             out["small_requests"]["per_call_saturation"]["req_s"], 3)
         out["serve_stats"] = {"requests": st.requests, "batches": st.batches,
                               "coalesced_requests": st.coalesced_requests,
-                              "max_batch": st.max_batch, "memory_waits": st.memory_waits}
+                              "max_batch": st.max_batch, "memory_waits": st.memory_waits,
+                              "launch_ns": st.launch_ns, "complete_ns": st.complete_ns}
         out["throughput_ratio_saturation"] = round(
             out["served_saturation"]["req_s"] / out["per_call_saturation"]["req_s"], 3)
         out["throughput_ratio_saturation_depth1"] = round(

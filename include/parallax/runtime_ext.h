@@ -200,6 +200,9 @@ typedef struct parallax_request {
 typedef struct parallax_serve_stats {
     uint64_t requests, batches, coalesced_requests, solo_batches, max_batch;
     uint64_t peak_inflight_bytes, memory_waits, inflight_bytes, queued;
+    /* scheduler threads' time (ns, summed over threads): forming batches and launching them,
+     * handing finished batches back to their requests */
+    uint64_t launch_ns, complete_ns;
 } parallax_serve_stats;
 
 /* Starts the serving loop (cfg may be NULL: defaults); a no-op when it runs already. */

@@ -62,7 +62,8 @@ class ServeStats(C.Structure):
     """parallax_serve_stats"""
     _fields_ = [(n, C.c_uint64) for n in (
         "requests", "batches", "coalesced_requests", "solo_batches", "max_batch",
-        "peak_inflight_bytes", "memory_waits", "inflight_bytes", "queued")]
+        "peak_inflight_bytes", "memory_waits", "inflight_bytes", "queued", "launch_ns",
+        "complete_ns")]
 
 # name -> (restype, argtypes); variadic launches are declared with their fixed part only.
 _SIGNATURES = {

@@ -6,14 +6,15 @@
 //
 // Clients submit requests (reduce / scan / sort / copy_if over operands already resident on
 // the device: PARALLAX_DEVICE_RESIDENT arena blocks or device memory) from any number of
-// threads. `schedulers` host threads share one arrival queue; each owns an equal share of
+// threads. `schedulers` host threads share the queued requests; each owns an equal share of
 // `lanes` independent device lanes (a workspace each: stream, scratch, descriptor table,
 // pinned result slots) and keeps them busy:
 //   * completion: a lane whose batch finished (event query) hands every request its result
-//     and releases the request's admitted bytes and arena temporaries;
+//     and releases the request's admitted bytes;
 //   * admission: requests are taken in arrival order while the in-flight byte budget
-//     allows and their temporaries (sort) can be carved out of the arena; the head request
-//     that does not fit waits for completions (no overtaking, so no starvation);
+//     allows (operands plus sort temporaries, which come from the lane's own buffer); the
+//     head request that does not fit waits for completions (no overtaking, so no
+//     starvation);
 //   * coalescing: the head request and every queued request of the same kind (operation,
 //     element type, predicate, scan flavour) up to `solo_elements` long become ONE
 //     segmented launch over per-request descriptors (segmented.cu, sort.cu): a planner plus
@@ -32,6 +33,7 @@
 #include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <chrono>
 #include <thread>
 #include <vector>
 
@@ -64,54 +66,63 @@ struct Request {
     size_t es = 0;
     void* result = nullptr;    // caller's host memory: reduce value / kept count
     uint64_t footprint = 0;    // admitted bytes (operands + temporaries)
-    void* tmp = nullptr;       // sort temporary: arena block (host-side address)
     bool coalescible = false;
-    // completion: the finisher sets done under m and notifies while holding it, then sets
-    // `released` as its very last access to the request; the waiter (which deletes the
-    // request afterwards) returns only once `released` is set
+    uint64_t seq = 0;          // arrival order
+    // completion: the finisher writes status and done_ns, then sets `released` as its very
+    // last access to the request; the waiter (which deletes the request afterwards) reads
+    // them only once it sees `released`
     int status = PARALLAX_OK;
     uint64_t done_ns = 0;
-    bool done = false;
     std::atomic<bool> released{false};
-    std::mutex m;
-    std::condition_variable cv;
 };
 
+// No lock and no wake-up: a condition variable would make the scheduler thread issue a
+// futex wake for every finished request whose waiter sleeps (measured: 4.3 us of scheduler
+// time per small request, the serving loop's bound), so waiters poll the flag instead.
 void finish(Request* r, int status) {
     r->status = status;
     r->done_ns = now_ns();
-    {
-        std::lock_guard<std::mutex> g(r->m);
-        r->done = true;
-        r->cv.notify_one();
-    }
     r->released.store(true, std::memory_order_release);
 }
 
 // Blocks until the request has been finished; returns its status. Short requests finish
 // within microseconds of their launch, so the waiter first polls the completion flag for up
-// to 20 us (no sleep / wake-up latency), then sleeps on the condition variable.
+// to 20 us, then sleeps between polls (about 20 us asked; the kernel's timer slack makes it
+// longer), which costs a long request no more than that in latency.
 int wait_request(Request* r, uint64_t* done_ns) {
     const uint64_t poll_until = now_ns() + 20000;
     for (int i = 1; !r->released.load(std::memory_order_acquire); ++i) {
         __builtin_ia32_pause();
         if ((i & 63) == 0 && now_ns() > poll_until) break;
     }
-    if (!r->released.load(std::memory_order_acquire)) {
-        std::unique_lock<std::mutex> lk(r->m);
-        r->cv.wait(lk, [&] { return r->done; });
-    }
-    while (!r->released.load(std::memory_order_acquire)) std::this_thread::yield();
+    while (!r->released.load(std::memory_order_acquire))
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
     if (done_ns) *done_ns = r->done_ns;
     return r->status;
 }
 
-bool same_kind(const Request& a, const Request& b) {
-    return a.op == b.op && a.t == b.t && a.by_key == b.by_key && a.red == b.red && a.mode == b.mode &&
-           a.exclusive == b.exclusive && a.init_bits == b.init_bits &&
-           a.pred.kind == b.pred.kind && a.pred.negate == b.pred.negate &&
-           a.pred.i == b.pred.i && a.pred.u == b.pred.u &&
-           (a.pred.f == b.pred.f || (a.pred.f != a.pred.f && b.pred.f != b.pred.f));
+// The kind of a coalescible request, as a map key: requests of equal keys run as one launch
+// (operation, element type, sort_kv flavour, reduce operator, compaction mode, scan flavour
+// and init, and the whole predicate: kind, negation, threshold, modulus and remainder).
+struct KindKey {
+    uint64_t v[8];
+    bool operator<(const KindKey& o) const { return memcmp(v, o.v, sizeof v) < 0; }
+};
+KindKey kind_key(const Request& r) {
+    KindKey k;
+    memset(&k, 0, sizeof k);
+    k.v[0] = (uint64_t)r.op | (uint64_t)(int)r.t << 8 | (uint64_t)r.by_key << 16 |
+             (uint64_t)(int)r.red << 24 | (uint64_t)(int)r.mode << 32 | (uint64_t)r.exclusive << 40;
+    k.v[1] = r.init_bits;
+    k.v[2] = (uint64_t)(int)r.pred.kind | (uint64_t)r.pred.negate << 8;
+    k.v[3] = (uint64_t)r.pred.i;
+    k.v[4] = r.pred.u;
+    double f = r.pred.f;
+    if (f != f) f = __builtin_nan("");  // every NaN threshold is one kind
+    memcpy(&k.v[5], &f, 8);
+    k.v[6] = (uint64_t)r.pred.mod_m;
+    k.v[7] = (uint64_t)r.pred.mod_r;
+    return k;
 }
 
 struct Lane {
@@ -123,6 +134,10 @@ struct Lane {
     uint64_t* d_res = nullptr;   // device alias of h_res
     std::vector<Request*> reqs;
     bool busy = false;
+    // temporaries of a coalesced sort batch (one per request, 256-byte aligned), grown when a
+    // batch needs more; only this lane's scheduler thread touches it, between its batches
+    void* d_tmp = nullptr;
+    size_t tmp_cap = 0;
 };
 
 class Server {
@@ -132,10 +147,17 @@ class Server {
     std::vector<std::thread> thr;
     std::mutex mu;
     std::condition_variable cv_sched;
-    std::deque<Request*> queue;
+    // Queued requests: one FIFO per kind of coalescible request and one for requests that
+    // run alone. Each request carries its arrival number, so the oldest queued request is the
+    // oldest of the FIFO fronts, and a batch takes the head's kind from its FIFO directly
+    // (no scan of the whole queue under the lock).
+    std::map<KindKey, std::deque<Request*>> kinds;
+    std::deque<Request*> solo;
+    uint64_t queued = 0, arrivals = 0;
     bool stopping = false;
-    uint64_t inflight = 0;
+    std::atomic<uint64_t> inflight{0};  // admitted bytes (released without the lock)
     parallax_serve_stats stats{};
+    std::atomic<uint64_t> launch_ns{0}, complete_ns{0};  // scheduler time, all threads
 
     bool init(const parallax_serve_config* c) {
         if (c) cfg = *c;
@@ -172,12 +194,29 @@ class Server {
         r->coalescible = r->coalescible && r->n <= cfg.solo_elements;
         // a sort long enough for the radix path runs alone: the segmented sort merges
         if (r->op == ReqOp::SORT && r->n >= sort_radix_min(r->t)) r->coalescible = false;
+        const KindKey key = r->coalescible ? kind_key(*r) : KindKey{};
         {
             std::lock_guard<std::mutex> g(mu);
-            queue.push_back(r);
+            r->seq = arrivals++;
+            (r->coalescible ? kinds[key] : solo).push_back(r);
+            ++queued;
             ++stats.requests;
         }
         cv_sched.notify_one();
+    }
+
+    // Lane buffers go with the server (stop() has joined the threads; the lanes' workspaces
+    // stay in the runtime's list, like every workspace).
+    ~Server() {
+        for (Lane& l : lanes) {
+            if (l.ws) cudaStreamSynchronize(l.ws->stream());
+            if (l.d_tmp) cudaFree(l.d_tmp);
+            if (l.d_desc) cudaFree(l.d_desc);
+            if (l.h_desc) cudaFreeHost(l.h_desc);
+            if (l.h_res) cudaFreeHost(l.h_res);
+            if (l.done) cudaEventDestroy(l.done);
+        }
+        cudaGetLastError();
     }
 
     void stop() {
@@ -192,56 +231,38 @@ class Server {
 
   private:
     // ---- admission (mutex held) ----------------------------------------------------------------
-    enum class Admit { YES, WAIT, REJECT };
-    Admit admit(Request* r) {
-        const bool idle = inflight == 0;
-        if (!idle && inflight + r->footprint > cfg.inflight_bytes) return Admit::WAIT;
-        if (r->op == ReqOp::SORT && r->coalescible && r->n > 1) {
-            void* p = parallax_arena_alloc(r->n * r->es, 256);
-            if (!p) return idle ? Admit::REJECT : Admit::WAIT;  // REJECT: cannot fit even alone
-            parallax_arena_set_residency(p, PARALLAX_DEVICE_RESIDENT);
-            r->tmp = p;
-        }
-        inflight += r->footprint;
-        if (inflight > stats.peak_inflight_bytes) stats.peak_inflight_bytes = inflight;
-        return Admit::YES;
+    // Admits r when the in-flight byte budget allows it (an idle server admits anything).
+    bool admit(Request* r) {
+        const uint64_t now = inflight.load();
+        if (now != 0 && now + r->footprint > cfg.inflight_bytes) return false;
+        const uint64_t after = inflight.fetch_add(r->footprint) + r->footprint;
+        if (after > stats.peak_inflight_bytes) stats.peak_inflight_bytes = after;
+        return true;
     }
 
-    // Takes the next batch off the queue (mutex held); empty when the head must wait.
-    // Requests rejected at admission are taken off the queue and finished last (their
-    // waiters may free them at once).
+    // Takes the next batch off the queues (mutex held); empty when the head must wait.
     std::vector<Request*> form_batch() {
-        std::vector<Request*> b, rejected;
-        while (!queue.empty()) {
-            Request* head = queue.front();
-            const Admit a = admit(head);
-            if (a == Admit::WAIT) {
-                ++stats.memory_waits;
-                break;
-            }
-            queue.pop_front();
-            if (a == Admit::REJECT) {
-                rejected.push_back(head);
-                continue;
-            }
-            b.push_back(head);
-            break;
+        std::vector<Request*> b;
+        if (!queued) return b;
+        std::deque<Request*>* dq = solo.empty() ? nullptr : &solo;  // the oldest request's FIFO
+        for (auto& kv : kinds)
+            if (!kv.second.empty() && (!dq || kv.second.front()->seq < dq->front()->seq))
+                dq = &kv.second;
+        Request* head = dq->front();
+        if (!admit(head)) {
+            ++stats.memory_waits;
+            return b;
         }
-        if (!b.empty() && b[0]->coalescible) {
-            for (auto it = queue.begin(); it != queue.end() && b.size() < cfg.max_batch;) {
-                Request* r = *it;
-                if (!r->coalescible || !same_kind(*r, *b[0])) {
-                    ++it;
-                    continue;
-                }
-                const Admit a = admit(r);
-                if (a == Admit::WAIT) break;  // keep arrival order for what does not fit
-                it = queue.erase(it);
-                if (a == Admit::REJECT) rejected.push_back(r);
-                else b.push_back(r);
+        dq->pop_front();
+        --queued;
+        b.push_back(head);
+        if (head->coalescible) {  // its kind's later arrivals, in order
+            while (!dq->empty() && b.size() < cfg.max_batch && admit(dq->front())) {
+                b.push_back(dq->front());
+                dq->pop_front();
+                --queued;
             }
         }
-        for (Request* r : rejected) finish(r, PARALLAX_ERR_OUT_OF_MEMORY);
         return b;
     }
 
@@ -265,6 +286,24 @@ class Server {
             }
             return false;
         }
+        char* tmp = nullptr;  // a sort batch's temporaries, from the lane's own buffer
+        if (h.op == ReqOp::SORT) {
+            size_t need = 0;
+            for (size_t i = 0; i < S; ++i) need += (l.reqs[i]->n * l.reqs[i]->es + 255) / 256 * 256;
+            if (need > l.tmp_cap) {  // the lane is idle between its batches: safe to replace
+                if (l.d_tmp) cudaFree(l.d_tmp);
+                l.d_tmp = nullptr;
+                l.tmp_cap = 0;
+                const size_t cap = need + need / 2;
+                if (cudaMalloc(&l.d_tmp, cap) != cudaSuccess) {
+                    cudaGetLastError();
+                    set_error(PARALLAX_ERR_OUT_OF_MEMORY, "serve: sort temporaries of %zu bytes", need);
+                    return false;
+                }
+                l.tmp_cap = cap;
+            }
+            tmp = static_cast<char*>(l.d_tmp);
+        }
         uint64_t total = 0, max_len = 0;
         for (size_t i = 0; i < S; ++i) {
             const Request& r = *l.reqs[i];
@@ -273,8 +312,12 @@ class Server {
             d.in = reinterpret_cast<uint64_t>(r.d_in);
             d.out = reinterpret_cast<uint64_t>(r.d_out ? r.d_out : (void*)r.d_in);
             d.n = r.n;
-            d.aux = r.op == ReqOp::SORT ? reinterpret_cast<uint64_t>(r.tmp ? arena_dev(r.tmp) : nullptr)
-                                        : reinterpret_cast<uint64_t>(l.d_res + i);
+            if (r.op == ReqOp::SORT) {
+                d.aux = reinterpret_cast<uint64_t>(tmp);
+                tmp += (r.n * r.es + 255) / 256 * 256;
+            } else {
+                d.aux = reinterpret_cast<uint64_t>(l.d_res + i);
+            }
             total += r.n;
             if (r.n > max_len) max_len = r.n;
         }
@@ -311,15 +354,10 @@ class Server {
                 if (r->op == ReqOp::REDUCE) memcpy(r->result, &v, r->es);
                 else if (r->op == ReqOp::COMPACT) memcpy(r->result, &v, 8);
             }
-            if (r->tmp) {
-                parallax_arena_free(r->tmp);
-                r->tmp = nullptr;
-            }
         }
-        {
-            std::lock_guard<std::mutex> g(mu);
-            for (Request* r : l.reqs) inflight -= r->footprint;
-        }
+        uint64_t released = 0;
+        for (Request* r : l.reqs) released += r->footprint;
+        inflight.fetch_sub(released);
         for (Request* r : l.reqs) finish(r, status);  // r may be deleted right after
         l.reqs.clear();
         l.busy = false;
@@ -338,14 +376,17 @@ class Server {
                     any_busy = true;
                     continue;
                 }
+                const uint64_t t0 = now_ns();
                 complete(l, e == cudaSuccess ? PARALLAX_OK : PARALLAX_ERR_CUDA);
+                complete_ns.fetch_add(now_ns() - t0, std::memory_order_relaxed);
                 if (e != cudaSuccess) cudaGetLastError();
                 progress = true;
             }
             std::unique_lock<std::mutex> lk(mu);
             for (size_t li = lo; li < hi; ++li) {
                 Lane& l = lanes[li];
-                if (l.busy || queue.empty()) continue;
+                if (l.busy || !queued) continue;
+                const uint64_t t0 = now_ns();
                 std::vector<Request*> b = form_batch();
                 if (b.empty()) break;
                 l.reqs = std::move(b);
@@ -365,11 +406,12 @@ class Server {
                     cudaGetLastError();
                     complete(l, st);
                 }
+                launch_ns.fetch_add(now_ns() - t0, std::memory_order_relaxed);
                 lk.lock();
                 progress = true;
                 any_busy = true;
             }
-            if (stopping && queue.empty() && !any_busy) {
+            if (stopping && !queued && !any_busy) {
                 bool busy = false;
                 for (size_t li = lo; li < hi; ++li) busy |= lanes[li].busy;
                 if (!busy) break;
@@ -379,7 +421,7 @@ class Server {
                 lk.unlock();
                 std::this_thread::yield();  // poll the lanes' events
             } else {
-                cv_sched.wait(lk, [&] { return stopping || !queue.empty(); });
+                cv_sched.wait(lk, [&] { return stopping || queued; });
             }
         }
     }
@@ -502,9 +544,7 @@ PXB_EXPORT int parallax_serve_submit(const parallax_request* req, uint64_t* tick
     if (r->n == 0) {  // nothing to do on the device
         if (r->result && (r->op == ReqOp::REDUCE || r->op == ReqOp::COMPACT))
             memset(r->result, 0, r->op == ReqOp::REDUCE ? r->es : 8);
-        r->done = true;
-        r->done_ns = now_ns();
-        r->released.store(true, std::memory_order_release);
+        finish(r, PARALLAX_OK);
     } else {
         s->submit(r);
     }
@@ -550,8 +590,10 @@ PXB_EXPORT int parallax_serve_get_stats(parallax_serve_stats* out) {
     }
     std::lock_guard<std::mutex> g2(g_srv->mu);
     *out = g_srv->stats;
-    out->inflight_bytes = g_srv->inflight;
-    out->queued = g_srv->queue.size();
+    out->launch_ns = g_srv->launch_ns.load();
+    out->complete_ns = g_srv->complete_ns.load();
+    out->inflight_bytes = g_srv->inflight.load();
+    out->queued = g_srv->queued;
     return PARALLAX_OK;
 }
 

@@ -83,6 +83,12 @@ def mix(px, dev, ox, seed0=100):
         out.append(Req(px, dev, "copy_if:f32:gt:0.5", make(ox, "f32", n, s + 5000), "compact"))
         out.append(Req(px, dev, "remove_if:i32:lt:0", make(ox, "i32", n, s + 6000), "compact"))
         out.append(Req(px, dev, "copy_if:i32:mod:3:0", make(ox, "i32", n, s + 7000), "compact"))
+        # same operation and type, another predicate: must never share a launch with the above
+        out.append(Req(px, dev, "copy_if:i32:mod:5:1", make(ox, "i32", n, s + 7500), "compact"))
+        # key-value records with random values: sorted stably by key, not by the whole record
+        recs = (make(ox, "u32", n, s + 8000).astype(np.uint64) % np.uint64(37)) << np.uint64(32)
+        recs |= make(ox, "u32", n, s + 8500).astype(np.uint64)
+        out.append(Req(px, dev, "sort_kv:u32", recs, "sort"))
     return out
 
 
@@ -98,11 +104,14 @@ def oracle_of(ox, r: Req):
         return ox.scan(x, exclusive=True, init=3)
     if r.kind == "scan":
         return ox.scan(x)
+    if r.kind == "sort" and r.spec.startswith("sort_kv"):
+        return x[np.argsort(x >> np.uint64(32), kind="stable")]
     if r.kind == "sort":
         return ox.sort(x)
     pk = {"gt": ox.P_GT, "lt": ox.P_LT, "mod": ox.P_MOD}[r.spec.split(":")[2]]
     if pk == ox.P_MOD:
-        out, k = ox.compact(x, ox.COPY_IF, pk, 0, 3, 0)
+        m, rem = (int(v) for v in r.spec.split(":")[3:5])
+        out, k = ox.compact(x, ox.COPY_IF, pk, 0, m, rem)
     else:
         c = float(r.spec.split(":")[3])
         out, k = ox.compact(x, ox.REMOVE_IF if r.spec.startswith("remove") else ox.COPY_IF, pk, c)
