@@ -131,103 +131,76 @@ Workspace* new_workspace() {
 // launch.
 static constexpr size_t kStatusEntry = sizeof(StatusEntry);
 
+// Replaces a workspace buffer by a larger one (at least `bytes`, doubling from `min_cap`),
+// optionally zeroed. In stream order: cudaFreeAsync / cudaMallocAsync on the workspace's
+// stream wait only for that stream's earlier work (which may still use the old buffer),
+// where cudaStreamSynchronize + cudaFree + cudaMalloc would also wait for every other stream
+// of the device - a lane of the serving loop that met a larger request than before stalled
+// behind the other lanes' running sorts. Growth inside a stream capture is refused.
+static bool regrow(Workspace& ws, void** buf, size_t* cap_io, size_t bytes, size_t min_cap,
+                   bool zero, const char* what) {
+    cudaStream_t s = ws.stream();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "%s: buffer growth inside a stream capture", what);
+        return false;
+    }
+    cudaGetLastError();
+    if (*buf) {
+        if (!cuda_ok(cudaFreeAsync(*buf, s), what)) return false;
+        *buf = nullptr;
+        *cap_io = 0;
+    }
+    size_t cap = min_cap;
+    while (cap < bytes) cap <<= 1;
+    if (!cuda_ok(cudaMallocAsync(buf, cap, s), what)) {
+        *buf = nullptr;
+        return false;
+    }
+    if (zero && !cuda_ok(cudaMemsetAsync(*buf, 0, cap, s), what)) return false;
+    *cap_io = cap;
+    ++ws.generation;
+    return true;
+}
+
 char* Workspace::scratch(uint64_t tiles) {
     size_t bytes = kScratchSmall + tiles * kStatusEntry;
     if (bytes <= scratch_cap) return static_cast<char*>(d_scratch);
-    // Growth: earlier launches on this stream may still use the old buffer.
-    cudaStream_t s = stream();
-    if (d_scratch) {
-        if (!cuda_ok(cudaStreamSynchronize(s), "scratch sync")) return nullptr;
-        cudaFree(d_scratch);
-        d_scratch = nullptr;
-        scratch_cap = 0;
-    }
-    size_t cap = 1 << 20;
-    while (cap < bytes) cap <<= 1;
-    if (!cuda_ok(cudaMalloc(&d_scratch, cap), "cudaMalloc(scratch)")) return nullptr;
-    // Zero once: look-back status words then read as "not ready" for every epoch, and
-    // the self-resetting ticket counters start at zero.
-    if (!cuda_ok(cudaMemsetAsync(d_scratch, 0, cap, s), "cudaMemset(scratch)")) return nullptr;
-    scratch_cap = cap;
+    // Zeroed: look-back status words then read as "not ready" for every epoch, and the
+    // self-resetting ticket counters start at zero.
+    if (!regrow(*this, &d_scratch, &scratch_cap, bytes, 1 << 20, true, "scratch")) return nullptr;
     epoch = 1;
-    ++generation;
     return static_cast<char*>(d_scratch);
 }
 
 void* Workspace::seg(size_t bytes) {
     if (bytes <= seg_cap) return d_seg;
-    cudaStream_t s = stream();
-    if (d_seg) {
-        if (!cuda_ok(cudaStreamSynchronize(s), "segment buffer sync")) return nullptr;
-        cudaFree(d_seg);
-        d_seg = nullptr;
-        seg_cap = 0;
-    }
-    size_t cap = 1 << 20;
-    while (cap < bytes) cap <<= 1;
-    if (!cuda_ok(cudaMalloc(&d_seg, cap), "cudaMalloc(segment buffer)")) return nullptr;
-    if (!cuda_ok(cudaMemsetAsync(d_seg, 0, cap, s), "cudaMemset(segment buffer)")) return nullptr;
-    seg_cap = cap;
-    ++generation;
-    return d_seg;
+    return regrow(*this, &d_seg, &seg_cap, bytes, 1 << 20, true, "segment buffer") ? d_seg : nullptr;
 }
 
 void* Workspace::seg_status(uint64_t entries) {
     if (entries <= seg_status_cap) return d_seg_status;
-    cudaStream_t s = stream();
-    if (d_seg_status) {
-        if (!cuda_ok(cudaStreamSynchronize(s), "segment status sync")) return nullptr;
-        cudaFree(d_seg_status);
-        d_seg_status = nullptr;
-        seg_status_cap = 0;
-    }
-    uint64_t cap = 1 << 14;
-    while (cap < entries) cap <<= 1;
-    if (!cuda_ok(cudaMalloc(&d_seg_status, cap * kStatusEntry), "cudaMalloc(segment status)"))
+    size_t bytes_cap = seg_status_cap * kStatusEntry;
+    if (!regrow(*this, &d_seg_status, &bytes_cap, entries * kStatusEntry, (1 << 14) * kStatusEntry,
+                true, "segment status"))
         return nullptr;
-    if (!cuda_ok(cudaMemsetAsync(d_seg_status, 0, cap * kStatusEntry, s), "cudaMemset(segment status)"))
-        return nullptr;
-    seg_status_cap = cap;
-    ++generation;
+    seg_status_cap = bytes_cap / kStatusEntry;
     return d_seg_status;
 }
 
 void* Workspace::radix(size_t bytes) {
     if (bytes <= radix_cap) return d_radix;
-    cudaStream_t s = stream();
-    if (d_radix) {
-        if (!cuda_ok(cudaStreamSynchronize(s), "radix buffer sync")) return nullptr;
-        cudaFree(d_radix);
-        d_radix = nullptr;
-        radix_cap = 0;
-    }
-    size_t cap = 1 << 20;
-    while (cap < bytes) cap <<= 1;
-    if (!cuda_ok(cudaMalloc(&d_radix, cap), "cudaMalloc(radix buffer)")) return nullptr;
-    if (!cuda_ok(cudaMemsetAsync(d_radix, 0, cap, s), "cudaMemset(radix buffer)")) return nullptr;
-    radix_cap = cap;
+    if (!regrow(*this, &d_radix, &radix_cap, bytes, 1 << 20, true, "radix buffer")) return nullptr;
     radix_epoch = 1;
-    ++generation;
     return d_radix;
 }
 
 void* Workspace::seg_radix(size_t bytes) {
     if (bytes <= seg_radix_cap) return d_seg_radix;
-    cudaStream_t s = stream();
-    if (d_seg_radix) {
-        if (!cuda_ok(cudaStreamSynchronize(s), "segmented radix buffer sync")) return nullptr;
-        cudaFree(d_seg_radix);
-        d_seg_radix = nullptr;
-        seg_radix_cap = 0;
-    }
-    size_t cap = 1 << 20;
-    while (cap < bytes) cap <<= 1;
-    if (!cuda_ok(cudaMalloc(&d_seg_radix, cap), "cudaMalloc(segmented radix buffer)")) return nullptr;
-    if (!cuda_ok(cudaMemsetAsync(d_seg_radix, 0, cap, s), "cudaMemset(segmented radix buffer)"))
-        return nullptr;
-    seg_radix_cap = cap;
-    ++generation;
-    return d_seg_radix;
+    return regrow(*this, &d_seg_radix, &seg_radix_cap, bytes, 1 << 20, true,
+                  "segmented radix buffer")
+               ? d_seg_radix
+               : nullptr;
 }
 
 bool Workspace::copy_streams() {
@@ -299,36 +272,14 @@ bool graph_launch(Workspace& ws, const std::string& key, const std::function<boo
 
 void* Workspace::temp(size_t bytes) {
     if (bytes <= temp_cap) return d_temp;
-    cudaStream_t s = stream();
-    if (d_temp) {
-        if (!cuda_ok(cudaStreamSynchronize(s), "temp sync")) return nullptr;
-        cudaFree(d_temp);
-        d_temp = nullptr;
-        temp_cap = 0;
-    }
-    size_t cap = 1 << 20;
-    while (cap < bytes) cap <<= 1;
-    if (!cuda_ok(cudaMalloc(&d_temp, cap), "cudaMalloc(temp)")) return nullptr;
-    temp_cap = cap;
-    ++generation;
-    return d_temp;
+    return regrow(*this, &d_temp, &temp_cap, bytes, 1 << 20, false, "temp") ? d_temp : nullptr;
 }
 
 void* Workspace::stage(int slot, size_t bytes) {
     if (bytes <= stage_cap[slot]) return d_stage[slot];
-    cudaStream_t s = stream();
-    if (d_stage[slot]) {
-        if (!cuda_ok(cudaStreamSynchronize(s), "stage sync")) return nullptr;
-        cudaFree(d_stage[slot]);
-        d_stage[slot] = nullptr;
-        stage_cap[slot] = 0;
-    }
-    size_t cap = 1 << 20;
-    while (cap < bytes) cap <<= 1;
-    if (!cuda_ok(cudaMalloc(&d_stage[slot], cap), "cudaMalloc(stage)")) return nullptr;
-    stage_cap[slot] = cap;
-    ++generation;
-    return d_stage[slot];
+    return regrow(*this, &d_stage[slot], &stage_cap[slot], bytes, 1 << 20, false, "stage")
+               ? d_stage[slot]
+               : nullptr;
 }
 
 uint32_t Workspace::next_epoch() {
@@ -479,7 +430,18 @@ PXB_EXPORT int parallax_set_stream(void* cuda_stream) {
     settle_deferred_here();
     Workspace* ws = workspace();
     if (!ws) return PARALLAX_ERR_NO_DEVICE;
-    ws->user_stream = static_cast<cudaStream_t>(cuda_stream);
+    cudaStream_t next = static_cast<cudaStream_t>(cuda_stream);
+    cudaStream_t prev = ws->stream();
+    if ((next ? next : ws->own_stream) != prev) {
+        // The workspace buffers pass from one stream to the other: work on the new stream
+        // is ordered after what the old one has enqueued (async calls still running there
+        // use the same scratch, and buffer growth frees in stream order).
+        if (!cuda_ok(cudaEventRecord(ws->done, prev), "cudaEventRecord(set_stream)") ||
+            !cuda_ok(cudaStreamWaitEvent(next ? next : ws->own_stream, ws->done, 0),
+                     "cudaStreamWaitEvent(set_stream)"))
+            return PARALLAX_ERR_CUDA;
+    }
+    ws->user_stream = next;
     return PARALLAX_OK;
 }
 PXB_EXPORT int parallax_set_async(int async) {

@@ -26,6 +26,7 @@
 // was batched with (integer results are bit-exact, floating-point ones are within the
 // primitives' stated tolerance of the fp64 oracle either way).
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 #include <time.h>
 
@@ -134,9 +135,11 @@ struct Lane {
     uint64_t* d_res = nullptr;   // device alias of h_res
     std::vector<Request*> reqs;
     bool busy = false;
-    // temporaries of a coalesced sort batch (one per request, 256-byte aligned), grown when a
-    // batch needs more; only this lane's scheduler thread touches it, between its batches
-    void* d_tmp = nullptr;
+    // temporaries of a coalesced sort batch (one per request, 256-byte aligned): a
+    // device-resident arena block, grown when a batch needs more (arena blocks come and go
+    // without the device synchronisation of cudaMalloc / cudaFree, which would stall every
+    // lane behind the running sorts); only this lane's scheduler thread touches it
+    void* tmp_block = nullptr;  // host-side arena address
     size_t tmp_cap = 0;
 };
 
@@ -165,7 +168,10 @@ class Server {
         if (cfg.max_batch == 0) cfg.max_batch = 1024;
         if (cfg.solo_elements == 0) cfg.solo_elements = 1ull << 18;
         if (cfg.inflight_bytes == 0) cfg.inflight_bytes = parallax_arena_capacity() / 2;
-        if (cfg.schedulers == 0) cfg.schedulers = 2;
+        if (cfg.schedulers == 0) {
+            const char* e = getenv("PARALLAX_SERVE_SCHEDULERS");
+            cfg.schedulers = e && atoi(e) > 0 ? (uint32_t)atoi(e) : 2;
+        }
         if (cfg.schedulers > cfg.lanes) cfg.schedulers = cfg.lanes;
         lanes.resize(cfg.lanes);
         for (Lane& l : lanes) {
@@ -210,7 +216,7 @@ class Server {
     ~Server() {
         for (Lane& l : lanes) {
             if (l.ws) cudaStreamSynchronize(l.ws->stream());
-            if (l.d_tmp) cudaFree(l.d_tmp);
+            if (l.tmp_block) parallax_arena_free(l.tmp_block);
             if (l.d_desc) cudaFree(l.d_desc);
             if (l.h_desc) cudaFreeHost(l.h_desc);
             if (l.h_res) cudaFreeHost(l.h_res);
@@ -291,18 +297,20 @@ class Server {
             size_t need = 0;
             for (size_t i = 0; i < S; ++i) need += (l.reqs[i]->n * l.reqs[i]->es + 255) / 256 * 256;
             if (need > l.tmp_cap) {  // the lane is idle between its batches: safe to replace
-                if (l.d_tmp) cudaFree(l.d_tmp);
-                l.d_tmp = nullptr;
+                if (l.tmp_block) parallax_arena_free(l.tmp_block);
+                l.tmp_block = nullptr;
                 l.tmp_cap = 0;
                 const size_t cap = need + need / 2;
-                if (cudaMalloc(&l.d_tmp, cap) != cudaSuccess) {
-                    cudaGetLastError();
+                void* blk = parallax_arena_alloc(cap, 256);
+                if (!blk) {
                     set_error(PARALLAX_ERR_OUT_OF_MEMORY, "serve: sort temporaries of %zu bytes", need);
                     return false;
                 }
+                parallax_arena_set_residency(blk, PARALLAX_DEVICE_RESIDENT);
+                l.tmp_block = blk;
                 l.tmp_cap = cap;
             }
-            tmp = static_cast<char*>(l.d_tmp);
+            tmp = static_cast<char*>(arena_dev(l.tmp_block));
         }
         uint64_t total = 0, max_len = 0;
         for (size_t i = 0; i < S; ++i) {
