@@ -220,7 +220,9 @@ struct Arena {
             }
             return commit((size_t)(p - host_base), need);
         }
-        // first fit in offset order
+        // first fit in offset order (a best-fit index by size, measured on the serving mix of
+        // small requests with hundreds of blocks live, made allocation-heavy clients ~10 %
+        // slower: the first fitting range is usually among the first few)
         for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
             size_t off = align_up(it->first, a);
             size_t pad = off - it->first;
@@ -445,7 +447,8 @@ using namespace pxb;
 
 PXB_EXPORT void* parallax_arena_alloc(size_t size, size_t align) {
     void* p = arena().allocate(size, align ? align : 16);
-    if (getenv("PARALLAX_DEBUG"))
+    static const bool debug = getenv("PARALLAX_DEBUG") != nullptr;
+    if (debug)
         fprintf(stderr, "[parallax_arena_alloc] %zu bytes -> %p\n", size, p);
     return p;
 }

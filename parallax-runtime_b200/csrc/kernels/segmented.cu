@@ -174,6 +174,39 @@ k_item_descs(SegSrc src, uint64_t S, const uint32_t* __restrict__ item_start,
     }
 }
 
+// The planner and k_item_descs in one launch, for work lists of at most kPlanItemsMax
+// items (one launch less per call: a batch of small requests costs its host thread a
+// launch, not the device time). item_start is read back with plain loads: this CTA wrote it.
+constexpr uint64_t kPlanItemsMax = 8192;
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_seg_plan_items(SegSrc src, uint64_t S, uint64_t count, uint32_t tile, uint32_t* item_start,
+                 uint32_t* counters, SegEmpty empty, uint32_t* seg_zero, StatusEntry* status,
+                 uint64_t status_cap, volatile int32_t* err, ItemDesc* __restrict__ items) {
+    seg_plan_block<BLOCK>(src, S, count, tile, item_start, counters, empty, seg_zero, status,
+                          status_cap, err, nullptr);
+    __syncthreads();
+    const uint32_t total = item_start[S];
+    for (uint32_t i = threadIdx.x; i < total; i += BLOCK) {
+        uint64_t lo = 0, hi = S;  // largest s with item_start[s] <= i
+        while (hi - lo > 1) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (item_start[mid] <= i) lo = mid;
+            else hi = mid;
+        }
+        ItemDesc d;
+        d.seg = (uint32_t)lo;
+        d.first_item = item_start[lo];
+        d.seg_items = item_start[lo + 1] - d.first_item;
+        d.k = i - d.first_item;
+        d.len = src.len(lo);
+        d.in = src.in_addr(lo);
+        d.out = src.out_addr(lo);
+        d.aux = src.aux_addr(lo);
+        items[i] = d;
+    }
+}
+
 __device__ __forceinline__ ItemDesc load_desc(const ItemDesc* items, uint32_t i) {
     const uint4* p = reinterpret_cast<const uint4*>(items + i);
     uint4 w[3];
@@ -462,7 +495,7 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                 s_prev = begin > 0 ? in[begin - 1] : T(0);
             __syncthreads();
             // this thread's row: slots [tid * ITEMS, +ITEMS) = tile indices from r0
-            const int r0 = tid * ITEMS - (int)mis;
+            [[maybe_unused]] const int r0 = tid * ITEMS - (int)mis;
             T x[ITEMS];
             {
                 const uint4* row = reinterpret_cast<const uint4*>(sm + tid * ITEMS);
@@ -751,6 +784,13 @@ bool enqueue_shape(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     args.red = c.red;
     args.pred = make_seg_pred<T>(c.pred);
     auto plan = [&](SegEmpty empty, bool tickets) {
+        if (items_cap <= kPlanItemsMax) {
+            k_seg_plan_items<256><<<1, 256, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE,
+                                                    b.item_start, b.counters, empty,
+                                                    tickets ? b.tickets : nullptr, b.status,
+                                                    b.status_cap, err, b.items);
+            return;
+        }
         k_seg_plan<256><<<1, 256, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE, b.item_start,
                                           b.counters, empty, tickets ? b.tickets : nullptr,
                                           b.status, b.status_cap, err, nullptr);
@@ -939,7 +979,12 @@ bool run(Workspace& ws, const SegCall& c, bool graph) {
     // data-dependent and partition writes every element)
     const uint64_t bytes = (c.op == SEG_SCAN || c.op == SEG_PARTITION ? 2 : 1) * c.count * es;
     ProfScope prof(ws, op_name(c), bytes);
-    count_launch(c.op == SEG_PARTITION ? 4 : 3);
+    {  // planner (+ item descriptors unless it writes them) + the pass(es)
+        const uint64_t V = 16 / es;
+        const uint64_t tile = (uint64_t)kShapes[shape].block * kShapes[shape].vpt * V - V;
+        const int plan = items_bound(c, tile) <= kPlanItemsMax ? 1 : 2;
+        count_launch(plan + (c.op == SEG_PARTITION ? 2 : 1));
+    }
     if (!graph) return enqueue(ws, c, shape);
     return graph_launch(ws, graph_key(c, shape), [&] { return enqueue(ws, c, shape); });
 }

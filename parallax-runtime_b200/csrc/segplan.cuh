@@ -93,12 +93,15 @@ enum class SegEmpty : int { NONE = 0, ZERO_RESULT = 1, ZERO_COUNT = 2 };
 // CSR offsets that are not non-decreasing within [0, count] write kErrSegmentOffsets to the
 // mapped error word; such segments get no work items, so no kernel touches memory outside
 // the caller's buffers.
+// The planner's work, by one CTA of BLOCK threads (k_seg_plan; planners that go on to write
+// more of the work list call it first).
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK)
-k_seg_plan(SegSrc src, uint64_t S, uint64_t count, uint32_t tile,
-           uint32_t* __restrict__ item_start, uint32_t* __restrict__ counters, SegEmpty empty,
-           uint32_t* __restrict__ seg_zero, StatusEntry* status, uint64_t status_cap,
-           volatile int32_t* err, uint32_t* __restrict__ item_seg) {
+__device__ __forceinline__ void seg_plan_block(SegSrc src, uint64_t S, uint64_t count,
+                                               uint32_t tile, uint32_t* item_start,
+                                               uint32_t* counters, SegEmpty empty,
+                                               uint32_t* seg_zero, StatusEntry* status,
+                                               uint64_t status_cap, volatile int32_t* err,
+                                               uint32_t* item_seg) {
     __shared__ uint32_t s_warp[BLOCK / 32];
     __shared__ uint32_t s_carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -158,6 +161,16 @@ k_seg_plan(SegSrc src, uint64_t S, uint64_t count, uint32_t tile,
         __syncthreads();
         if (tid == 0) counters[2] = 1;
     }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_seg_plan(SegSrc src, uint64_t S, uint64_t count, uint32_t tile,
+           uint32_t* __restrict__ item_start, uint32_t* __restrict__ counters, SegEmpty empty,
+           uint32_t* __restrict__ seg_zero, StatusEntry* status, uint64_t status_cap,
+           volatile int32_t* err, uint32_t* __restrict__ item_seg) {
+    seg_plan_block<BLOCK>(src, S, count, tile, item_start, counters, empty, seg_zero, status,
+                          status_cap, err, item_seg);
 }
 
 struct Workspace;

@@ -90,8 +90,17 @@ void finish(Request* r, int status) {
 // within microseconds of their launch, so the waiter first polls the completion flag for up
 // to 20 us, then sleeps between polls (about 20 us asked; the kernel's timer slack makes it
 // longer), which costs a long request no more than that in latency.
+// How long a waiter polls its request's flag before it sleeps (PARALLAX_SERVE_SPIN_US).
+uint64_t spin_ns() {
+    static const uint64_t ns = [] {
+        const char* e = getenv("PARALLAX_SERVE_SPIN_US");
+        return (e && *e ? strtoull(e, nullptr, 10) : 20ull) * 1000ull;
+    }();
+    return ns;
+}
+
 int wait_request(Request* r, uint64_t* done_ns) {
-    const uint64_t poll_until = now_ns() + 20000;
+    const uint64_t poll_until = now_ns() + spin_ns();
     for (int i = 1; !r->released.load(std::memory_order_acquire); ++i) {
         __builtin_ia32_pause();
         if ((i & 63) == 0 && now_ns() > poll_until) break;
@@ -129,7 +138,8 @@ KindKey kind_key(const Request& r) {
 struct Lane {
     Workspace* ws = nullptr;
     cudaEvent_t done = nullptr;
-    SegDesc* h_desc = nullptr;   // pinned
+    SegDesc* h_desc = nullptr;   // pinned, mapped
+    SegDesc* m_desc = nullptr;   // device alias of h_desc
     SegDesc* d_desc = nullptr;   // device
     uint64_t* h_res = nullptr;   // pinned, mapped: one 8-byte result slot per request
     uint64_t* d_res = nullptr;   // device alias of h_res
@@ -178,7 +188,10 @@ class Server {
             l.ws = new_workspace();
             if (!l.ws) return false;
             if (!cuda_ok(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming), "serve event") ||
-                !cuda_ok(cudaHostAlloc((void**)&l.h_desc, cfg.max_batch * sizeof(SegDesc), 0),
+                !cuda_ok(cudaHostAlloc((void**)&l.h_desc, cfg.max_batch * sizeof(SegDesc),
+                                       cudaHostAllocMapped),
+                         "serve descriptors (host)") ||
+                !cuda_ok(cudaHostGetDevicePointer((void**)&l.m_desc, l.h_desc, 0),
                          "serve descriptors (host)") ||
                 !cuda_ok(cudaMalloc((void**)&l.d_desc, cfg.max_batch * sizeof(SegDesc)),
                          "serve descriptors (device)") ||
@@ -329,20 +342,24 @@ class Server {
             total += r.n;
             if (r.n > max_len) max_len = r.n;
         }
-        if (!cuda_ok(cudaMemcpyAsync(l.d_desc, l.h_desc, S * sizeof(SegDesc), cudaMemcpyHostToDevice, s),
-                     "serve descriptor upload"))
-            return false;
+        // Reduce, scan and compaction read the descriptors only in their planner (once per
+        // segment and per work item), so they read the mapped host table in place: no
+        // upload call. The sorts read them in every pass: they get a device copy.
         switch (h.op) {
             case ReqOp::REDUCE:
-                return launch_segmented_descs(ws, SegKind::REDUCE, h.t, h.pred, false, 0, l.d_desc,
+                return launch_segmented_descs(ws, SegKind::REDUCE, h.t, h.pred, false, 0, l.m_desc,
                                               S, total, h.red);
             case ReqOp::SCAN:
                 return launch_segmented_descs(ws, SegKind::SCAN, h.t, h.pred, !h.exclusive,
-                                              h.exclusive ? h.init_bits : 0, l.d_desc, S, total);
+                                              h.exclusive ? h.init_bits : 0, l.m_desc, S, total);
             case ReqOp::COMPACT:
-                return launch_segmented_descs(ws, SegKind::COPY_IF, h.t, h.pred, false, 0, l.d_desc,
+                return launch_segmented_descs(ws, SegKind::COPY_IF, h.t, h.pred, false, 0, l.m_desc,
                                               S, total, RedOp::SUM, h.mode);
             case ReqOp::SORT:
+                if (!cuda_ok(cudaMemcpyAsync(l.d_desc, l.h_desc, S * sizeof(SegDesc),
+                                             cudaMemcpyHostToDevice, s),
+                             "serve descriptor upload"))
+                    return false;
                 return launch_segmented_sort_descs(ws, h.t, l.d_desc, S, total, max_len, h.by_key);
         }
         return false;
