@@ -94,7 +94,6 @@ static_assert(sizeof(ItemDesc) == 48, "item descriptor layout");
 struct SegBuffers {
     uint32_t* item_start;  // num_segments + 1
     ItemDesc* items;       // one per work item
-    uint32_t* tickets;     // num_segments, zeroed by the planner
     uint64_t* partials;    // one per work item
     StatusEntry* status;   // one per work item (a buffer of its own)
     uint64_t status_cap;   // entries in that buffer
@@ -333,6 +332,40 @@ __device__ __forceinline__ uint32_t lane_mask_lt() {
     return m;
 }
 
+// Second pass of a segmented reduce (and of the partition's count pass): one warp per
+// segment of more than one work item folds the items' partials in item order (lane-strided,
+// then the warp's tree) and writes the segment's result; one-item segments were written by
+// their item. A pass of its own instead of a last-arriving-item ticket keeps the fence and
+// the atomic off every item's path.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_seg_fold(SegBuffers b, uint64_t S, int red) {
+    using A = typename SegAcc<T>::type;
+    const uint64_t s = ((uint64_t)blockIdx.x * 256 + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= S) return;
+    const uint32_t first = b.item_start[s], n = b.item_start[s + 1] - first;
+    if (n < 2) return;
+    const uint64_t aux = b.items[first].aux;
+    if (red == RED_MAX || red == RED_MIN) {
+        T m = red_identity<T>(red);
+        for (uint32_t i = lane; i < n; i += 32) {
+            const T v = get_val<T>(&b.partials[first + i]);
+            m = red == RED_MAX ? OpMax()(m, v) : OpMin()(m, v);
+        }
+        m = red == RED_MAX ? warp_reduce(m, OpMax()) : warp_reduce(m, OpMin());
+        if (lane == 0) *reinterpret_cast<T*>(aux) = m;
+    } else {
+        A f = A(0);
+        for (uint32_t i = lane; i < n; i += 32) f = f + get_val<A>(&b.partials[first + i]);
+        f = warp_reduce(f, OpSum());
+        if (lane == 0) {
+            if (red == RED_COUNT) *reinterpret_cast<uint64_t*>(aux) = (uint64_t)f;
+            else *reinterpret_cast<T*>(aux) = (T)f;
+        }
+    }
+}
+
 // ---- the persistent kernel -------------------------------------------------------------------------
 template <typename T, int BLOCK, int VPT, int OP>
 __global__ void __launch_bounds__(BLOCK)
@@ -353,7 +386,6 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
     __shared__ ItemDesc s_it;
     __shared__ uint32_t s_item;
     __shared__ T s_prev;
-    __shared__ bool s_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t total = b.item_start[a.S];
     TileStatus<A> ts;
@@ -459,32 +491,15 @@ k_segmented(SegArgs<T> a, SegBuffers b, volatile int32_t* err) {
                 if (count) *reinterpret_cast<uint64_t*>(it.aux) = (uint64_t)sum;
                 else *reinterpret_cast<T*>(it.aux) = mm ? m : (T)sum;
             };
-            if (it.seg_items == 1) {
-                if (tid == 0) write(tot, totm);
-            } else {
-                if (tid == 0) {
-                    if (mm) put_val(&b.partials[item], totm);
-                    else put_val(&b.partials[item], tot);
-                    __threadfence();
-                    s_last = atomicAdd(&b.tickets[it.seg], 1u) == it.seg_items - 1;
-                }
-                __syncthreads();
-                if (s_last) {  // fold the segment's partials in item order
-                    __threadfence();
-                    A f = A(0);
-                    T fm = red_identity<T>(a.red);
-                    for (uint32_t i = tid; i < it.seg_items; i += BLOCK) {
-                        if (a.red == RED_MAX) fm = OpMax()(fm, get_val<T>(&b.partials[it.first_item + i]));
-                        else if (a.red == RED_MIN) fm = OpMin()(fm, get_val<T>(&b.partials[it.first_item + i]));
-                        else f = f + get_val<A>(&b.partials[it.first_item + i]);
-                    }
-                    if (a.red == RED_MAX) fm = block_fold<BLOCK>(fm, redT, OpMax());
-                    else if (a.red == RED_MIN) fm = block_fold<BLOCK>(fm, redT, OpMin());
-                    else f = block_fold<BLOCK>(f, red, OpSum());
-                    if (tid == 0) write(f, fm);
-                }
+            // A one-item segment's result is final; otherwise the item leaves its partial
+            // for k_seg_fold (no fence, ticket or extra barrier on the item's path: the next
+            // item's loads follow at once). block_fold's closing barrier has ordered every
+            // read of s_it and of the fold scratch before the next claim overwrites them.
+            if (tid == 0) {
+                if (it.seg_items == 1) write(tot, totm);
+                else if (mm) put_val(&b.partials[item], totm);
+                else put_val(&b.partials[item], tot);
             }
-            __syncthreads();
         } else {
             if (vec_ok) {
                 stage<T, BLOCK, VPT>(sm, in, begin, len, mis, T(0));
@@ -698,7 +713,7 @@ constexpr int min_tile() {  // the smallest tile of any shape, in elements of T
 // Carves the buffers for S segments and at most `items` work items out of the workspace's
 // segment buffer (zeroed when it is (re)allocated).
 bool seg_buffers(Workspace& ws, uint64_t S, uint64_t items, SegBuffers* out) {
-    const size_t need = 256 + up256((S + 1) * 4) + up256(S * 4) + up256(items * 8) +
+    const size_t need = 256 + up256((S + 1) * 4) + up256(items * 8) +
                         up256(items * sizeof(ItemDesc));
     char* p = static_cast<char*>(ws.seg(need));
     out->status = static_cast<StatusEntry*>(ws.seg_status(items));
@@ -708,8 +723,6 @@ bool seg_buffers(Workspace& ws, uint64_t S, uint64_t items, SegBuffers* out) {
     p += 256;
     out->item_start = reinterpret_cast<uint32_t*>(p);
     p += up256((S + 1) * 4);
-    out->tickets = reinterpret_cast<uint32_t*>(p);
-    p += up256(S * 4);
     out->partials = reinterpret_cast<uint64_t*>(p);
     p += up256(items * 8);
     out->items = reinterpret_cast<ItemDesc*>(p);
@@ -768,6 +781,13 @@ bool launch_kernel(Workspace& ws, const SegArgs<T>& args, const SegBuffers& b, u
     return cuda_ok(cudaGetLastError(), "segmented launch");
 }
 
+template <typename T>
+bool launch_fold(Workspace& ws, const SegBuffers& b, uint64_t S, int red) {
+    const uint64_t blocks = (S * 32 + 255) / 256;
+    k_seg_fold<T><<<(unsigned)(blocks ? blocks : 1), 256, 0, ws.stream()>>>(b, S, red);
+    return cuda_ok(cudaGetLastError(), "segmented fold launch");
+}
+
 template <typename T, int BLOCK, int VPT>
 bool enqueue_shape(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     using Sh = SegShape<T, BLOCK, VPT>;
@@ -783,16 +803,16 @@ bool enqueue_shape(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     args.unique = c.unique;
     args.red = c.red;
     args.pred = make_seg_pred<T>(c.pred);
-    auto plan = [&](SegEmpty empty, bool tickets) {
+    auto plan = [&](SegEmpty empty) {
         if (items_cap <= kPlanItemsMax) {
             k_seg_plan_items<256><<<1, 256, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE,
                                                     b.item_start, b.counters, empty,
-                                                    tickets ? b.tickets : nullptr, b.status,
+                                                    nullptr, b.status,
                                                     b.status_cap, err, b.items);
             return;
         }
         k_seg_plan<256><<<1, 256, 0, s>>>(c.src, c.S, c.count, (uint32_t)TILE, b.item_start,
-                                          b.counters, empty, tickets ? b.tickets : nullptr,
+                                          b.counters, empty, nullptr,
                                           b.status, b.status_cap, err, nullptr);
         const uint64_t dg = (items_cap + 255) / 256;
         k_item_descs<<<(unsigned)(dg < 1184 ? dg : 1184), 256, 0, s>>>(c.src, c.S, b.item_start,
@@ -800,21 +820,24 @@ bool enqueue_shape(Workspace& ws, const SegCall& c, const SegBuffers& b) {
     };
     switch (c.op) {
         case SEG_REDUCE:
-            plan(c.red == RED_COUNT ? SegEmpty::ZERO_COUNT : SegEmpty::ZERO_RESULT, true);
-            return launch_kernel<T, BLOCK, VPT, SEG_REDUCE>(ws, args, b, items_cap);
+            plan(c.red == RED_COUNT ? SegEmpty::ZERO_COUNT : SegEmpty::ZERO_RESULT);
+            return launch_kernel<T, BLOCK, VPT, SEG_REDUCE>(ws, args, b, items_cap) &&
+                   launch_fold<T>(ws, b, c.S, c.red);
         case SEG_SCAN:
-            plan(SegEmpty::NONE, false);
+            plan(SegEmpty::NONE);
             return launch_kernel<T, BLOCK, VPT, SEG_SCAN>(ws, args, b, items_cap);
         case SEG_SELECT:
-            plan(SegEmpty::ZERO_COUNT, false);
+            plan(SegEmpty::ZERO_COUNT);
             return launch_kernel<T, BLOCK, VPT, SEG_SELECT>(ws, args, b, items_cap);
         default: {
             // count pass (per-segment kept totals into the counts), then the scatter; the
             // count pass uses no look-back status, so the scatter takes the plan's epoch
             SegArgs<T> cnt = args;
             cnt.red = RED_COUNT;
-            plan(SegEmpty::ZERO_COUNT, true);
-            if (!launch_kernel<T, BLOCK, VPT, SEG_REDUCE>(ws, cnt, b, items_cap)) return false;
+            plan(SegEmpty::ZERO_COUNT);
+            if (!launch_kernel<T, BLOCK, VPT, SEG_REDUCE>(ws, cnt, b, items_cap) ||
+                !launch_fold<T>(ws, b, c.S, RED_COUNT))
+                return false;
             return launch_kernel<T, BLOCK, VPT, SEG_PARTITION>(ws, args, b, items_cap);
         }
     }
@@ -979,11 +1002,11 @@ bool run(Workspace& ws, const SegCall& c, bool graph) {
     // data-dependent and partition writes every element)
     const uint64_t bytes = (c.op == SEG_SCAN || c.op == SEG_PARTITION ? 2 : 1) * c.count * es;
     ProfScope prof(ws, op_name(c), bytes);
-    {  // planner (+ item descriptors unless it writes them) + the pass(es)
+    {  // planner (+ item descriptors unless it writes them) + the pass(es) (+ the fold)
         const uint64_t V = 16 / es;
         const uint64_t tile = (uint64_t)kShapes[shape].block * kShapes[shape].vpt * V - V;
         const int plan = items_bound(c, tile) <= kPlanItemsMax ? 1 : 2;
-        count_launch(plan + (c.op == SEG_PARTITION ? 2 : 1));
+        count_launch(plan + (c.op == SEG_PARTITION ? 3 : c.op == SEG_REDUCE ? 2 : 1));
     }
     if (!graph) return enqueue(ws, c, shape);
     return graph_launch(ws, graph_key(c, shape), [&] { return enqueue(ws, c, shape); });

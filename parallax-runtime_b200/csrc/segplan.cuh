@@ -102,34 +102,48 @@ __device__ __forceinline__ void seg_plan_block(SegSrc src, uint64_t S, uint64_t 
                                                uint32_t* seg_zero, StatusEntry* status,
                                                uint64_t status_cap, volatile int32_t* err,
                                                uint32_t* item_seg) {
+    // Each thread takes kPer consecutive segments of a chunk and issues all their length
+    // loads before using any, so a chunk of BLOCK * kPer segments costs about one memory
+    // round trip (one segment per thread per chunk made S = 4096 sixteen dependent rounds).
+    constexpr int kPer = 16;
     __shared__ uint32_t s_warp[BLOCK / 32];
     __shared__ uint32_t s_carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_carry = 0;
     __syncthreads();
-    for (uint64_t base = 0; base < S; base += BLOCK) {
-        const uint64_t s = base + tid;
-        uint32_t items = 0;
-        if (s < S) {
-            uint64_t len;
-            if (src.offsets) {
-                const uint64_t a = src.offsets[s], b = src.offsets[s + 1];
-                const bool bad = b < a || b > count;
-                if (bad) *err = kErrSegmentOffsets;
-                len = bad ? 0 : b - a;
-            } else {
-                len = src.descs[s].n;
+    for (uint64_t base = 0; base < S; base += (uint64_t)BLOCK * kPer) {
+        const uint64_t s0 = base + (uint64_t)tid * kPer;
+        uint64_t len[kPer];
+        if (src.offsets) {
+            uint64_t o[kPer + 1];
+#pragma unroll
+            for (int j = 0; j <= kPer; ++j) o[j] = s0 + j <= S ? src.offsets[s0 + j] : 0;
+#pragma unroll
+            for (int j = 0; j < kPer; ++j) {
+                const bool bad = o[j + 1] < o[j] || o[j + 1] > count;
+                if (s0 + j < S && bad) *err = kErrSegmentOffsets;
+                len[j] = s0 + j < S && !bad ? o[j + 1] - o[j] : 0;
             }
-            items = (uint32_t)((len + tile - 1) / tile);
-            if (len == 0 && empty != SegEmpty::NONE) {
-                void* slot = reinterpret_cast<void*>(src.aux_addr(s));
+        } else {
+#pragma unroll
+            for (int j = 0; j < kPer; ++j) len[j] = s0 + j < S ? src.descs[s0 + j].n : 0;
+        }
+        uint32_t items[kPer];
+        uint32_t mine = 0;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            items[j] = (uint32_t)((len[j] + tile - 1) / tile);
+            mine += items[j];
+            if (s0 + j >= S) continue;
+            if (len[j] == 0 && empty != SegEmpty::NONE) {
+                void* slot = reinterpret_cast<void*>(src.aux_addr(s0 + j));
                 if (empty == SegEmpty::ZERO_COUNT) *static_cast<uint64_t*>(slot) = 0;
                 else if (src.elem == 8) *static_cast<uint64_t*>(slot) = 0;  // +0.0 / 0
                 else *static_cast<uint32_t*>(slot) = 0;
             }
-            if (seg_zero) seg_zero[s] = 0;
+            if (seg_zero) seg_zero[s0 + j] = 0;
         }
-        const uint32_t incl = warp_inclusive_scan(items, OpSum());
+        const uint32_t incl = warp_inclusive_scan(mine, OpSum());
         if (lane == 31) s_warp[warp] = incl;
         __syncthreads();
         uint32_t woff = 0, total = 0;
@@ -139,11 +153,14 @@ __device__ __forceinline__ void seg_plan_block(SegSrc src, uint64_t S, uint64_t 
             if (w < warp) woff += v;
             total += v;
         }
-        if (s < S) {
-            const uint32_t first = s_carry + woff + incl - items;
-            item_start[s] = first;
+        uint32_t first = s_carry + woff + incl - mine;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) {
+            if (s0 + j >= S) break;
+            item_start[s0 + j] = first;
             if (item_seg)  // small work lists: the inverse map too (saves a launch)
-                for (uint32_t i = 0; i < items; ++i) item_seg[first + i] = (uint32_t)s;
+                for (uint32_t i = 0; i < items[j]; ++i) item_seg[first + i] = (uint32_t)(s0 + j);
+            first += items[j];
         }
         __syncthreads();
         if (tid == 0) s_carry += total;

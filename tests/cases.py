@@ -113,4 +113,7 @@ def segment_layouts() -> dict:
                                   16383, 16384, 16385]),
         "big_and_small": offsets_of([1 << 20] + [7] * 100 + [300001] + [0, 1]),
         "lognormal": lognormal_offsets(11, 500, 512, 2.0, 0, 1 << 18),
+        # more segments than the planner takes per chunk (256 threads x 16), ragged and
+        # partly empty: the chunks' carries and a partial last chunk
+        "many": offsets_of([int(v) for v in np.random.default_rng(5).integers(0, 40, 9001)]),
     }
