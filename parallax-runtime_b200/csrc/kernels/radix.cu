@@ -424,39 +424,65 @@ bool launch_pass(const K* in, K* out, uint64_t n, int shift, const unsigned long
 }
 
 // ---- segmented radix sort -------------------------------------------------------------------
-// Digit counts of every segment for digit positions p0 .. P-1, one CTA per work item (tile):
-// shared-memory counts of the tile, then one global atomic add per nonzero (position,
-// digit). seg_hist must be zero on entry.
+// Digit counts of every segment for digit positions p0 .. P-1. A CTA takes kSegHistItems
+// consecutive work items (tiles; consecutive items are mostly of one segment), loads each
+// tile's keys into registers before counting them in shared memory (one memory round trip
+// per tile), and adds its counts to the segment's histogram with one global atomic per
+// nonzero (position, digit) when the segment changes and at its end: a long segment costs
+// one flush per kSegHistItems tiles instead of one per tile. seg_hist must be zero on entry.
 constexpr int kSegHistBlock = 512;
+constexpr int kSegHistItems = 8;
 
 template <typename K, int XF>
 __global__ void __launch_bounds__(kSegHistBlock)
     k_seg_radix_hist(SegRadix sr, int p0, uint32_t* __restrict__ seg_hist) {
     constexpr int P = sizeof(K);
     constexpr int TILE = RadixShape<K>::BLOCK * RadixShape<K>::ITEMS;
+    constexpr int PER = (TILE + kSegHistBlock - 1) / kSegHistBlock;
     __shared__ uint32_t h[P][kBins];
-    const uint32_t item = blockIdx.x;
-    if (item >= sr.item_start[sr.S]) return;
+    const uint32_t total = sr.item_start[sr.S];
+    const uint32_t i0 = blockIdx.x * kSegHistItems;
+    if (i0 >= total) return;
+    const uint32_t i1 = total - i0 < (uint32_t)kSegHistItems ? total : i0 + kSegHistItems;
     const int tid = threadIdx.x;
+    const int npos = P - p0;
     for (int i = tid; i < P * kBins; i += kSegHistBlock) (&h[0][0])[i] = 0u;
     __syncthreads();
-    const uint64_t seg = sr.item_seg[item];
-    const uint64_t k = item - sr.item_start[seg];
-    const uint64_t len = sr.src.len(seg);
-    if (len < 2) return;  // not sorted (see k_radix_pass)
-    const K* in = reinterpret_cast<const K*>(sr.src.in_addr(seg)) + k * TILE;
-    const uint64_t rem = len - k * TILE;
-    const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
-    for (uint32_t i = tid; i < cnt; i += kSegHistBlock) {
-        const K key = to_key<K, XF>(__ldcs(in + i));
-        for (int p = p0; p < P; ++p) atomicAdd(&h[p][digit_of(key, 8 * p)], 1u);
+    auto flush = [&](uint64_t seg) {  // called by the whole CTA (segment ids are uniform)
+        __syncthreads();
+        for (int i = tid; i < npos * kBins; i += kSegHistBlock) {
+            uint32_t& c = h[p0 + i / kBins][i % kBins];
+            if (c) atomicAdd(&seg_hist[(seg * npos + i / kBins) * kBins + i % kBins], c);
+            c = 0u;
+        }
+        __syncthreads();
+    };
+    uint64_t cur = sr.item_seg[i0];
+    for (uint32_t item = i0; item < i1; ++item) {
+        const uint64_t seg = sr.item_seg[item];
+        if (seg != cur) {
+            flush(cur);
+            cur = seg;
+        }
+        const uint64_t len = sr.src.len(seg);
+        if (len < 2) continue;  // not sorted (see k_radix_pass)
+        const uint64_t k = item - sr.item_start[seg];
+        const K* in = reinterpret_cast<const K*>(sr.src.in_addr(seg)) + k * TILE;
+        const uint64_t rem = len - k * TILE;
+        const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+        K key[PER];
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const uint32_t i = (uint32_t)(tid + j * kSegHistBlock);
+            key[j] = i < cnt ? to_key<K, XF>(__ldcs(in + i)) : K(0);
+        }
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            if ((uint32_t)(tid + j * kSegHistBlock) >= cnt) break;
+            for (int p = p0; p < P; ++p) atomicAdd(&h[p][digit_of(key[j], 8 * p)], 1u);
+        }
     }
-    __syncthreads();
-    const int npos = P - p0;
-    for (int i = tid; i < npos * kBins; i += kSegHistBlock) {
-        const uint32_t v = h[p0 + i / kBins][i % kBins];
-        if (v) atomicAdd(&seg_hist[(seg * npos + i / kBins) * kBins + i % kBins], v);
-    }
+    flush(cur);
 }
 
 // Advances the device-side epoch of the segmented radix words by `npass` (so every replay
@@ -548,7 +574,9 @@ bool seg_radix_sort_keys(Workspace& ws, SegSrc src, uint64_t count, uint64_t S, 
             k_seg_map<256><<<seg_map_grid(S), 256, 0, s>>>(item_start, S, item_seg);
         if (!cuda_ok(cudaMemsetAsync(seg_hist, 0, hist_bytes, s), "segment histogram clear"))
             return false;
-        k_seg_radix_hist<K, XF><<<(unsigned)items_cap, kSegHistBlock, 0, s>>>(sr, p0, seg_hist);
+        k_seg_radix_hist<K, XF>
+            <<<(unsigned)((items_cap + kSegHistItems - 1) / kSegHistItems), kSegHistBlock, 0, s>>>(
+                sr, p0, seg_hist);
         k_seg_radix_epoch<<<1, 256, 0, s>>>(counters, npos, status, words);
         for (int p = p0; p < P; ++p) {
             SegRadix q = sr;
