@@ -175,7 +175,7 @@ typedef struct parallax_serve_config {
     uint32_t lanes;          /* batches in flight on the device (0: 8) */
     uint32_t max_batch;      /* requests per coalesced launch (0: 1024) */
     uint64_t solo_elements;  /* longer requests run alone (0: 2^18); sorts that take the
-                                radix path (from 2^16 4-byte / 2^19 8-byte keys) always do */
+                                radix path (from 2^16 4-byte / 2^20 8-byte keys) always do */
     uint64_t inflight_bytes; /* admission budget: operand + temporary bytes of admitted,
                                 unfinished requests (0: half the arena capacity) */
     uint32_t schedulers;     /* host threads that form and launch batches, each owning an
