@@ -1156,9 +1156,16 @@ def run_serving(px, lib, seconds: float) -> dict:
             f: getattr(s1, f) - getattr(s0, f) for f in
             ("requests", "batches", "coalesced_requests", "launch_ns", "complete_ns")}
         out["small_requests"]["serve_stats"]["max_batch"] = s1.max_batch
+        # the same clients as one thread each: submissions and a non-blocking poll of the
+        # oldest outstanding request (parallax_serve_poll) on one thread, instead of a second
+        # thread per client blocked in parallax_serve_wait
+        out["small_requests"]["served_saturation_polling"] = one(4, 0.0, 16, inflight=32)
         lib.parallax_serve_stop()
         out["small_requests"]["throughput_ratio"] = round(
             out["small_requests"]["served_saturation"]["req_s"] /
+            out["small_requests"]["per_call_saturation"]["req_s"], 3)
+        out["small_requests"]["throughput_ratio_polling"] = round(
+            out["small_requests"]["served_saturation_polling"]["req_s"] /
             out["small_requests"]["per_call_saturation"]["req_s"], 3)
         out["serve_stats"] = {"requests": st.requests, "batches": st.batches,
                               "coalesced_requests": st.coalesced_requests,

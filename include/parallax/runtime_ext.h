@@ -175,7 +175,7 @@ typedef struct parallax_serve_config {
     uint32_t lanes;          /* batches in flight on the device (0: 8) */
     uint32_t max_batch;      /* requests per coalesced launch (0: 1024) */
     uint64_t solo_elements;  /* longer requests run alone (0: 2^18); sorts that take the
-                                radix path (from 2^16 4-byte / 2^20 8-byte keys) always do */
+                                radix path (from 2^20 keys) always do */
     uint64_t inflight_bytes; /* admission budget: operand + temporary bytes of admitted,
                                 unfinished requests (0: half the arena capacity) */
     uint32_t schedulers;     /* host threads that form and launch batches, each owning an
@@ -209,11 +209,16 @@ typedef struct parallax_serve_stats {
 int parallax_serve_start(const parallax_serve_config* cfg);
 /* Finishes every submitted request, then stops the loop. */
 int parallax_serve_stop(void);
-/* Queues a request; *ticket is waited on exactly once with parallax_serve_wait. */
+/* Queues a request; *ticket is waited on exactly once with parallax_serve_wait (or polled
+ * with parallax_serve_poll until it reports the request finished). */
 int parallax_serve_submit(const parallax_request* req, uint64_t* ticket);
 /* Blocks until the request finished; returns its parallax_status and, when done_ns is not
  * NULL, its completion time on parallax_clock_ns()'s clock. */
 int parallax_serve_wait(uint64_t ticket, uint64_t* done_ns);
+/* Non-blocking wait: *finished = 0 and PARALLAX_OK while the request runs (the ticket stays
+ * valid); once it has finished, *finished = 1 and the call returns what parallax_serve_wait
+ * would (status, done_ns) and consumes the ticket. */
+int parallax_serve_poll(uint64_t ticket, int* finished, uint64_t* done_ns);
 /* submit + wait: the blocking call a client thread makes. */
 int parallax_serve_call(const parallax_request* req);
 int parallax_serve_get_stats(parallax_serve_stats* out);

@@ -126,6 +126,7 @@ _SIGNATURES = {
     "parallax_serve_stop": (C.c_int, []),
     "parallax_serve_submit": (C.c_int, [C.POINTER(Request), C.POINTER(u64)]),
     "parallax_serve_wait": (C.c_int, [u64, C.POINTER(u64)]),
+    "parallax_serve_poll": (C.c_int, [u64, C.POINTER(C.c_int), C.POINTER(u64)]),
     "parallax_serve_call": (C.c_int, [C.POINTER(Request)]),
     "parallax_serve_get_stats": (C.c_int, [C.POINTER(ServeStats)]),
     "parallax_clock_ns": (u64, []),

@@ -627,9 +627,10 @@ bool seg_sort_dispatch(Workspace& ws, DType t, const SegSrc& src, uint64_t count
 
 // Sizes from which the radix sort (a histogram launch plus one pass per key byte) beats the
 // merge sort (a tile-sort launch plus log2(tiles) merge passes). PARALLAX_SORT=merge or
-// =radix forces one path (read on every call). 8-byte keys, both paths timed on B200
-// (random int64): 2^19 radix 0.134 / merge 0.099 ms, 2^20 0.139 / 0.143, 2^21 0.185 / 0.206.
-constexpr size_t kRadixMin4 = size_t(1) << 16;
+// =radix forces one path (read on every call). Both paths timed on B200 (random keys):
+// 4-byte 2^19 radix 0.074 / merge 0.062 ms, 2^20 0.082 / 0.088, 2^21 0.100 / 0.125;
+// 8-byte 2^19 0.134 / 0.099 ms, 2^20 0.139 / 0.143, 2^21 0.185 / 0.206.
+constexpr size_t kRadixMin4 = size_t(1) << 20;
 constexpr size_t kRadixMin8 = size_t(1) << 20;
 
 size_t sort_radix_min(DType t) { return dtype_size(t) == 4 ? kRadixMin4 : kRadixMin8; }

@@ -86,10 +86,6 @@ void finish(Request* r, int status) {
     r->released.store(true, std::memory_order_release);
 }
 
-// Blocks until the request has been finished; returns its status. Short requests finish
-// within microseconds of their launch, so the waiter first polls the completion flag for up
-// to 20 us, then sleeps between polls (about 20 us asked; the kernel's timer slack makes it
-// longer), which costs a long request no more than that in latency.
 // How long a waiter polls its request's flag before it sleeps (PARALLAX_SERVE_SPIN_US).
 uint64_t spin_ns() {
     static const uint64_t ns = [] {
@@ -99,6 +95,10 @@ uint64_t spin_ns() {
     return ns;
 }
 
+// Blocks until the request has been finished; returns its status. Short requests finish
+// within microseconds of their launch, so the waiter first polls the completion flag (20 us
+// by default), then sleeps between polls (about 20 us asked; the kernel's timer slack makes
+// it longer), which costs a long request no more than that in latency.
 int wait_request(Request* r, uint64_t* done_ns) {
     const uint64_t poll_until = now_ns() + spin_ns();
     for (int i = 1; !r->released.load(std::memory_order_acquire); ++i) {
@@ -166,7 +166,10 @@ class Server {
     // (no scan of the whole queue under the lock).
     std::map<KindKey, std::deque<Request*>> kinds;
     std::deque<Request*> solo;
-    uint64_t queued = 0, arrivals = 0;
+    // queued is changed under mu; a scheduler reads it without mu to skip the lock when
+    // there is nothing to form
+    std::atomic<uint64_t> queued{0};
+    uint64_t arrivals = 0;
     bool stopping = false;
     std::atomic<uint64_t> inflight{0};  // admitted bytes (released without the lock)
     parallax_serve_stats stats{};
@@ -407,6 +410,17 @@ class Server {
                 if (e != cudaSuccess) cudaGetLastError();
                 progress = true;
             }
+            if (any_busy && !progress) {
+                // lanes still running: take the queue lock only when a request waits and one
+                // of this scheduler's lanes is free (two schedulers polling their lanes would
+                // otherwise hold the lock that every submission needs most of the time)
+                bool free_lane = false;
+                for (size_t li = lo; li < hi && !free_lane; ++li) free_lane = !lanes[li].busy;
+                if (!free_lane || queued.load(std::memory_order_relaxed) == 0) {
+                    std::this_thread::yield();
+                    continue;
+                }
+            }
             std::unique_lock<std::mutex> lk(mu);
             for (size_t li = lo; li < hi; ++li) {
                 Lane& l = lanes[li];
@@ -594,6 +608,27 @@ PXB_EXPORT int parallax_serve_wait(uint64_t ticket, uint64_t* done_ns) {
     } else {
         st = wait_request(r, done_ns);
     }
+    delete r;
+    if (st != PARALLAX_OK) set_error(st, "served request failed (status %d)", st);
+    return st;
+}
+
+PXB_EXPORT int parallax_serve_poll(uint64_t ticket, int* finished, uint64_t* done_ns) {
+    set_ok();
+    auto* r = reinterpret_cast<Request*>(ticket);
+    if (!r || !finished) {
+        set_error(PARALLAX_ERR_INVALID_ARGUMENT, "parallax_serve_poll: null ticket or flag");
+        return PARALLAX_ERR_INVALID_ARGUMENT;
+    }
+    // One acquire load: a client that keeps many requests in flight checks its oldest one
+    // between submissions, with no thread of its own blocked in parallax_serve_wait.
+    if (!r->released.load(std::memory_order_acquire)) {
+        *finished = 0;
+        return PARALLAX_OK;
+    }
+    *finished = 1;
+    const int st = r->status;
+    if (done_ns) *done_ns = r->done_ns;
     delete r;
     if (st != PARALLAX_OK) set_error(st, "served request failed (status %d)", st);
     return st;

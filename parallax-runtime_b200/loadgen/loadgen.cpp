@@ -19,7 +19,8 @@
 // Latency = completion - arrival time. The per-call path issues a thread's requests in
 // order, so a request that arrives while its thread is busy waits, as it would in a client
 // with one connection; the served path submits at arrival and collects completions on a
-// second thread, with at most `max_inflight` outstanding requests per client thread.
+// second thread (mode 1) or on the same thread by polling (mode 4), with at most
+// `max_inflight` outstanding requests per client.
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -48,7 +49,9 @@ typedef struct px_loadgen_config {
                                 calls asynchronously on its own stream and synchronizes once
                                 per 64 calls, so the rate is what the device sustains for the
                                 mix with no host round trip per request (latencies are not
-                                meaningful in this mode) */
+                                meaningful in this mode), 4 served with one thread per client
+                                (submissions and parallax_serve_poll of the oldest outstanding
+                                request on the same thread) */
     double rate;             /* offered requests/s over all threads; <= 0: back-to-back */
     double seconds;          /* issuing window */
     uint64_t seed;
@@ -261,7 +264,7 @@ void warm_up(const px_loadgen_config& c) {
         it.t = 1;  // fp64: the largest buffers
         it.n = std::min<uint64_t>(1ull << c.log2_max, kPoolElems);
         while (!alloc_buf(it)) std::this_thread::yield();
-        if (c.mode != 1) {
+        if (c.mode != 1 && c.mode != 4) {
             run_call(it);
         } else if (submit(it) == PARALLAX_OK) {
             parallax_serve_wait(it.ticket, nullptr);
@@ -342,6 +345,66 @@ void client(const px_loadgen_config& c, int tid, StartLine* line, ThreadOut* out
             out->items.push_back(it);
             advance();
         }
+        return;
+    }
+    if (c.mode == 4) {
+        // served, one thread per client: submit at arrival while fewer than max_inflight of
+        // the client's requests are outstanding, and between submissions poll the oldest
+        // outstanding one (parallax_serve_poll), so no second thread waits per client. The
+        // item vector never reallocates (capacity reserved up front).
+        std::vector<Item>& items = out->items;
+        items.reserve(1 << 16);
+        std::deque<size_t> pending;
+        auto collect = [&]() -> bool {  // true when the oldest outstanding request finished
+            if (pending.empty()) return false;
+            Item& it = items[pending.front()];
+            int fin = 0;
+            uint64_t done = 0;
+            const int st = parallax_serve_poll(it.ticket, &fin, &done);
+            if (!fin) return false;
+            it.status = st;
+            it.done = done;
+            free_buf(it);
+            pending.pop_front();
+            return true;
+        };
+        uint32_t idle = 0;
+        auto pause = [&] {
+            __builtin_ia32_pause();
+            if ((++idle & 255) == 0) std::this_thread::yield();
+        };
+        sleep_until(t0);
+        Item next = make_item(r, c);
+        next.arrival = per_thread_rate > 0 ? next_arrival : now_ns();
+        for (;;) {
+            const uint64_t now = now_ns();
+            if ((per_thread_rate > 0 ? next.arrival : now) >= t_end ||
+                items.size() + 1 >= items.capacity())
+                break;
+            if (now >= next.arrival && pending.size() < c.max_inflight) {
+                if (!alloc_buf(next)) {  // arena full: wait for this client's oldest request
+                    if (!collect()) pause();
+                    continue;
+                }
+                if (per_thread_rate <= 0) next.arrival = now_ns();
+                items.push_back(next);
+                Item& stored = items.back();
+                if (submit(stored) != PARALLAX_OK) {
+                    stored.status = parallax_last_error();
+                    stored.done = now_ns();
+                    free_buf(stored);
+                } else {
+                    pending.push_back(items.size() - 1);
+                }
+                advance();
+                next = make_item(r, c);
+                next.arrival = per_thread_rate > 0 ? next_arrival : now_ns();
+                continue;
+            }
+            if (!collect()) pause();
+        }
+        while (!pending.empty())
+            if (!collect()) pause();
         return;
     }
     // served: submit at arrival, a waiter thread collects completions in order. The item
@@ -473,7 +536,7 @@ LG_EXPORT void px_loadgen_release(void) {
     g_pool.ready = false;
 }
 
-// Runs one measurement; the serving loop must be running for mode 1.
+// Runs one measurement; the serving loop must be running for modes 1 and 4.
 LG_EXPORT int px_loadgen_run(const px_loadgen_config* cfg, px_loadgen_result* res) {
     if (!cfg || !res || !g_pool.ready) return PARALLAX_ERR_INVALID_ARGUMENT;
     px_loadgen_config c = *cfg;

@@ -246,6 +246,30 @@ def test_served_equals_plain_abi(server, px, dev, ox):
     assert r.output() == np.frombuffer(bytes(out), np.int64)[0] == ox.reduce_sum(x)
 
 
+def test_poll_until_finished(server, px, dev, ox):
+    """parallax_serve_poll: not finished (ticket kept) until the request completes, then the
+    status and result parallax_serve_wait would give; an empty request is finished at once."""
+    lib = server
+    x = make(ox, "f64", 300001, 78)
+    r = Req(px, dev, "reduce:sum:f64", x, "reduce")
+    t = C.c_uint64()
+    assert lib.parallax_serve_submit(C.byref(r.req), C.byref(t)) == px.OK
+    fin, done, polls = C.c_int(0), C.c_uint64(0), 0
+    while True:
+        st = lib.parallax_serve_poll(t.value, C.byref(fin), C.byref(done))
+        polls += 1
+        if fin.value:
+            break
+        assert st == px.OK
+    assert st == px.OK and done.value > 0 and polls >= 1
+    assert np.isclose(r.output(), ox.reduce_sum(x), rtol=1e-12)
+    e = Req(px, dev, "reduce:sum:f64", x[:0], "reduce")
+    assert lib.parallax_serve_submit(C.byref(e.req), C.byref(t)) == px.OK
+    assert lib.parallax_serve_poll(t.value, C.byref(fin), None) == px.OK and fin.value == 1
+    assert lib.parallax_serve_poll(0, C.byref(fin), None) == px.ERR_INVALID_ARGUMENT
+    lib.parallax_clear_error()
+
+
 def test_errors(server, px, dev):
     lib = server
     r = px.Request()
