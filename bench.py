@@ -266,12 +266,19 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a while to start: wait for its first sample, then drop what came
+        # before the timed region, so every sample counted was taken inside it
+        t_end = time.perf_counter() + 3.0
+        while not self.lines and time.perf_counter() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.lines.clear()
 
     def _read(self):
         for ln in self.proc.stdout:
@@ -646,10 +653,10 @@ def main() -> None:
     lib.parallax_profile_enable(1)
 
     clocks = ClockSampler(local)
+    clocks.start()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
     launches0 = lib.parallax_launch_count()
     t_wall = time.perf_counter()
     for _ in range(args.steps):
