@@ -294,9 +294,15 @@ class ClockSampler:
             self.proc.kill()
         if self.t:
             self.t.join(timeout=2)
+        return self.summary(self.lines)
+
+    @staticmethod
+    def summary(lines: list[str]) -> dict:
+        """Median SM clock, the max clock and the throttle reasons seen, from nvidia-smi's
+        CSV lines (the QUERY fields, no header, no units)."""
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in lines:
             f = [v.strip() for v in ln.split(",")]
             if len(f) < 9:
                 continue

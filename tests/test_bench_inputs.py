@@ -38,3 +38,22 @@ def test_step_inputs_shapes(bench):
     assert kept["copy_if_i32"] == int(np.count_nonzero(x["i32"] % 3 == 0))
     assert bench.op_key("inclusive_scan_f64") == "f64" and bench.op_key("sort_f32") == "sort_f32"
     assert set(bench.make_inputs(12, 11, keys={"sort_u32"})) == {"sort_u32"}
+
+
+def test_clock_summary(bench):
+    """Throttle reasons and the median clock come from the sampled CSV lines; malformed and
+    unavailable fields are skipped."""
+    lines = [
+        "0, 1965, 1965, 812.3, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "0, 1965, 1965, 990.1, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "0, 1890, 1965, 1000.2, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "garbage",
+        "0, [N/A], 1965, 0, 0x0, Not Active, Not Active, Not Active, Not Active",
+    ]
+    c = bench.ClockSampler.summary(lines)
+    assert c["samples"] == 3 and c["sm_mhz"] == 1965.0 and c["sm_max_mhz"] == 1965.0
+    assert c["reasons"] == ["sw_power_cap"]
+    hw = bench.ClockSampler.summary(
+        ["0, 1200, 1965, 700, 0x8, Active, Not Active, Active, Not Active"])
+    assert hw["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"] and hw["sm_mhz"] == 1200.0
+    assert bench.ClockSampler.summary([])["samples"] == 0
